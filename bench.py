@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark: explicit uGIMP MPM steps on the 3D granular column collapse.
+
+Workload (per GPU): 3D column collapse, domain 1.2 x 0.4 x 0.6 m, h = 5 mm,
+column 0.5 x 0.2 x 0.4 m at 2x2x2 particles per cell = 2 560 000 particles,
+Mohr-Coulomb (phi = 30 deg, c = 0, psi = 0), rho = 2650, E = 1 MPa, nu = 0.3,
+free-slip walls, CFL 0.2, FP32 bulk with FP64 positions and det(F).  A bench
+step is one MPM time step over all particles (cell re-sort every 8 steps
+included).  The particle state (~0.5 GB) exceeds the 126 MB L2, so no flush is
+needed between steps.
+
+Metric: particle-updates/s = particles x steps / device time (max over ranks).
+Multi-GPU runs are independent replicas (the reference has no multi-GPU path):
+value = sum of particles x steps over ranks / max time, scaling "weak".
+
+--impl reference times the CPU restatement of the reference's path
+(oracle/, OpenMP on all host cores) on the same workload, one MPM step per
+bench step.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mc3d", default="literal", choices=["literal", "restated"])
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only W warm-up + K device steps (the command profilers wrap)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def make_case(mc3d):
+    import __graft_entry__ as g
+    pkg = g.load_package()
+    case = pkg.workloads.column_collapse_3d(mc3d=mc3d)
+    return pkg, case
+
+
+def pin_particles(mp):
+    """Move the particle arrays into page-locked host memory (torch pinned
+    buffers viewed as numpy) so host<->device copies run at full PCIe rate."""
+    try:
+        import torch
+    except ImportError:
+        return
+    for name in ("xi", "vs", "sig", "eps", "epsq", "epsk", "epsv", "Omega", "Omega0", "rho", "rho0", "F",
+                 "ms", "sigm"):
+        a = getattr(mp, name)
+        t = torch.empty(a.size, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        b = t.numpy()
+        if a.ndim == 2:
+            b = b.reshape(a.shape[1], a.shape[0]).T   # column-major view
+        b[...] = a
+        setattr(mp, name + "_pinned_owner", t)
+        setattr(mp, name, b)
+
+
+# algorithmic bytes (SURVEY-style accounting)
+BP_STEP_3D = 212       # particle state read + written once per step
+BN_STEP_3D = 156       # compulsory grid traffic per active node per step
+BP_G2P_3D = 200        # fused G2P+stress+P2G kernel: its own particle bytes
+BN_G2P_3D = 40         # Δu read (3 floats) + m, p, f written (7 floats)
+
+
+def run_b200(args):
+    rank, world, local = dist_env()
+    pkg, case = make_case(args.mc3d)
+    lib = pkg._lib
+    use_dist = world > 1
+    if use_dist:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    npart = case.mp.np
+    dt = case.dt
+    K, W = args.steps, max(args.warmup, 3)
+
+    # ---- end to end through the public API: host arrays -> device -> host ----
+    pin_particles(case.mp)
+    out = pkg.Particle3D(dx=case.mp.dx, dy=case.mp.dy, dz=case.mp.dz, xi=case.mp.xi, rho=case.mp.rho)
+    pin_particles(out)
+
+    def e2e_once(nsteps):
+        t0 = time.perf_counter()
+        dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
+        dev.step(dt, 0.0, nsteps)
+        dev.download(lib.F_REFERENCE, out)
+        t1 = time.perf_counter()
+        dev.close()
+        return t1 - t0
+
+    e2e_once(W)                       # warm: context, module load, first allocations
+    e2e_t = e2e_once(K)
+    h2d = npart * 8 * (3 + 3 + 6 + 6 + 3 + 4 + 9) + npart * 8   # uploaded particle columns (FP64) + nid
+    d2h = npart * 8 * (1 + 3 + 3 + 1 + 6 + 1 + 1 + 1 + 6 + 1)   # device2host! field set (FP64)
+
+    # ---- device-timed region (inputs resident in HBM) ----
+    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
+    dev.step(dt, 0.0, W)
+    Ti = W * dt
+    if use_dist:
+        dist.barrier()
+    launches0 = dev.stats().launches
+    with ClockSampler(local) as clk:
+        dev.step_async(dt, Ti, K)
+        dev.sync()
+    st = dev.stats()
+    ms = st.last_step_ms
+    launches = st.launches - launches0
+    na = st.active_nodes
+    Ti += K * dt
+    t_max = ms
+    if use_dist:
+        tt = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * npart * K / (t_max * 1e-3)
+
+    # ---- per-kernel device times (events on the library stream) ----
+    dev.set_profiling(True)
+    dev.step(dt, Ti, 16)
+    kt = dev.kernel_times()
+    dev.set_profiling(False)
+    dev.close()
+    dom = "g2p_p2g"
+    dom_ms = kt.get(dom, (float("nan"), 0))[0]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    alg_bytes = npart * BP_G2P_3D + na * BN_G2P_3D
+    achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
+    step_bytes = npart * BP_STEP_3D + na * BN_STEP_3D
+    step_achieved = step_bytes / (ms * 1e-3 / K) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "g2p_p2g_traffic.json")
+    if os.path.exists(tp):
+        try:
+            tj = json.load(open(tp))
+            traffic = tj["bytes_per_particle"] * npart + tj.get("bytes_per_active_node", 0) * na
+        except (OSError, KeyError, ValueError):
+            traffic = None
+
+    result = {
+        "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": t_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded lattice + jitter, seed 1002)",
+        "config": {"workload": "3D granular column collapse, uGIMP, MUSL va=:a",
+                   "particles": npart, "nodes": case.grid.ni, "active_nodes": na,
+                   "h": case.meta["h"], "constitutive": "mohrcoulomb", "mc3d": args.mc3d,
+                   "precision": "FP32 bulk, FP64 positions and det(F)",
+                   "sort_every": 8, "l2": "particle state 0.5 GB > 126 MB L2 (no flush needed)",
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": launches,
+        "kernel_ms": {k: v[0] for k, v in kt.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                     "step_achieved": step_achieved, "step_frac": step_achieved / peak},
+        "e2e": {"value": npart * K / e2e_t, "unit": "particle-updates/s",
+                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+                "what": "DeviceModel upload from pinned host arrays + K steps + device2host! field set"},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(args.mc3d)
+    if use_dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+def oracle_threads():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def cpu_baseline(mc3d, steps=4):
+    """The FP64 CPU restatement of the reference path (OpenMP, all host cores)
+    on the same 2.56 M-particle column: 1 warm-up step + `steps` timed steps."""
+    from oracle import oracle as orc
+    pkg, case = make_case(mc3d)
+    nth = oracle_threads()
+    o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc, nthreads=nth)
+    o.run(case.dt, 0.0, 1)
+    t0 = time.perf_counter()
+    o.run(case.dt, case.dt, steps)
+    t = time.perf_counter() - t0
+    return {"value": case.mp.np * steps / t, "unit": "particle-updates/s", "cores": nth,
+            "kind": "port", "sample": f"{steps} steps of the full {case.mp.np}-particle column after 1 warm-up step"}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    pkg, case = make_case(args.mc3d)
+    nth = oracle_threads()
+    o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc, nthreads=nth)
+    K, W = args.steps, max(args.warmup, 3)
+    # each bench step: one MPM step of the full workload; bounded so the run ends in minutes
+    t_first = time.perf_counter()
+    o.run(case.dt, 0.0, 1)
+    t1 = time.perf_counter() - t_first
+    budget = 240.0
+    Wr = min(W - 1, max(0, int(budget * 0.2 / max(t1, 1e-3))))
+    o.run(case.dt, case.dt, Wr)
+    Kr = K if (K * t1) < budget else max(1, int(budget / max(t1, 1e-3)))
+    t0 = time.perf_counter()
+    o.run(case.dt, (1 + Wr) * case.dt, Kr)
+    t = time.perf_counter() - t0
+    value = case.mp.np * Kr / t
+    line = {
+        "impl": "reference", "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": t / Kr * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seed 1002)",
+        "config": {"workload": "3D granular column collapse, uGIMP, MUSL va=:a", "particles": case.mp.np,
+                   "constitutive": "mohrcoulomb", "mc3d": args.mc3d,
+                   "implementation": "FP64 C++ restatement of the reference CPU path (oracle/), OpenMP"},
+        "cpu_baseline": {"value": value, "unit": "particle-updates/s", "cores": nth, "kind": "port",
+                         "sample": f"{Kr} MPM steps of the full {case.mp.np}-particle column "
+                                   f"(after {1 + Wr} warm-up steps)"},
+        "e2e": {"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_profile(args):
+    """Minimal launch sequence for profilers: upload, W + K steps, exit."""
+    pkg, case = make_case(args.mc3d)
+    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+    dev.step(case.dt, 0.0, args.warmup)
+    dev.step(case.dt, args.warmup * case.dt, args.steps)
+    st = dev.stats()
+    dev.close()
+    print(json.dumps({"profile_run": True, "steps": args.steps, "warmup": args.warmup,
+                      "last_ms": st.last_step_ms, "launches": st.launches}))
+
+
+def main():
+    args = parse()
+    if args.profile_run:
+        run_profile(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

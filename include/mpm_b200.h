@@ -1,0 +1,209 @@
+/*
+ * mpm_b200.h -- C ABI of libmpm_b200.so, the B200 (sm_100a) backend for the
+ * one-phase explicit uGIMP MPM step of MaterialPointSolver.jl.
+ *
+ * The entry points replace the reference's device boundary and step workflow
+ * (paths relative to the MaterialPointSolver.jl repository):
+ *
+ *   mpm_create + mpm_upload   host2device   ext/CUDAExt/devicehelpfunc_cuda.jl:17-37
+ *   mpm_step                  procedure!    src/solvers/OS_MUSL.jl:12-102, called
+ *                                           per step by submit_work!, src/solver.jl:84,119
+ *   mpm_download              device2host!  ext/CUDAExt/devicehelpfunc_cuda.jl:39-69
+ *   mpm_destroy               clean_device! ext/CUDAExt/devicehelpfunc_cuda.jl:71-100
+ *   mpm_compute_p2c           the p2c part of resetmpstatus_OS!, src/solvers/utils_OS.jl:203-205,325-328
+ *   mpm_peak_bandwidth        Tpeak,        ext/CUDAExt/devicehelpfunc_cuda.jl:102-136
+ *
+ * Host arrays are passed as views of the caller's arrays in the reference's
+ * layout: Julia column-major `n x k` matrices (component k of item i at
+ * ptr[i + ld*k]), element type tagged per view, indices 1-based.
+ *
+ * Conventions: every function returns MPM_OK (0) or a negative MPM_E_* code;
+ * nothing throws across the ABI; mpm_last_error() returns the message of the
+ * last failure on a handle.  One handle is used by one host thread at a time.
+ * All device memory belongs to the handle until mpm_destroy().
+ */
+#ifndef MPM_B200_H
+#define MPM_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_ABI_VERSION 1
+
+/* return codes */
+#define MPM_OK 0
+#define MPM_E_ARG (-1)           /* invalid argument / descriptor */
+#define MPM_E_CUDA (-2)          /* CUDA runtime error (message has details) */
+#define MPM_E_OUT_OF_GRID (-3)   /* a particle's stencil left the grid */
+#define MPM_E_NONPOSITIVE_J (-4) /* det(F) <= 0 on some particle */
+#define MPM_E_NAN (-5)           /* non-finite particle state */
+#define MPM_E_STATE (-6)         /* call out of order (e.g. step before upload) */
+#define MPM_E_CELL_OVERFLOW (-7) /* more particles in one cell than the sort handles */
+#define MPM_E_UNSUPPORTED (-8)   /* option not provided by this backend */
+
+/* constitutive models (Args.constitutive) */
+#define MPM_LINEARELASTIC 0
+#define MPM_DRUCKERPRAGER 1
+#define MPM_MOHRCOULOMB 2
+
+/* arithmetic of the device step */
+#define MPM_PREC_MIXED 0 /* FP32 bulk, FP64 positions and det(F)/volume */
+#define MPM_PREC_FP64 1  /* all FP64 (self-check mode) */
+
+/* velocity update mode (Args.va) */
+#define MPM_VA_A 0
+#define MPM_VA_V 1
+
+/* 3D Mohr-Coulomb: the reference's 3D mcP! body is commented out, so its 3D
+ * "mohrcoulomb" run is the elastic predictor only (LITERAL).  RESTATED applies
+ * the predictor-corrector Mohr-Coulomb return mapping. */
+#define MPM_MC3D_LITERAL 0
+#define MPM_MC3D_RESTATED 1
+
+/* element type tags of host views */
+#define MPM_T_F64 0
+#define MPM_T_F32 1
+#define MPM_T_I64 2
+#define MPM_T_I32 3
+
+typedef struct mpm_handle mpm_handle;
+
+/* Model description: grid (Grid2D/3D), particle sizes (Particle2D/3D dx,dy,dz)
+ * and run arguments (Args2D/3D). */
+typedef struct {
+    int32_t abi_version;   /* MPM_ABI_VERSION */
+    int32_t dim;           /* 2 or 3 */
+    int32_t precision;     /* MPM_PREC_* */
+    int32_t device;        /* CUDA device ordinal */
+    int64_t np;            /* particles (mp.np) */
+    int64_t nmat;          /* materials (length of the Property arrays) */
+    int64_t nnx, nny, nnz; /* nodes per axis (grid.nnx, nny, nnz; nnz = 1 in 2D) */
+    double x1, y1, z1;     /* grid origin */
+    double dx, dy, dz;     /* cell size */
+    double lpx, lpy, lpz;  /* particle size (mp.dx, mp.dy, mp.dz) */
+    int32_t constitutive;  /* MPM_LINEARELASTIC / DRUCKERPRAGER / MOHRCOULOMB */
+    int32_t va;            /* MPM_VA_A / MPM_VA_V */
+    int32_t mvl;           /* Args.MVL */
+    int32_t mc3d;          /* MPM_MC3D_* */
+    double FLIP, PIC;      /* Args.FLIP, Args.PIC */
+    double zeta_s;         /* Args.ζs */
+    double gravity;        /* Args.gravity */
+    double Te;             /* Args.Te */
+    int32_t time_f32;      /* 1: accumulate Ti in Float32 (reference FP32 mode) */
+    int32_t sort_every;    /* re-sort period in steps (0 = library default) */
+} mpm_desc;
+
+/* A host array view. */
+typedef struct {
+    void *ptr;     /* NULL = not supplied */
+    int32_t type;  /* MPM_T_* */
+    int32_t pad;
+    int64_t ld;    /* leading dimension (rows) of the column-major array */
+} mpm_view;
+
+/* Host views of the reference structs' arrays (names as in the reference). */
+typedef struct {
+    /* Particle2D/3D */
+    mpm_view xi;      /* ξ      np x dim   */
+    mpm_view vs;      /* vs     np x dim   */
+    mpm_view sig;     /* σij    np x 4|6   (Voigt xx,yy,zz,xy[,yz,zx]) */
+    mpm_view eps;     /* ϵijs   np x 4|6   */
+    mpm_view epsq;    /* ϵq     np         */
+    mpm_view epsk;    /* ϵk     np         */
+    mpm_view epsv;    /* ϵv     np         */
+    mpm_view Omega;   /* Ω      np         */
+    mpm_view Omega0;  /* Ω0     np         */
+    mpm_view rho;     /* ρs     np         */
+    mpm_view rho0;    /* ρs0    np         */
+    mpm_view F;       /* F      np x dim^2 (row-major components) */
+    mpm_view ms;      /* ms     np         (download only) */
+    mpm_view sigm;    /* σm     np         (download only) */
+    mpm_view p2c;     /* p2c    np         (download only, 1-based) */
+    /* Property */
+    mpm_view nid;     /* nid    np         (1-based material id) */
+    mpm_view Ks, Gs, c, phi, psi, sigt, Hp, cr; /* nmat each */
+    /* VBoundary2D/3D, per node in the reference's node order */
+    mpm_view vx_idx, vx_val, vy_idx, vy_val, vz_idx, vz_val;
+} mpm_host_views;
+
+/* download field mask */
+#define MPM_F_XI (1u << 0)
+#define MPM_F_VS (1u << 1)
+#define MPM_F_SIG (1u << 2)
+#define MPM_F_EPS (1u << 3)
+#define MPM_F_EPSQ (1u << 4)
+#define MPM_F_EPSK (1u << 5)
+#define MPM_F_EPSV (1u << 6)
+#define MPM_F_OMEGA (1u << 7)
+#define MPM_F_MS (1u << 8)
+#define MPM_F_SIGM (1u << 9)
+#define MPM_F_F (1u << 10)
+#define MPM_F_RHO (1u << 11)
+#define MPM_F_P2C (1u << 12)
+/* the set device2host! copies (devicehelpfunc_cuda.jl:46-55) */
+#define MPM_F_REFERENCE (MPM_F_SIGM | MPM_F_VS | MPM_F_XI | MPM_F_OMEGA | MPM_F_SIG | \
+                         MPM_F_EPSK | MPM_F_EPSQ | MPM_F_EPSV | MPM_F_EPS | MPM_F_MS)
+
+typedef struct {
+    int64_t steps_done;        /* steps run on this handle */
+    int64_t sorts_done;        /* particle re-sorts */
+    int64_t active_nodes;      /* nodes with mass > 0 in the current P2G accumulators */
+    int64_t launches;          /* kernel launches issued by this handle so far */
+    int32_t error_flags;       /* sticky device error bits (MPM_E_* as 1 << -code) */
+    int32_t kernels_per_step;  /* kernel launches per step */
+    double last_step_ms;       /* device time of the last mpm_step call, ms */
+    double device_bytes;       /* device memory held by the handle, bytes */
+} mpm_stats;
+
+/* ---- lifecycle (host2device / clean_device!) ---- */
+int mpm_create(const mpm_desc *desc, mpm_handle **out);
+int mpm_upload(mpm_handle *h, const mpm_host_views *v);
+int mpm_destroy(mpm_handle *h);
+
+/* ---- the step (procedure!) ----
+ * Runs `nsteps` consecutive steps starting at time Ti0 with step dt; Ti is
+ * advanced like submit_work!'s `Ti += ΔT` (in Float32 if desc.time_f32).
+ * Returns after the device finished; *Ti_out (optional) receives the end time. */
+int mpm_step(mpm_handle *h, double dt, double Ti0, int64_t nsteps, double *Ti_out);
+/* Asynchronous variant on the handle's stream; errors surface at mpm_sync. */
+int mpm_step_async(mpm_handle *h, double dt, double Ti0, int64_t nsteps);
+int mpm_sync(mpm_handle *h);
+
+/* ---- results (device2host!) ---- */
+int mpm_download(mpm_handle *h, const mpm_host_views *v, uint32_t field_mask);
+/* p2c (1-based, the reference's formula) of the current positions, original order. */
+int mpm_compute_p2c(mpm_handle *h, int64_t *p2c_out);
+/* Current device order: out[k] = 0-based original index of the k-th stored particle. */
+int mpm_download_order(mpm_handle *h, int64_t *order_out);
+/* Re-sort particles by cell now (normally done every desc.sort_every steps). */
+int mpm_sort(mpm_handle *h);
+
+/* ---- grid introspection for per-stage checks ----
+ * Runs the stages of one step selected by stage_mask (bit 0 P2G, 1 grid solve,
+ * 2 double mapping (DM1+DM2), 3 DM3, 4 G2P + stress) at time Ti, then copies
+ * grid field `field` (0 mass, 1 momentum, 2 force, 3 vsT, 4 as, 5 Δu, 6 vs)
+ * into host (ni x dim column-major FP64, reference node order). */
+int mpm_run_stages(mpm_handle *h, double dt, double Ti, uint32_t stage_mask);
+int mpm_download_grid(mpm_handle *h, int32_t field, double *out);
+
+/* ---- diagnostics ---- */
+/* sizeof(mpm_desc), sizeof(mpm_view), sizeof(mpm_host_views), sizeof(mpm_stats):
+ * lets a binding verify its struct layouts against the library's. */
+int mpm_abi_sizes(int64_t *desc, int64_t *view, int64_t *views, int64_t *stats);
+int mpm_get_stats(mpm_handle *h, mpm_stats *out);
+const char *mpm_last_error(mpm_handle *h);
+/* Triad bandwidth probe (Tpeak): bytes moved / best time, GB/s. */
+int mpm_peak_bandwidth(int32_t device, double *gbs_out);
+/* Average device time per launch of each kernel over the last timed mpm_step
+ * (enabled by mpm_set_profiling): names and ms, up to `cap` entries. */
+int mpm_set_profiling(mpm_handle *h, int32_t on);
+int mpm_get_kernel_times(mpm_handle *h, const char **names, double *ms, int64_t *launches,
+                         int32_t cap, int32_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPM_B200_H */

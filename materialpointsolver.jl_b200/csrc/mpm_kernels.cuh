@@ -1,0 +1,520 @@
+// mpm_kernels.cuh -- the kernels of one explicit uGIMP MUSL step.
+//
+// Step order of procedure!(…, Val(:OS), Val(:MUSL), Val(:a)),
+// src/solvers/OS_MUSL.jl:58-102, mapped onto four launches:
+//
+//   k_solve      solvegrid_a_OS! / solvegrid_OS!   (nodes)     utils_OS.jl:507-640
+//   k_dmap       doublemapping1(_a)_OS! + doublemapping2_OS!   utils_OS.jl:698-959
+//   k_dm3        doublemapping3_OS!                (nodes)     utils_OS.jl:968-1016
+//   k_g2p<FUSE>  G2P_OS! + liE! + dpP!/mcP!, and with FUSE the next step's
+//                resetmpstatus_OS! + P2G_OS! at the new positions
+//                                                   utils_OS.jl:178-496, 1025-1153
+//
+// resetgridstatus_OS! (utils_OS.jl:58-99) has no launch: the node passes clear
+// the accumulators right after consuming them (k_solve clears momentum and
+// force, k_dm3 clears mass and momentum), so the grid is zero again when the
+// next P2G scatters.  Particle weights are recomputed from positions in each
+// particle pass instead of being stored per particle.
+#pragma once
+#include "mpm_device.cuh"
+
+namespace mpm {
+
+// Particle state, structure of arrays.  Positions are FP64 in every mode.
+template <int D, typename R> struct PDev {
+    static constexpr int NV = D == 2 ? 4 : 6;
+    static constexpr int NF = D * D;
+    double *x[3];
+    R *v[3];
+    R *sig[6];
+    R *F[9];
+    R *eps[6];
+    R *epsq, *epsk, *epsv;
+    R *m, *vol0, *vol;
+    uint32_t *mat, *orig;
+};
+
+template <typename R> struct GDev {
+    using T4 = typename Vec<R>::T4;
+    AxisC<R> ax[3];
+    int nnx, nny, nnz;
+    T4 *acc0;   // (m, px, py, pz)  P2G / DM2 accumulator
+    T4 *acc1;   // (fx, fy, fz, 0)  P2G force accumulator
+    T4 *gvT;    // vsT
+    T4 *gas;    // as
+    T4 *gvs;    // vs (PIC / va = :v)
+    T4 *gdu;    // Δus
+    const uint8_t *bcmask;  // bit d: velocity component d fixed
+    const T4 *bcval;        // fixed values (NULL when all zero)
+    const Mat<R> *mat;
+    int *err;
+    uint8_t *bflag;         // per node block: 1 if some particle window touched it
+    int nbx, nby, nbz;      // node blocks per axis (blocks of BX x BY x BZ nodes)
+};
+
+// Node blocks: 4 (x) x 8 (y) x 4 (z) nodes in 3D, 16 (x) x 8 (y) in 2D; one
+// 128-thread CTA per block in the node passes, y fastest (128-byte rows).
+template <int D> struct Blk {
+    static constexpr int BX = D == 3 ? 4 : 16, BY = 8, BZ = D == 3 ? 4 : 1;
+    static constexpr int NT = BX * BY * BZ;
+};
+
+// Flag the node blocks covered by a particle's 3^D window.
+template <int D, typename R>
+__device__ __forceinline__ void mark_blocks(const GDev<R> &g, const AxisW<R> *w) {
+    using B = Blk<D>;
+    int x0 = clampi(w[0].base, 0, g.nnx - 1) / B::BX, x1 = clampi(w[0].base + 2, 0, g.nnx - 1) / B::BX;
+    int y0 = clampi(w[1].base, 0, g.nny - 1) / B::BY, y1 = clampi(w[1].base + 2, 0, g.nny - 1) / B::BY;
+    int z0 = 0, z1 = 0;
+    if (D == 3) { z0 = clampi(w[2].base, 0, g.nnz - 1) / B::BZ; z1 = clampi(w[2].base + 2, 0, g.nnz - 1) / B::BZ; }
+    for (int bz = z0; bz <= z1; ++bz)
+        for (int bx = x0; bx <= x1; ++bx)
+            for (int by = y0; by <= y1; ++by) {
+                int b = (bz * g.nbx + bx) * g.nby + by;
+                if (g.bflag[b] == 0) g.bflag[b] = 1;
+            }
+}
+
+// node of thread t in block b (returns -1 outside the grid)
+template <int D, typename R> __device__ __forceinline__ int block_node(const GDev<R> &g, int b, int t) {
+    using B = Blk<D>;
+    int by = b % g.nby;
+    int r = b / g.nby;
+    int bx = r % g.nbx;
+    int bz = r / g.nbx;
+    int ly = t % B::BY, lx = (t / B::BY) % B::BX, lz = t / (B::BY * B::BX);
+    int ix = bx * B::BX + lx, iy = by * B::BY + ly, iz = bz * B::BZ + lz;
+    if (ix >= g.nnx || iy >= g.nny || (D == 3 && iz >= g.nnz)) return -1;
+    return D == 2 ? ix * g.nny + iy : (iz * g.nnx + ix) * g.nny + iy;
+}
+
+struct StepParams {
+    double dt;
+    double G;        // gravity of the scatter (P2G) in this launch
+    double FLIP, PIC, zeta;
+    int plastic;     // Ti >= Te
+    int constitutive;
+    int va;          // 0 = :a, 1 = :v
+    int need_vs;     // DM gathers grid vs
+    int64_t np;
+};
+
+template <int D> __device__ __forceinline__ int node_id(int ix, int iy, int iz, int nnx, int nny) {
+    return D == 2 ? ix * nny + iy : (iz * nnx + ix) * nny + iy;
+}
+
+// Cell of a particle per axis (0-based), Julia rule: x and z by fld, y by cld
+// (utils_OS.jl:247-249, 380-383).
+template <int D, typename R>
+__device__ __forceinline__ void particle_cell(const double *xp, const GDev<R> &g, int *ci) {
+    ci[0] = q2i(jl_fld(xp[0] - g.ax[0].x1, g.ax[0].h));
+    ci[1] = q2i(jl_cld(xp[1] - g.ax[1].x1, g.ax[1].h)) - 1;
+    if (D == 3) ci[2] = q2i(jl_fld(xp[2] - g.ax[2].x1, g.ax[2].h));
+}
+
+// Weights of the 3^D window of a particle.  Returns false if the particle is
+// out of the grid (its contributions are then dropped and the flag raised).
+template <int D, typename R>
+__device__ __forceinline__ bool particle_weights(const double *xp, const GDev<R> &g, AxisW<R> *w) {
+    int ci[3];
+    particle_cell<D, R>(xp, g, ci);
+    bool bad = false;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        int c = ci[a];
+        if (c < 0 || c >= g.ax[a].nc) { bad = true; c = clampi(c, 0, g.ax[a].nc - 1); }
+        if (axis_weights<R>(xp[a], c, g.ax[a], w[a])) bad = true;
+    }
+    if (bad) {
+#pragma unroll
+        for (int a = 0; a < D; ++a)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = R(0); w[a].dN[k] = R(0); }
+    }
+    return !bad;
+}
+
+template <int D, typename R>
+__device__ __forceinline__ int window_node(const GDev<R> &g, const AxisW<R> *w, int a, int b, int c) {
+    int ix = clampi(w[0].base + a, 0, g.nnx - 1);
+    int iy = clampi(w[1].base + b, 0, g.nny - 1);
+    int iz = D == 3 ? clampi(w[2].base + c, 0, g.nnz - 1) : 0;
+    return node_id<D>(ix, iy, iz, g.nnx, g.nny);
+}
+
+// ---------------------------------------------------------------------------
+// P2G scatter of one particle (P2G_OS!, utils_OS.jl:424-496): nodal mass,
+// momentum and force; gravity on the last axis.  Nodes with N == 0 are skipped
+// like the reference's `if Ni ≠ 0`.
+// ---------------------------------------------------------------------------
+template <int D, typename R>
+__device__ __forceinline__ void p2g_scatter(const GDev<R> &g, const AxisW<R> *w, R m, R vol,
+                                            const R *v, const R *s, R G) {
+    mark_blocks<D, R>(g, w);
+    R p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : R(0)};
+    constexpr int NC = D == 3 ? 3 : 1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                R Nz = D == 3 ? w[2].N[c] : R(1);
+                R N = D == 3 ? w[0].N[a] * w[1].N[b] * Nz : w[0].N[a] * w[1].N[b];
+                if (N == R(0)) continue;
+                int n = window_node<D, R>(g, w, a, b, c);
+                R NiM = m * N;
+                if (D == 2) {
+                    R gx = w[0].dN[a] * w[1].N[b];
+                    R gy = w[1].dN[b] * w[0].N[a];
+                    R fx = -vol * (gx * s[0] + gy * s[3]);
+                    R fy = -vol * (gy * s[1] + gx * s[3]) + NiM * G;
+                    red_add4(&g.acc0[n], NiM, N * p[0], N * p[1], R(0));
+                    red_add4(&g.acc1[n], fx, fy, R(0), R(0));
+                } else {
+                    R gx = w[0].dN[a] * w[1].N[b] * Nz;
+                    R gy = w[1].dN[b] * w[0].N[a] * Nz;
+                    R gz = w[2].dN[c] * w[0].N[a] * w[1].N[b];
+                    R fx = -vol * (gx * s[0] + gy * s[3] + gz * s[5]);
+                    R fy = -vol * (gy * s[1] + gx * s[3] + gz * s[4]);
+                    R fz = -vol * (gz * s[2] + gx * s[5] + gy * s[4]) + NiM * G;
+                    red_add4(&g.acc0[n], NiM, N * p[0], N * p[1], N * p[2]);
+                    red_add4(&g.acc1[n], fx, fy, fz, R(0));
+                }
+            }
+}
+
+template <int D, typename R>
+__device__ __forceinline__ void load_x(const PDev<D, R> &P, int64_t i, double *x) {
+    x[0] = P.x[0][i]; x[1] = P.x[1][i];
+    x[2] = D == 3 ? P.x[2][i] : 0.0;
+}
+
+// Standalone P2G (first step after an upload; per-stage checks).
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_p2g(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    double x[3];
+    load_x<D, R>(P, i, x);
+    AxisW<R> w[3];
+    if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
+    R v[3] = {P.v[0][i], P.v[1][i], D == 3 ? P.v[2][i] : R(0)};
+    R s[6];
+#pragma unroll
+    for (int k = 0; k < PDev<D, R>::NV; ++k) s[k] = P.sig[k][i];
+    p2g_scatter<D, R>(g, w, P.m[i], P.vol[i], v, s, (R)sp.G);
+}
+
+// ---------------------------------------------------------------------------
+// Grid solve: solvegrid_a_OS! (va = :a, utils_OS.jl:547-640) or solvegrid_OS!
+// (va = :v, utils_OS.jl:507-535, 650-687).  Clears momentum and force.
+// ---------------------------------------------------------------------------
+template <int D, typename R>
+__global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
+    if (g.bflag[blockIdx.x] == 0) return;
+    int i = block_node<D, R>(g, blockIdx.x, threadIdx.x);
+    if (i < 0) return;
+    using T4 = typename Vec<R>::T4;
+    T4 a0 = g.acc0[i];
+    T4 a1 = g.acc1[i];
+    if (a0.x == R(0) && a0.y == R(0) && a0.z == R(0) && a0.w == R(0) && a1.x == R(0) && a1.y == R(0) &&
+        a1.z == R(0)) {
+        // untouched node: every derived quantity is 0 (ms_denom = 0); the BC
+        // can only write its value, which is 0 unless bcval is present.
+        if (g.bcval == nullptr || g.bcmask[i] == 0) {
+            g.gvT[i] = mk4<R>(0, 0, 0, 0);
+            g.gas[i] = mk4<R>(0, 0, 0, 0);
+            if (sp.need_vs) g.gvs[i] = mk4<R>(0, 0, 0, 0);
+            return;
+        }
+    }
+    const R eps = sizeof(R) == 8 ? R(2.220446049250313e-16) : R(1.1920929e-7);
+    R m = a0.x;
+    R md = m < eps ? R(0) : R(1) / m;
+    R p[3] = {a0.y, a0.z, a0.w};
+    R f[3] = {a1.x, a1.y, a1.z};
+    uint8_t bm = g.bcmask[i];
+    R bv[3] = {R(0), R(0), R(0)};
+    if (g.bcval) { T4 b = g.bcval[i]; bv[0] = b.x; bv[1] = b.y; bv[2] = b.z; }
+    const R dt = (R)sp.dt;
+    R vs[3], vT[3], as[3];
+    R ss = R(0);
+#pragma unroll
+    for (int d = 0; d < D; ++d) ss += f[d] * f[d];
+    R damp = -(R)sp.zeta * sqrt(ss);
+    if (sp.va == 0) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            if (bm & (1 << d)) p[d] = bv[d];
+            vs[d] = p[d] * md;
+            R Fs = f[d] + damp * sgn(vs[d]);
+            vT[d] = vs[d] + Fs * dt * md;
+            as[d] = Fs * md;
+            if (bm & (1 << d)) { vT[d] = bv[d]; as[d] = bv[d]; }
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            vs[d] = p[d] * md;
+            R Fs = f[d] + damp * sgn(vs[d]);
+            vT[d] = (p[d] + Fs * dt) * md;
+            as[d] = R(0);
+            if (bm & (1 << d)) vT[d] = bv[d];
+        }
+    }
+    if (D == 2) { vs[2] = vT[2] = as[2] = R(0); }
+    g.gvT[i] = mk4<R>(vT[0], vT[1], vT[2], 0);
+    g.gas[i] = mk4<R>(as[0], as[1], as[2], 0);
+    if (sp.need_vs) g.gvs[i] = mk4<R>(vs[0], vs[1], vs[2], 0);
+    g.acc0[i] = mk4<R>(m, 0, 0, 0);
+    g.acc1[i] = mk4<R>(0, 0, 0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Double mapping: doublemapping1_a_OS! / doublemapping1_OS! (new particle
+// velocity from the grid) fused with doublemapping2_OS! (re-scatter of the
+// particle momentum with the same weights).  The position update of DM1 is
+// carried out by k_g2p, which gathers the same ΣN·vsT with the same weights.
+// ---------------------------------------------------------------------------
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_dmap(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    using T4 = typename Vec<R>::T4;
+    double x[3];
+    load_x<D, R>(P, i, x);
+    AxisW<R> w[3];
+    particle_weights<D, R>(x, g, w);   // out-of-grid particles get zero weights
+    R tT[3] = {0, 0, 0}, ta[3] = {0, 0, 0}, tv[3] = {0, 0, 0};
+    constexpr int NC = D == 3 ? 3 : 1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                R N = D == 3 ? w[0].N[a] * w[1].N[b] * w[2].N[c] : w[0].N[a] * w[1].N[b];
+                if (N == R(0)) continue;
+                int n = window_node<D, R>(g, w, a, b, c);
+                T4 vT = g.gvT[n];
+                tT[0] += N * vT.x; tT[1] += N * vT.y; tT[2] += N * vT.z;
+                if (sp.va == 0) {
+                    T4 as = g.gas[n];
+                    ta[0] += N * as.x; ta[1] += N * as.y; ta[2] += N * as.z;
+                }
+                if (sp.need_vs) {
+                    T4 vs = g.gvs[n];
+                    tv[0] += N * vs.x; tv[1] += N * vs.y; tv[2] += N * vs.z;
+                }
+            }
+    const R dt = (R)sp.dt, FLIP = (R)sp.FLIP, PIC = (R)sp.PIC;
+    R vn[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        R vo = P.v[d][i];
+        if (sp.va == 0) vn[d] = FLIP * vo + PIC * tv[d] + ta[d] * dt;
+        else vn[d] = FLIP * (vo + (tT[d] - tv[d])) + PIC * tT[d];
+        P.v[d][i] = vn[d];
+    }
+    R m = P.m[i];
+    R p[3] = {m * vn[0], m * vn[1], D == 3 ? m * vn[2] : R(0)};
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                R N = D == 3 ? w[0].N[a] * w[1].N[b] * w[2].N[c] : w[0].N[a] * w[1].N[b];
+                if (N == R(0)) continue;
+                int n = window_node<D, R>(g, w, a, b, c);
+                red_add4(&g.acc0[n], R(0), p[0] * N, p[1] * N, p[2] * N);
+            }
+}
+
+// doublemapping3_OS!, utils_OS.jl:968-1016: grid velocity from the re-mapped
+// momentum, BC, Δus = vs·ΔT.  Clears mass and momentum for the next P2G.
+template <int D, typename R>
+__global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
+    if (g.bflag[blockIdx.x] == 0) return;
+    __syncthreads();
+    if (threadIdx.x == 0) g.bflag[blockIdx.x] = 0;   // re-armed by the next scatter
+    int i = block_node<D, R>(g, blockIdx.x, threadIdx.x);
+    if (i < 0) return;
+    using T4 = typename Vec<R>::T4;
+    T4 a0 = g.acc0[i];
+    uint8_t bm = g.bcmask[i];
+    if (a0.x == R(0) && a0.y == R(0) && a0.z == R(0) && a0.w == R(0) &&
+        (g.bcval == nullptr || bm == 0)) {
+        g.gdu[i] = mk4<R>(0, 0, 0, 0);
+        return;
+    }
+    const R eps = sizeof(R) == 8 ? R(2.220446049250313e-16) : R(1.1920929e-7);
+    R md = a0.x < eps ? R(0) : R(1) / a0.x;
+    R p[3] = {a0.y, a0.z, a0.w};
+    R bv[3] = {R(0), R(0), R(0)};
+    if (g.bcval) { T4 b = g.bcval[i]; bv[0] = b.x; bv[1] = b.y; bv[2] = b.z; }
+    const R dt = (R)sp.dt;
+    R du[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        R vs = p[d] * md;
+        if (bm & (1 << d)) vs = bv[d];
+        du[d] = vs * dt;
+    }
+    g.gdu[i] = mk4<R>(du[0], du[1], du[2], 0);
+    g.acc0[i] = mk4<R>(0, 0, 0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// G2P_OS! (utils_OS.jl:1025-1153) + the position update of DM1 + liE! +
+// dpP!/mcP!.  With FUSE, the next step's P2G scatters the updated particle
+// (resetmpstatus_OS! + P2G_OS! at the new position, gravity sp.G).
+// ---------------------------------------------------------------------------
+template <int D, typename R, bool FUSE>
+__global__ void __launch_bounds__(256) k_g2p(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    using T4 = typename Vec<R>::T4;
+    constexpr int NV = PDev<D, R>::NV, NF = PDev<D, R>::NF;
+    double x[3];
+    load_x<D, R>(P, i, x);
+    AxisW<R> w[3];
+    particle_weights<D, R>(x, g, w);
+    R tT[3] = {0, 0, 0};
+    R dF[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    constexpr int NC = D == 3 ? 3 : 1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                R Nz = D == 3 ? w[2].N[c] : R(1);
+                R N = D == 3 ? w[0].N[a] * w[1].N[b] * Nz : w[0].N[a] * w[1].N[b];
+                if (N == R(0)) continue;
+                int n = window_node<D, R>(g, w, a, b, c);
+                T4 vT = g.gvT[n];
+                T4 du = g.gdu[n];
+                tT[0] += N * vT.x; tT[1] += N * vT.y;
+                if (D == 3) tT[2] += N * vT.z;
+                if (D == 2) {
+                    R gx = w[0].dN[a] * w[1].N[b];
+                    R gy = w[1].dN[b] * w[0].N[a];
+                    dF[0] += du.x * gx; dF[1] += du.x * gy;
+                    dF[2] += du.y * gx; dF[3] += du.y * gy;
+                } else {
+                    R gx = w[0].dN[a] * w[1].N[b] * Nz;
+                    R gy = w[1].dN[b] * w[0].N[a] * Nz;
+                    R gz = w[2].dN[c] * w[0].N[a] * w[1].N[b];
+                    dF[0] += du.x * gx; dF[1] += du.x * gy; dF[2] += du.x * gz;
+                    dF[3] += du.y * gx; dF[4] += du.y * gy; dF[5] += du.y * gz;
+                    dF[6] += du.z * gx; dF[7] += du.z * gy; dF[8] += du.z * gz;
+                }
+            }
+    // position: ξ += ΔT·ΣN·vsT, accumulated in FP64
+#pragma unroll
+    for (int d = 0; d < D; ++d) x[d] += (double)tT[d] * sp.dt;
+    const R dT1 = R(1) / (R)sp.dt;
+    R de[6], ev;
+    if (D == 2) {
+        R exx = dF[0] * dT1, eyy = dF[3] * dT1, exy = R(0.5) * (dF[1] + dF[2]) * dT1;
+        ev = sqrt(exx * exx + eyy * eyy + R(2) * exy * exy);
+        de[0] = dF[0]; de[1] = dF[3]; de[2] = R(0); de[3] = dF[1] + dF[2];
+    } else {
+        R exx = dF[0] * dT1, eyy = dF[4] * dT1, ezz = dF[8] * dT1;
+        R exy = R(0.5) * (dF[1] + dF[3]) * dT1, eyz = R(0.5) * (dF[5] + dF[7]) * dT1,
+          exz = R(0.5) * (dF[2] + dF[6]) * dT1;
+        ev = sqrt(exx * exx + eyy * eyy + ezz * ezz + R(2) * (exy * exy + eyz * eyz + exz * exz));
+        de[0] = dF[0]; de[1] = dF[4]; de[2] = dF[8];
+        de[3] = dF[1] + dF[3]; de[4] = dF[5] + dF[7]; de[5] = dF[2] + dF[6];
+    }
+    // strain
+    if (D == 2) {
+        P.eps[0][i] += de[0]; P.eps[1][i] += de[1]; P.eps[3][i] += de[3];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) P.eps[k][i] += de[k];
+    }
+    P.epsv[i] = ev;
+    // F <- (I + ΔF) F; J = det F in FP64; Ω = J Ω0
+    R f[9], fn[9];
+#pragma unroll
+    for (int k = 0; k < NF; ++k) f[k] = P.F[k][i];
+    double J;
+    if (D == 2) {
+        fn[0] = (dF[0] + R(1)) * f[0] + dF[1] * f[2];
+        fn[1] = (dF[0] + R(1)) * f[1] + dF[1] * f[3];
+        fn[2] = (dF[3] + R(1)) * f[2] + dF[2] * f[0];
+        fn[3] = (dF[3] + R(1)) * f[3] + dF[2] * f[1];
+        J = (double)fn[0] * (double)fn[3] - (double)fn[1] * (double)fn[2];
+    } else {
+        fn[0] = (dF[0] + R(1)) * f[0] + dF[1] * f[3] + dF[2] * f[6];
+        fn[1] = (dF[0] + R(1)) * f[1] + dF[1] * f[4] + dF[2] * f[7];
+        fn[2] = (dF[0] + R(1)) * f[2] + dF[1] * f[5] + dF[2] * f[8];
+        fn[3] = (dF[4] + R(1)) * f[3] + dF[3] * f[0] + dF[5] * f[6];
+        fn[4] = (dF[4] + R(1)) * f[4] + dF[3] * f[1] + dF[5] * f[7];
+        fn[5] = (dF[4] + R(1)) * f[5] + dF[3] * f[2] + dF[5] * f[8];
+        fn[6] = (dF[8] + R(1)) * f[6] + dF[7] * f[3] + dF[6] * f[0];
+        fn[7] = (dF[8] + R(1)) * f[7] + dF[7] * f[4] + dF[6] * f[1];
+        fn[8] = (dF[8] + R(1)) * f[8] + dF[7] * f[5] + dF[6] * f[2];
+        double g0 = fn[0], g1 = fn[1], g2 = fn[2], g3 = fn[3], g4 = fn[4], g5 = fn[5], g6 = fn[6],
+               g7 = fn[7], g8 = fn[8];
+        J = g0 * g4 * g8 + g1 * g5 * g6 + g2 * g3 * g7 - g6 * g4 * g2 - g7 * g5 * g0 - g8 * g3 * g1;
+    }
+#pragma unroll
+    for (int k = 0; k < NF; ++k) P.F[k][i] = fn[k];
+    R vol = (R)(J * (double)P.vol0[i]);
+    P.vol[i] = vol;
+    // stress: liE! then dpP! / mcP! (OS_MUSL.jl:82-96)
+    const Mat<R> M = g.mat[P.mat[i]];
+    R s[6], srot[6];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) s[k] = P.sig[k][i];
+    lin_elastic<D, R>(s, dF, de, M, srot);
+    R eq = P.epsq[i], ek = P.epsk[i];
+    if (sp.plastic) {
+        if (sp.constitutive == 1) {
+            drucker_prager<D, R>(s, eq, ek, M);
+            P.epsq[i] = eq; P.epsk[i] = ek;
+        } else if (sp.constitutive == 2 && D == 2) {
+            mohr_coulomb_2d<R>(s, eq, ek, M);
+            P.epsq[i] = eq; P.epsk[i] = ek;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NV; ++k) P.sig[k][i] = s[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) P.x[d][i] = x[d];
+    bool bad = !(J > 0.0);
+    bool nan = !isfinite(x[0]) || !isfinite(x[1]) || !isfinite((double)s[0]) || !isfinite((double)s[1]);
+    if (bad) atomicOr(g.err, ERR_J);
+    if (nan) atomicOr(g.err, ERR_NAN);
+    if (FUSE) {
+        if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
+        R v[3] = {P.v[0][i], P.v[1][i], D == 3 ? P.v[2][i] : R(0)};
+        p2g_scatter<D, R>(g, w, P.m[i], vol, v, s, (R)sp.G);
+    }
+}
+
+// p2c of the current positions, 1-based, in the original particle order.
+template <int D, typename R>
+__global__ void k_p2c(PDev<D, R> P, GDev<R> g, int64_t np, int64_t *out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    double xp[3];
+    load_x<D, R>(P, i, xp);
+    // p2c = cld(y - y1, dy) + fld(z - z1, dz)*ncy*ncx + fld(x - x1, dx)*ncy
+    double cy = jl_cld(xp[1] - g.ax[1].x1, g.ax[1].h);
+    double cx = jl_fld(xp[0] - g.ax[0].x1, g.ax[0].h);
+    double v;
+    if (D == 2) v = cy + cx * (double)g.ax[1].nc;
+    else {
+        double cz = jl_fld(xp[2] - g.ax[2].x1, g.ax[2].h);
+        v = cy + cz * (double)g.ax[1].nc * (double)g.ax[0].nc + cx * (double)g.ax[1].nc;
+    }
+    int64_t r = (v >= -9.0e18 && v <= 9.0e18) ? (int64_t)trunc(v) : (int64_t)(-1);
+    out[P.orig[i]] = r;
+}
+
+}  // namespace mpm

@@ -1,0 +1,234 @@
+"""Host driver: the reference's entry point and device boundary over the C ABI.
+
+``materialpointsolver(args, grid, mp, attr, bc)`` mirrors ``materialpointsolver!``
+(src/MaterialPointSolver.jl:61-76) and ``submit_work!`` (src/solver.jl:37-131)
+for ``args.device == "B200"``: upload once (host2device), advance
+``while Ti < Ttol`` with the step workflow, download the fields device2host!
+copies, free the device.  The per-step workflow is ``procedure`` (the
+``procedure!`` of src/solvers/OS_MUSL.jl:12-102); the driver hands the device
+runs of consecutive steps so the host is not in the loop of every step.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _lib
+from .types import Grid3D
+
+
+def _view(a, typ=None):
+    v = _lib.View()
+    if a is None:
+        v.ptr = None
+        return v
+    if not (a.flags["F_CONTIGUOUS"] or a.ndim == 1):
+        raise ValueError("host arrays must be column-major (Fortran order)")
+    t = {np.dtype(np.float64): _lib.T_F64, np.dtype(np.float32): _lib.T_F32,
+         np.dtype(np.int64): _lib.T_I64, np.dtype(np.int32): _lib.T_I32}[a.dtype]
+    v.ptr = a.ctypes.data
+    v.type = t
+    v.ld = a.shape[0]
+    return v
+
+
+def host_views(grid, mp, attr, bc):
+    """Views of the reference structs' arrays, in the library's layout terms."""
+    hv = _lib.HostViews()
+    for name in ("xi", "vs", "sig", "eps", "epsq", "epsk", "epsv", "Omega", "Omega0", "rho", "rho0", "F",
+                 "ms", "sigm", "p2c"):
+        setattr(hv, name, _view(getattr(mp, name)))
+    hv.nid = _view(attr.nid)
+    for name in ("Ks", "Gs", "c", "phi", "psi", "sigt", "Hp", "cr"):
+        setattr(hv, name, _view(getattr(attr, name)))
+    hv.vx_idx, hv.vx_val = _view(bc.vx_s_idx), _view(bc.vx_s_val)
+    hv.vy_idx, hv.vy_val = _view(bc.vy_s_idx), _view(bc.vy_s_val)
+    if grid.dim == 3:
+        hv.vz_idx, hv.vz_val = _view(bc.vz_s_idx), _view(bc.vz_s_val)
+    return hv
+
+
+def make_desc(args, grid, mp, attr, device=0):
+    d = _lib.Desc()
+    d.abi_version = _lib.ABI_VERSION
+    d.dim = grid.dim
+    d.precision = _lib.PREC_FP64 if getattr(args, "gpu_precision", "mixed") == "fp64" else _lib.PREC_MIXED
+    d.device = device
+    d.np = mp.np
+    d.nmat = len(attr.Es)
+    d.nnx, d.nny = grid.nnx, grid.nny
+    d.nnz = grid.nnz if grid.dim == 3 else 1
+    d.x1, d.y1, d.dx, d.dy = grid.x1, grid.y1, grid.dx, grid.dy
+    d.z1 = grid.z1 if grid.dim == 3 else 0.0
+    d.dz = grid.dz if grid.dim == 3 else 1.0
+    d.lpx, d.lpy = mp.dx, mp.dy
+    d.lpz = mp.dz if grid.dim == 3 else 1.0
+    d.constitutive = {"linearelastic": 0, "druckerprager": 1, "mohrcoulomb": 2}.get(args.constitutive, -1)
+    d.va = 0 if args.va == "a" else 1
+    d.mvl = int(args.MVL)
+    d.mc3d = 1 if getattr(args, "mc3d", "literal") == "restated" else 0
+    d.FLIP, d.PIC, d.zeta_s, d.gravity, d.Te = args.FLIP, args.PIC, args.zeta_s, args.gravity, args.Te
+    d.time_f32 = 1 if args.precision == "FP32" else 0
+    d.sort_every = getattr(args, "sort_every", 0)
+    return d
+
+
+class DeviceModel:
+    """Device-resident model: the B200 counterpart of the (dev_grid, dev_mp,
+    dev_attr, dev_bc) tuple host2device returns."""
+
+    def __init__(self, args, grid, mp, attr, bc, device=0):
+        L = _lib.lib()
+        self.args, self.grid, self.mp, self.attr, self.bc = args, grid, mp, attr, bc
+        self.desc = make_desc(args, grid, mp, attr, device)
+        h = C.c_void_p()
+        _lib.check(L.mpm_create(C.byref(self.desc), C.byref(h)))
+        self.h = h
+        self.upload()
+
+    # host2device (devicehelpfunc_cuda.jl:17-37)
+    def upload(self):
+        hv = host_views(self.grid, self.mp, self.attr, self.bc)
+        _lib.check(_lib.lib().mpm_upload(self.h, C.byref(hv)), self.h)
+
+    def step(self, dt, Ti, nsteps=1):
+        out = C.c_double()
+        _lib.check(_lib.lib().mpm_step(self.h, dt, Ti, nsteps, C.byref(out)), self.h)
+        return out.value
+
+    def step_async(self, dt, Ti, nsteps=1):
+        _lib.check(_lib.lib().mpm_step_async(self.h, dt, Ti, nsteps), self.h)
+
+    def sync(self):
+        _lib.check(_lib.lib().mpm_sync(self.h), self.h)
+
+    # device2host! (devicehelpfunc_cuda.jl:39-69)
+    def download(self, mask=_lib.F_REFERENCE, mp=None):
+        mp = mp if mp is not None else self.mp
+        hv = host_views(self.grid, mp, self.attr, self.bc)
+        _lib.check(_lib.lib().mpm_download(self.h, C.byref(hv), mask), self.h)
+
+    def p2c(self):
+        out = np.zeros(self.mp.np, np.int64)
+        _lib.check(_lib.lib().mpm_compute_p2c(self.h, out.ctypes.data_as(C.POINTER(C.c_int64))), self.h)
+        return out
+
+    def order(self):
+        out = np.zeros(self.mp.np, np.int64)
+        _lib.check(_lib.lib().mpm_download_order(self.h, out.ctypes.data_as(C.POINTER(C.c_int64))), self.h)
+        return out
+
+    def sort(self):
+        _lib.check(_lib.lib().mpm_sort(self.h), self.h)
+
+    def run_stages(self, dt, Ti, mask):
+        _lib.check(_lib.lib().mpm_run_stages(self.h, dt, Ti, mask), self.h)
+
+    def grid_field(self, field):
+        D = self.grid.dim
+        n = self.grid.ni * (1 if field == 0 else D)
+        out = np.zeros(n, np.float64)
+        _lib.check(_lib.lib().mpm_download_grid(self.h, field, out.ctypes.data_as(C.POINTER(C.c_double))),
+                   self.h)
+        return out if field == 0 else out.reshape((self.grid.ni, D), order="F")
+
+    def stats(self):
+        s = _lib.Stats()
+        _lib.check(_lib.lib().mpm_get_stats(self.h, C.byref(s)), self.h)
+        return s
+
+    def set_profiling(self, on=True):
+        _lib.check(_lib.lib().mpm_set_profiling(self.h, 1 if on else 0), self.h)
+
+    def kernel_times(self):
+        cap = 32
+        names = (C.c_char_p * cap)()
+        ms = (C.c_double * cap)()
+        nl = (C.c_int64 * cap)()
+        cnt = C.c_int32()
+        _lib.check(_lib.lib().mpm_get_kernel_times(self.h, names, ms, nl, cap, C.byref(cnt)), self.h)
+        return {names[i].decode(): (ms[i], nl[i]) for i in range(min(cnt.value, cap))}
+
+    # clean_device! (devicehelpfunc_cuda.jl:71-100)
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().mpm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def host2device(args, grid, mp, attr, bc, device=0):
+    return DeviceModel(args, grid, mp, attr, bc, device)
+
+
+def device2host(args, mp, dev, verbose=False):
+    dev.download(_lib.F_REFERENCE, mp)
+    if verbose:
+        print("downloading from :B200 -> host")
+
+
+def clean_device(dev):
+    dev.close()
+
+
+def time_sequence(args, Ti0=0.0):
+    """Ti values of submit_work!'s loop (src/solver.jl:118-125): `while Ti < Ttol;
+    …; Ti += ΔT` with Ti in the model's float type T2."""
+    f32 = args.precision == "FP32"
+    T = np.float32 if f32 else np.float64
+    Ti, dt, Ttol = T(Ti0), T(args.dT), T(args.Ttol)
+    n = 0
+    while Ti < Ttol:
+        Ti = T(Ti + dt)
+        n += 1
+    return n
+
+
+def procedure(args, dev, dT, Ti):
+    """One step, the B200 counterpart of procedure!(…, Val(:OS), Val(:MUSL), Val(va))."""
+    dev.step(dT, Ti, 1)
+
+
+def materialpointsolver(args, grid, mp, attr, bc, workflow=None, device=0, verbose=False):
+    """Entry point mirroring materialpointsolver! (src/MaterialPointSolver.jl:61-76).
+
+    ``workflow=None`` runs the library's step for all steps in one device call;
+    a callable ``workflow(args, dev, dT, Ti)`` is called once per step instead,
+    like the reference's ``workflow`` keyword."""
+    if args.device != "B200":
+        raise ValueError("this package provides the :B200 device backend (args.device = 'B200')")
+    if args.coupling != "OS" or args.scheme != "MUSL":
+        raise NotImplementedError("only the one-phase MUSL scheme is provided")
+    if args.basis != "uGIMP":
+        raise NotImplementedError("only the uGIMP basis is provided")
+    if args.hdf5:
+        raise NotImplementedError("HDF5 snapshots are not provided by this backend")
+    dev = host2device(args, grid, mp, attr, bc, device)
+    try:
+        mp.p2c[:] = dev.p2c().astype(mp.p2c.dtype)   # initmpstatus! (src/solver.jl:45)
+        nsteps = time_sequence(args)
+        args.start_time = time.time()
+        if workflow is None:
+            Ti = dev.step(args.dT, 0.0, nsteps) if nsteps else 0.0
+        else:
+            T = np.float32 if args.precision == "FP32" else np.float64
+            Ti = T(0.0)
+            for _ in range(nsteps):
+                workflow(args, dev, args.dT, float(Ti))
+                Ti = T(Ti + T(args.dT))
+        args.end_time = time.time()
+        args.iter_num += nsteps
+        device2host(args, mp, dev, verbose=verbose)
+    finally:
+        clean_device(dev)
+    if verbose:
+        dtw = args.end_time - args.start_time
+        print(f"wall time {dtw:.3f} s, {nsteps} iterations, {nsteps / max(dtw, 1e-12):.3e} it/s")
+    return None

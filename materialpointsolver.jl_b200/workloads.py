@@ -1,0 +1,146 @@
+"""Seeded synthetic inputs for the benchmark configurations.
+
+The reference publishes no dataset for this path; these builders produce the
+granular column-collapse and slope inputs with the sizes, material constants
+and boundary conditions the configurations name, through the same host
+constructors a reference user calls (UserArgs*, UserGrid*, UserParticle*,
+UserProperty, UserVBoundary*).  Positions are a regular lattice of lp = h/2
+(2 particles per cell per axis) with a seeded uniform jitter.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .types import (UserArgs2D, UserArgs3D, UserGrid2D, UserGrid3D, UserParticle2D,
+                    UserParticle3D, UserProperty, UserVBoundary2D, UserVBoundary3D,
+                    jl_range, meshbuilder)
+
+
+def elastic_constants(E, nu):
+    K = E / (3.0 * (1.0 - 2.0 * nu))
+    G = E / (2.0 * (1.0 + nu))
+    return K, G
+
+
+def cfl_dt(h, K, G, rho, cfl=0.2):
+    """Δt = CFL·h / c_p with the P-wave speed c_p = sqrt((K + 4G/3)/ρ)."""
+    return cfl * h / math.sqrt((K + 4.0 * G / 3.0) / rho)
+
+
+class Case:
+    """A ready-to-run set of reference-style structs plus run metadata."""
+
+    def __init__(self, name, args, grid, mp, attr, bc, dt, nsteps_full, meta):
+        self.name, self.args, self.grid, self.mp, self.attr, self.bc = name, args, grid, mp, attr, bc
+        self.dt = dt
+        self.nsteps_full = nsteps_full
+        self.meta = meta
+
+
+def column_collapse_2d(*, h=0.005, ppc=2, seed=1001, jitter=0.1, width=0.2, height=0.1,
+                       domain=(0.6, 0.15), pad=2, precision="FP64", constitutive="druckerprager",
+                       E=0.84e6, nu=0.3, rho=2650.0, phi_deg=19.8, c=0.0, psi_deg=0.0,
+                       gravity=-9.81, Ttol=1.0, cfl=0.2, gpu_precision="mixed", project_path="/tmp",
+                       **extra):
+    """2D granular column collapse (uGIMP, plane strain).  Defaults: domain
+    0.6 x 0.15 m, h = 5 mm, 2x2 particles per cell in a 0.2 x 0.1 m column
+    (3 200 particles), DP with friction 19.8°, cohesion 0, dilation 0, fixed
+    left wall, free-slip floor, CFL 0.2, 1 s.  The grid carries `pad` extra
+    cells on every side so no particle's stencil leaves it."""
+    K, G = elastic_constants(E, nu)
+    dt = cfl_dt(h, K, G, rho, cfl)
+    lp = h / ppc
+    rng = np.random.Generator(np.random.PCG64(seed))
+    xs = jl_range(lp / 2, lp, width - lp / 2)
+    ys = jl_range(lp / 2, lp, height - lp / 2)
+    pts = meshbuilder(xs, ys)
+    pts = pts + rng.uniform(-jitter * h, jitter * h, size=pts.shape)
+    npart = pts.shape[0]
+    akw = dict(Ttol=Ttol, Te=0, ΔT=dt, FLIP=1, PIC=0, constitutive=constitutive, basis="uGIMP",
+               device="B200", coupling="OS", scheme="MUSL", va="a", gravity=gravity, ζs=0,
+               project_name="column2d", project_path=project_path, ϵ=precision,
+               gpu_precision=gpu_precision, make_project_dir=False)
+    akw.update(extra)
+    args = UserArgs2D(**akw)
+    grid = UserGrid2D(ϵ=precision, x1=-pad * h, x2=domain[0] + pad * h, y1=-pad * h,
+                      y2=domain[1] + pad * h, dx=h, dy=h, NIC=9)
+    mp = UserParticle2D(ϵ=precision, NIC=9, dx=lp, dy=lp, ξ=pts, ρs=np.full(npart, rho))
+    attr = UserProperty(ϵ=precision, nid=np.ones(npart, np.int64), ν=[nu], Es=[E], Gs=[G], Ks=[K],
+                        σt=[0.0], ϕ=[math.radians(phi_deg)], ϕr=[0.0], ψ=[math.radians(psi_deg)],
+                        c=[c], cr=[0.0], Hp=[0.0])
+    gx = grid.xi[:, 0]
+    gy = grid.xi[:, 1]
+    eps = 1e-9 * h
+    left = gx <= 0.0 + eps
+    right = gx >= domain[0] - eps
+    floor = gy <= 0.0 + eps
+    vx_idx = (left | right).astype(np.int64)
+    vy_idx = (left | floor).astype(np.int64)
+    bc = UserVBoundary2D(ϵ=precision, vx_s_idx=vx_idx, vx_s_val=np.zeros(grid.ni),
+                         vy_s_idx=vy_idx, vy_s_val=np.zeros(grid.ni))
+    nsteps = int(math.ceil(Ttol / dt))
+    return Case("column_collapse_2d", args, grid, mp, attr, bc, dt, nsteps,
+                dict(np=npart, h=h, K=K, G=G, seed=seed))
+
+
+def column_collapse_3d(*, h=0.005, ppc=2, seed=1002, jitter=0.1, column=(0.5, 0.2, 0.4),
+                       domain=(1.2, 0.4, 0.6), pad=2, precision="FP64", constitutive="mohrcoulomb",
+                       E=1.0e6, nu=0.3, rho=2650.0, phi_deg=30.0, c=0.0, psi_deg=0.0, gravity=-9.81,
+                       Ttol=1.0, cfl=0.2, gpu_precision="mixed", mc3d="literal", project_path="/tmp",
+                       **extra):
+    """3D granular column collapse.  Defaults: domain 1.2 x 0.4 x 0.6 m
+    (z up), h = 5 mm, 2x2x2 particles per cell in a 0.5 x 0.2 x 0.4 m column
+    (2 560 000 particles), Mohr-Coulomb φ = 30°, c = 0, ψ = 0, ρ = 2650,
+    E = 1 MPa, ν = 0.3, free-slip walls and floor, CFL 0.2, 1 s."""
+    K, G = elastic_constants(E, nu)
+    dt = cfl_dt(h, K, G, rho, cfl)
+    lp = h / ppc
+    rng = np.random.Generator(np.random.PCG64(seed))
+    xs = jl_range(lp / 2, lp, column[0] - lp / 2)
+    ys = jl_range(lp / 2, lp, column[1] - lp / 2)
+    zs = jl_range(lp / 2, lp, column[2] - lp / 2)
+    pts = meshbuilder(xs, ys, zs)
+    pts += rng.uniform(-jitter * h, jitter * h, size=pts.shape)
+    npart = pts.shape[0]
+    akw = dict(Ttol=Ttol, Te=0, ΔT=dt, FLIP=1, PIC=0, constitutive=constitutive, basis="uGIMP",
+               device="B200", coupling="OS", scheme="MUSL", va="a", gravity=gravity, ζs=0,
+               project_name="column3d", project_path=project_path, ϵ=precision,
+               gpu_precision=gpu_precision, mc3d=mc3d, make_project_dir=False)
+    akw.update(extra)
+    args = UserArgs3D(**akw)
+    grid = UserGrid3D(ϵ=precision, x1=-pad * h, x2=domain[0] + pad * h, y1=-pad * h,
+                      y2=domain[1] + pad * h, z1=-pad * h, z2=domain[2] + pad * h, dx=h, dy=h, dz=h,
+                      NIC=27)
+    mp = UserParticle3D(ϵ=precision, NIC=27, dx=lp, dy=lp, dz=lp, ξ=pts, ρs=np.full(npart, rho))
+    attr = UserProperty(ϵ=precision, nid=np.ones(npart, np.int64), ν=[nu], Es=[E], Gs=[G], Ks=[K],
+                        σt=[0.0], ϕ=[math.radians(phi_deg)], ϕr=[0.0], ψ=[math.radians(psi_deg)],
+                        c=[c], cr=[0.0], Hp=[0.0])
+    # boundary flags per node, built from the node coordinates without forming grid.ξ
+    nnx, nny, nnz = grid.nnx, grid.nny, grid.nnz
+    vx = grid._vx
+    vy = grid._vy
+    vz = grid._vz
+    eps = 1e-9 * h
+    bx = ((vx <= eps) | (vx >= domain[0] - eps))
+    by = ((vy <= eps) | (vy >= domain[1] - eps))
+    bz = (vz <= eps)
+    # node id = (iz*nnx + ix)*nny + iy
+    fx = np.broadcast_to(bx[None, :, None], (nnz, nnx, nny)).ravel().astype(np.int64)
+    fy = np.broadcast_to(by[None, None, :], (nnz, nnx, nny)).ravel().astype(np.int64)
+    fz = np.broadcast_to(bz[:, None, None], (nnz, nnx, nny)).ravel().astype(np.int64)
+    zeros = np.zeros(grid.ni)
+    bc = UserVBoundary3D(ϵ=precision, vx_s_idx=fx, vx_s_val=zeros, vy_s_idx=fy, vy_s_val=zeros,
+                         vz_s_idx=fz, vz_s_val=zeros)
+    nsteps = int(math.ceil(Ttol / dt))
+    return Case("column_collapse_3d", args, grid, mp, attr, bc, dt, nsteps,
+                dict(np=npart, h=h, K=K, G=G, seed=seed))
+
+
+def small_column_3d(**kw):
+    """A scaled-down 3D column (same physics and boundary conditions) that the
+    oracle steps in well under a second."""
+    base = dict(h=0.02, column=(0.2, 0.1, 0.16), domain=(0.4, 0.16, 0.24), seed=1002)
+    base.update(kw)
+    return column_collapse_3d(**base)
