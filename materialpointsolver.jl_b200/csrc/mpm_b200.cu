@@ -4,13 +4,14 @@
 // reference's column-major host arrays, the per-step launch sequence and the
 // cell sort.  Kernels live in mpm_kernels.cuh / mpm_sort.cuh.
 #include "../../include/mpm_b200.h"
-#include "mpm_sort.cuh"
+#include "mpm_tiled.cuh"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -66,7 +67,7 @@ struct mpm_handle {
     // particle arrays: two copies (A = current, B = sort target)
     void *pbuf[2] = {nullptr, nullptr};
     // grid
-    void *acc0 = nullptr, *acc1 = nullptr, *gvT = nullptr, *gas = nullptr, *gvs = nullptr, *gdu = nullptr;
+    void *acc = nullptr, *gat = nullptr, *gvs = nullptr;   // node records (see mpm_kernels.cuh)
     uint8_t *bcmask = nullptr;
     void *bcval = nullptr;
     uint8_t *bflag = nullptr;
@@ -76,8 +77,12 @@ struct mpm_handle {
     int *err = nullptr;
     // sort
     uint32_t *keys = nullptr, *cnt = nullptr, *off = nullptr, *bsum = nullptr, *big = nullptr, *nbig = nullptr;
-    uint2 *pairs = nullptr;
+    uint2 *pairs = nullptr, *pairs2 = nullptr;
     uint32_t nk = 0, big_cap = 0;
+    uint32_t *tiles = nullptr, *ntiles = nullptr;
+    uint32_t ntile_total = 0;
+    int nsm = 148;
+    bool tiled = false;
     SortGeom sg{};
     // staging
     void *stage = nullptr;
@@ -150,6 +155,7 @@ template <typename R> GDev<R> gdev_from(mpm_handle *h) {
         AxisC<R> &c = g.ax[a];
         c.x1 = x1[a];
         c.h = hh[a];
+        c.inv_h = 1.0 / hh[a];
         c.supp = hh[a] + 0.5 * lp[a];
         c.hr = (R)hh[a];
         c.lp = (R)lp[a];
@@ -165,12 +171,9 @@ template <typename R> GDev<R> gdev_from(mpm_handle *h) {
     g.nnx = (int)nn[0];
     g.nny = (int)nn[1];
     g.nnz = (int)nn[2];
-    g.acc0 = (T4 *)h->acc0;
-    g.acc1 = (T4 *)h->acc1;
-    g.gvT = (T4 *)h->gvT;
-    g.gas = (T4 *)h->gas;
+    g.acc = (Node8<R> *)h->acc;
+    g.gat = (Node8<R> *)h->gat;
     g.gvs = (T4 *)h->gvs;
-    g.gdu = (T4 *)h->gdu;
     g.bcmask = h->bcmask;
     g.bcval = (const T4 *)h->bcval;
     g.mat = (const Mat<R> *)h->mat;
@@ -337,12 +340,15 @@ template <int D, typename R> void do_sort(mpm_handle *h) {
     k_sort_scatter<D, R><<<cdiv(np, 256), 256, 0, st>>>(A, np, h->keys, h->off, h->cnt, h->pairs);
     k_sort_buckets<<<cdiv(h->nk, 256), 256, 0, st>>>(h->off, h->nk, h->pairs, h->big, h->nbig, h->big_cap, h->err);
     k_sort_big<<<64, 512, 0, st>>>(h->off, h->big, h->nbig, h->big_cap, h->pairs);
-    k_permute<D, R><<<cdiv(np, 256), 256, 0, st>>>(A, B, h->pairs, np);
+    CK(cudaMemsetAsync(h->ntiles, 0, 4, st));
+    k_tile_list<<<cdiv(h->ntile_total, 256), 256, 0, st>>>(h->off, h->ntile_total, Tile<D>::CPT, h->tiles, h->ntiles);
+    k_tile_transpose<Tile<D>::CPT><<<h->nsm * 8, Tile<D>::CPT, 0, st>>>(h->off, h->tiles, h->ntiles, h->pairs, h->pairs2);
+    k_permute<D, R><<<cdiv(np, 256), 256, 0, st>>>(A, B, h->pairs2, np);
     LAUNCH_CHECK();
     std::swap(h->pbuf[0], h->pbuf[1]);
     h->since_sort = 0;
     h->sorts_done++;
-    h->launches += 8;
+    h->launches += 10;
 }
 
 // ---- step --------------------------------------------------------------------------
@@ -400,8 +406,7 @@ template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, do
 template <int D, typename R> void standalone_p2g(mpm_handle *h, double Ti, Launcher &L) {
     const int64_t np = h->d.np;
     using T4 = typename Vec<R>::T4;
-    CK(cudaMemsetAsync(h->acc0, 0, h->ni * sizeof(T4), h->stream));
-    CK(cudaMemsetAsync(h->acc1, 0, h->ni * sizeof(T4), h->stream));
+    CK(cudaMemsetAsync(h->acc, 0, h->ni * sizeof(Node8<R>), h->stream));
     CK(cudaMemsetAsync(h->bflag, 0, (size_t)h->nbx * h->nby * h->nbz, h->stream));
     PDev<D, R> P = pdev_from<D, R>(h, 0);
     GDev<R> g = gdev_from<R>(h);
@@ -409,6 +414,31 @@ template <int D, typename R> void standalone_p2g(mpm_handle *h, double Ti, Launc
     if (np) L.run("p2g", [&] { k_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
     h->acc_valid = true;
     h->acc_Ti = Ti;
+}
+
+struct TiledCfg {
+    size_t smem_dm = 0, smem_g2p = 0;
+    int grid_dm = 0, grid_g2p = 0;
+    bool ready = false;
+};
+
+// dynamic shared memory and persistent grid size (CTAs per SM x SMs) of the tiled kernels
+template <int D, typename R> const TiledCfg &tiled_cfg(mpm_handle *h, int need_vs) {
+    static thread_local TiledCfg per[8][2];   // per device ordinal (mod 8) and need_vs
+    TiledCfg &cc = per[h->dev & 7][need_vs ? 1 : 0];
+    if (cc.ready) return cc;
+    using W = Win<D>;
+    cc.smem_dm = (size_t)(need_vs ? 9 : 6) * W::WN * sizeof(R);
+    cc.smem_g2p = (size_t)6 * W::WN * sizeof(R);
+    CK(cudaFuncSetAttribute(k_dmap_tile<D, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cc.smem_dm));
+    CK(cudaFuncSetAttribute(k_g2p_tile<D, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cc.smem_g2p));
+    int a = 0, b = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_dmap_tile<D, R>, 256, cc.smem_dm));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_g2p_tile<D, R>, 256, cc.smem_g2p));
+    cc.grid_dm = std::max(a, 1) * h->nsm;
+    cc.grid_g2p = std::max(b, 1) * h->nsm;
+    cc.ready = true;
+    return cc;
 }
 
 template <int D, typename R> void run_steps(mpm_handle *h, double dt, double Ti0, int64_t nsteps) {
@@ -431,9 +461,17 @@ template <int D, typename R> void run_steps(mpm_handle *h, double dt, double Ti0
         GDev<R> g = gdev_from<R>(h);
         StepParams sp = make_params<D, R>(h, dt, Ti, gravity_at(h->d, Tn));
         L.run("solve", [&] { k_solve<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-        if (np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
-        L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-        if (np) L.run("g2p_p2g", [&] { k_g2p<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        if (h->tiled) {
+            TileList tl{h->tiles, h->ntiles, h->off, h->sg};
+            const TiledCfg &c = tiled_cfg<D, R>(h, sp.need_vs);
+            if (np) L.run("dmap", [&] { k_dmap_tile<D, R><<<c.grid_dm, 256, c.smem_dm, h->stream>>>(P, g, sp, tl); });
+            L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+            if (np) L.run("g2p_p2g", [&] { k_g2p_tile<D, R><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl); });
+        } else {
+            if (np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+            L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+            if (np) L.run("g2p_p2g", [&] { k_g2p<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        }
         Ti = Tn;
         h->since_sort++;
         h->steps_done++;
@@ -628,10 +666,10 @@ template <int D, typename R> struct P2CAll {
     }
 };
 
-template <typename T4>
-__global__ void k_count_active(const T4 *acc0, int64_t ni, unsigned long long *out) {
+template <typename R>
+__global__ void k_count_active(const Node8<R> *acc, int64_t ni, unsigned long long *out) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long c = (i < ni && acc0[i].x > 0) ? 1ull : 0ull;
+    unsigned long long c = (i < ni && acc[i].a.x > 0) ? 1ull : 0ull;
     c = __reduce_add_sync(0xffffffffu, (unsigned)c);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
@@ -641,7 +679,7 @@ template <int D, typename R> struct CountActive {
         using T4 = typename Vec<R>::T4;
         unsigned long long *d = (unsigned long long *)h->bsum;   // scratch word
         CK(cudaMemsetAsync(d, 0, 8, h->stream));
-        k_count_active<T4><<<cdiv(h->ni, 256), 256, 0, h->stream>>>((const T4 *)h->acc0, h->ni, d);
+        k_count_active<R><<<cdiv(h->ni, 256), 256, 0, h->stream>>>((const Node8<R> *)h->acc, h->ni, d);
         LAUNCH_CHECK();
         unsigned long long v = 0;
         CK(cudaMemcpyAsync(&v, d, 8, cudaMemcpyDeviceToHost, h->stream));
@@ -683,17 +721,18 @@ template <int D, typename R> struct GridOut {
         using T4 = typename Vec<R>::T4;
         const int64_t ni = h->ni, nny = h->d.nny;
         std::vector<T4> a(ni);
-        void *src = nullptr;
-        switch (field) {
-            case 0: case 1: src = h->acc0; break;
-            case 2: src = h->acc1; break;
-            case 3: src = h->gvT; break;
-            case 4: src = h->gas; break;
-            case 5: src = h->gdu; break;
-            case 6: src = h->gvs; break;
-            default: throw Err{MPM_E_ARG, "grid field out of range"};
+        // field -> (record array, half): 0 mass, 1 momentum (acc.a), 2 force (acc.b),
+        // 3 vsT (gat.a), 4 as / 5 Δus (gat.b: as after the solve, Δus after DM3), 6 vs
+        if (field < 0 || field > 6) throw Err{MPM_E_ARG, "grid field out of range"};
+        if (field == 6) {
+            if (!h->gvs) throw Err{MPM_E_ARG, "grid vs is kept only with PIC != 0 or va = :v"};
+            CK(cudaMemcpy(a.data(), h->gvs, ni * sizeof(T4), cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<Node8<R>> rec(ni);
+            CK(cudaMemcpy(rec.data(), field <= 2 ? h->acc : h->gat, ni * sizeof(Node8<R>), cudaMemcpyDeviceToHost));
+            const bool second = field == 2 || field == 4 || field == 5;
+            for (int64_t r = 0; r < ni; ++r) a[r] = second ? rec[r].b : rec[r].a;
         }
-        CK(cudaMemcpy(a.data(), src, ni * sizeof(T4), cudaMemcpyDeviceToHost));
         for (int64_t r = 0; r < ni; ++r) {
             int64_t inode = r;
             if (D == 2) {
@@ -773,17 +812,11 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         size_t pb = pbuf_bytes(d->dim, h->fp64, d->np);
         h->pbuf[0] = dalloc(h, pb);
         h->pbuf[1] = dalloc(h, pb);
-        h->acc0 = dalloc(h, ni * T4);
-        h->acc1 = dalloc(h, ni * T4);
-        h->gvT = dalloc(h, ni * T4);
-        h->gas = dalloc(h, ni * T4);
-        h->gdu = dalloc(h, ni * T4);
+        h->acc = dalloc(h, ni * 2 * T4);
+        h->gat = dalloc(h, ni * 2 * T4);
         h->gvs = (d->PIC != 0.0 || d->va == MPM_VA_V) ? dalloc(h, ni * T4) : nullptr;
-        CK(cudaMemset(h->acc0, 0, ni * T4));
-        CK(cudaMemset(h->acc1, 0, ni * T4));
-        CK(cudaMemset(h->gvT, 0, ni * T4));
-        CK(cudaMemset(h->gas, 0, ni * T4));
-        CK(cudaMemset(h->gdu, 0, ni * T4));
+        CK(cudaMemset(h->acc, 0, ni * 2 * T4));
+        CK(cudaMemset(h->gat, 0, ni * 2 * T4));
         if (h->gvs) CK(cudaMemset(h->gvs, 0, ni * T4));
         h->bcmask = (uint8_t *)dalloc(h, ni);
         CK(cudaMemset(h->bcmask, 0, ni));
@@ -821,6 +854,17 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         h->big = (uint32_t *)dalloc(h, h->big_cap * 4);
         h->nbig = (uint32_t *)dalloc(h, 4);
         h->pairs = (uint2 *)dalloc(h, npa * 8);
+        h->pairs2 = (uint2 *)dalloc(h, npa * 8);
+        h->ntile_total = h->nk / (d->dim == 3 ? Tile<3>::CPT : Tile<2>::CPT);
+        h->tiles = (uint32_t *)dalloc(h, (size_t)h->ntile_total * 4);
+        h->ntiles = (uint32_t *)dalloc(h, 4);
+        CK(cudaMemset(h->ntiles, 0, 4));
+        CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, d->device));
+        // MPM_B200_TILED=1 selects the shared-memory tiled particle passes instead
+        // of the per-particle kernels (vector reductions into L2); both compute the
+        // same step.  The per-particle kernels are the faster ones on B200, where
+        // shared-memory float atomics are the tiled passes' limiter.
+        if (const char *e = getenv("MPM_B200_TILED")) h->tiled = (e[0] == '1');
         *out = h;
         return MPM_OK;
     } catch (const Err &e) {

@@ -67,6 +67,7 @@ template <typename R> __device__ __forceinline__ R sgn(R x) { return (R)((x > R(
 // ---------------------------------------------------------------------------
 template <typename R> struct AxisC {
     double x1, h;       // grid origin / spacing (FP64, for distances)
+    double inv_h;       // 1/h (FP64) for the fast cell index
     double supp;        // h + lp/2: candidate test |Δ| < supp (utils_OS.jl:220-221)
     R hr, lp, half_lp, h_m_hl, h_p_hl;   // h, lp, lp/2, h - lp/2, h + lp/2
     R inv4hl, invhl, invh;               // 1/(4 h lp), 1/(h lp), 1/h
@@ -74,7 +75,8 @@ template <typename R> struct AxisC {
 };
 
 // 1-D uGIMP weight and derivative.  FP64 mode evaluates the CPU (division)
-// form of uGIMPbasis; FP32 mode the reciprocal form of uGIMPbasisx/y/z.
+// form of uGIMPbasis; FP32 mode the reciprocal form of uGIMPbasisx/y/z, with
+// |Δ|/h also taken as |Δ|·(1/h).
 template <typename R> __device__ __forceinline__ void ugimp1(R d, const AxisC<R> &c, R &N, R &dN) {
     R a = fabs(d);
     N = R(0); dN = R(0);
@@ -96,7 +98,7 @@ template <typename R> __device__ __forceinline__ void ugimp1(R d, const AxisC<R>
             N = R(1) - ((R(4) * d * d + c.lp * c.lp) * c.inv4hl);
             dN = -R(8) * d * c.inv4hl;
         } else if (a < c.h_m_hl) {
-            N = R(1) - (a / c.hr);
+            N = R(1) - a * c.invh;
             dN = sgn(d) * -c.invh;
         } else if (a < c.h_p_hl) {
             R t = c.h_p_hl - a;
@@ -117,23 +119,62 @@ template <typename R> struct AxisW {
 
 template <typename R>
 __device__ __forceinline__ bool axis_weights(double xp, int ci, const AxisC<R> &c, AxisW<R> &w) {
-    double dlo = xp - (c.x1 + (double)(ci - 1) * c.h);
-    int base = (fabs(dlo) < c.supp) ? ci - 1 : ci;
+    // distances to nodes ci-1 .. ci+1 (or ci .. ci+2) from the offset to node ci
+    const double s = xp - (c.x1 + (double)ci * c.h);
+    const int lo = (fabs(s + c.h) < c.supp) ? 1 : 0;
+    const int base = ci - lo;
     bool oob = false;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        int j = base + k;
-        double d = xp - (c.x1 + (double)j * c.h);
+        const double d = s + (double)(lo - k) * c.h;
         R n, dn;
         ugimp1<R>((R)d, c, n, dn);
-        if (j < 0 || j >= c.nn) {
-            if (n != R(0)) oob = true;
-            n = R(0); dn = R(0);
-        }
         w.N[k] = n; w.dN[k] = dn;
     }
     w.base = base;
+    if (base < 0 || base + 2 >= c.nn) {
+        // Window reaches past the grid (rare).  A node outside the grid with
+        // weight is an error.  A weightless one past the far end is traded for
+        // the weightless node ci - 1, so that every valid window lies inside
+        // the grid and its nodes can be read without guards.
+        bool heavy = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            int j = base + k;
+            if ((j < 0 || j >= c.nn) && w.N[k] != R(0)) heavy = true;
+        }
+        if (heavy || base < 0) {
+            oob = true;
+        } else {   // lo == 0: node ci - 1 = base - 1 is outside the support
+            w.base = base - 1;
+            w.N[2] = w.N[1]; w.dN[2] = w.dN[1];
+            w.N[1] = w.N[0]; w.dN[1] = w.dN[0];
+            w.N[0] = R(0); w.dN[0] = R(0);
+            if (w.base < 0) oob = true;
+        }
+    }
     return oob;
+}
+
+// Cell index with Julia's fld (x, z) / cld - 1 (y) semantics.  Away from an
+// integer quotient, floor((x - x1) * (1/h)) is the exact answer (the FP64
+// quotient is within 1e-9 cell of the exact one for grids below ~1e6 cells per
+// axis); within 1e-9 of an integer the exact-remainder rule decides.
+template <typename R> __device__ __forceinline__ int cell_fld(double x, const AxisC<R> &c) {
+    const double a = x - c.x1;
+    const double t = a * c.inv_h;
+    const double q = floor(t);
+    const double fr = t - q;
+    if (fr > 1e-9 && fr < 1.0 - 1e-9 && fabs(q) < 1.0e9) return (int)q;
+    return q2i(jl_fld(a, c.h));
+}
+template <typename R> __device__ __forceinline__ int cell_cld_m1(double x, const AxisC<R> &c) {
+    const double a = x - c.x1;
+    const double t = a * c.inv_h;
+    const double q = floor(t);
+    const double fr = t - q;
+    if (fr > 1e-9 && fr < 1.0 - 1e-9 && fabs(q) < 1.0e9) return (int)q;   // ceil(t) - 1
+    return q2i(jl_cld(a, c.h)) - 1;
 }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }

@@ -15,8 +15,19 @@
 // force, k_dm3 clears mass and momentum), so the grid is zero again when the
 // next P2G scatters.  Particle weights are recomputed from positions in each
 // particle pass instead of being stored per particle.
+//
+// Node data are two records of one 32-byte sector each (FP32): the
+// accumulator {m, px, py, pz | fx, fy, fz, 0} and the gather record
+// {vsT, 0 | as, 0}, whose second half k_dm3 overwrites with Δus once the
+// double mapping has consumed `as`.  Every particle-node touch therefore
+// reads or reduces one sector.
 #pragma once
 #include "mpm_device.cuh"
+
+// resident CTAs of 256 threads per SM the particle passes are register-capped for
+#ifndef MPM_P_MINB
+#define MPM_P_MINB 4
+#endif
 
 namespace mpm {
 
@@ -34,16 +45,17 @@ template <int D, typename R> struct PDev {
     uint32_t *mat, *orig;
 };
 
+template <typename R> struct alignas(2 * sizeof(typename Vec<R>::T4)) Node8 {
+    typename Vec<R>::T4 a, b;
+};
+
 template <typename R> struct GDev {
     using T4 = typename Vec<R>::T4;
     AxisC<R> ax[3];
     int nnx, nny, nnz;
-    T4 *acc0;   // (m, px, py, pz)  P2G / DM2 accumulator
-    T4 *acc1;   // (fx, fy, fz, 0)  P2G force accumulator
-    T4 *gvT;    // vsT
-    T4 *gas;    // as
-    T4 *gvs;    // vs (PIC / va = :v)
-    T4 *gdu;    // Δus
+    Node8<R> *acc;   // a = (m, px, py, pz), b = (fx, fy, fz, 0): P2G / DM2 accumulator
+    Node8<R> *gat;   // a = (vsT, 0), b = (as, 0) after k_solve, (Δus, 0) after k_dm3
+    T4 *gvs;         // vs (PIC != 0 or va = :v)
     const uint8_t *bcmask;  // bit d: velocity component d fixed
     const T4 *bcval;        // fixed values (NULL when all zero)
     const Mat<R> *mat;
@@ -52,27 +64,67 @@ template <typename R> struct GDev {
     int nbx, nby, nbz;      // node blocks per axis (blocks of BX x BY x BZ nodes)
 };
 
+// streaming (evict-first) access to the particle arrays, which are touched
+// once per pass, so that the node records stay resident in L2
+template <typename T> __device__ __forceinline__ T ldcs(const T *p) { return __ldcs(p); }
+template <typename T> __device__ __forceinline__ void stcs(T *p, T v) { __stcs(p, v); }
+
 // Node blocks: 4 (x) x 8 (y) x 4 (z) nodes in 3D, 16 (x) x 8 (y) in 2D; one
-// 128-thread CTA per block in the node passes, y fastest (128-byte rows).
+// 128-thread CTA per block in the node passes, y fastest.
 template <int D> struct Blk {
     static constexpr int BX = D == 3 ? 4 : 16, BY = 8, BZ = D == 3 ? 4 : 1;
     static constexpr int NT = BX * BY * BZ;
 };
 
-// Flag the node blocks covered by a particle's 3^D window.
+template <int D, typename R> __device__ __forceinline__ void block_range(const GDev<R> &g, const AxisW<R> *w,
+                                                                        int *lo, int *hi) {
+    using B = Blk<D>;
+    const int nn[3] = {g.nnx, g.nny, g.nnz};
+    const int bs[3] = {B::BX, B::BY, B::BZ};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (a < D) {
+            lo[a] = clampi(w[a].base, 0, nn[a] - 1) / bs[a];
+            hi[a] = clampi(w[a].base + 2, 0, nn[a] - 1) / bs[a];
+        } else {
+            lo[a] = 0; hi[a] = 0;
+        }
+    }
+}
+
+// Flag the node blocks covered by the windows of the calling lanes.  The
+// active lanes of a warp (neighbouring particles after the cell sort) mark the
+// bounding box of their windows together; a box wider than 64 blocks (lanes
+// far apart) falls back to per-lane marking.
 template <int D, typename R>
 __device__ __forceinline__ void mark_blocks(const GDev<R> &g, const AxisW<R> *w) {
-    using B = Blk<D>;
-    int x0 = clampi(w[0].base, 0, g.nnx - 1) / B::BX, x1 = clampi(w[0].base + 2, 0, g.nnx - 1) / B::BX;
-    int y0 = clampi(w[1].base, 0, g.nny - 1) / B::BY, y1 = clampi(w[1].base + 2, 0, g.nny - 1) / B::BY;
-    int z0 = 0, z1 = 0;
-    if (D == 3) { z0 = clampi(w[2].base, 0, g.nnz - 1) / B::BZ; z1 = clampi(w[2].base + 2, 0, g.nnz - 1) / B::BZ; }
-    for (int bz = z0; bz <= z1; ++bz)
-        for (int bx = x0; bx <= x1; ++bx)
-            for (int by = y0; by <= y1; ++by) {
-                int b = (bz * g.nbx + bx) * g.nby + by;
-                if (g.bflag[b] == 0) g.bflag[b] = 1;
-            }
+    int lo[3], hi[3];
+    block_range<D, R>(g, w, lo, hi);
+    const unsigned mask = __activemask();
+    int blo[3], bhi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        blo[a] = __reduce_min_sync(mask, lo[a]);
+        bhi[a] = __reduce_max_sync(mask, hi[a]);
+    }
+    const int nx = bhi[0] - blo[0] + 1, ny = bhi[1] - blo[1] + 1, nz = bhi[2] - blo[2] + 1;
+    const int total = nx * ny * nz;
+    if (total <= 64) {
+        const int lane = threadIdx.x & 31;
+        const int rank = __popc(mask & ((1u << lane) - 1u)), cnt = __popc(mask);
+        for (int k = rank; k < total; k += cnt) {
+            int by = blo[1] + k % ny, r = k / ny, bx = blo[0] + r % nx, bz = blo[2] + r / nx;
+            int b = (bz * g.nbx + bx) * g.nby + by;
+            if (g.bflag[b] == 0) g.bflag[b] = 1;
+        }
+    } else {
+        for (int bz = lo[2]; bz <= hi[2]; ++bz)
+            for (int bx = lo[0]; bx <= hi[0]; ++bx)
+                for (int by = lo[1]; by <= hi[1]; ++by) {
+                    int b = (bz * g.nbx + bx) * g.nby + by;
+                    if (g.bflag[b] == 0) g.bflag[b] = 1;
+                }
+    }
 }
 
 // node of thread t in block b (returns -1 outside the grid)
@@ -107,9 +159,9 @@ template <int D> __device__ __forceinline__ int node_id(int ix, int iy, int iz, 
 // (utils_OS.jl:247-249, 380-383).
 template <int D, typename R>
 __device__ __forceinline__ void particle_cell(const double *xp, const GDev<R> &g, int *ci) {
-    ci[0] = q2i(jl_fld(xp[0] - g.ax[0].x1, g.ax[0].h));
-    ci[1] = q2i(jl_cld(xp[1] - g.ax[1].x1, g.ax[1].h)) - 1;
-    if (D == 3) ci[2] = q2i(jl_fld(xp[2] - g.ax[2].x1, g.ax[2].h));
+    ci[0] = cell_fld<R>(xp[0], g.ax[0]);
+    ci[1] = cell_cld_m1<R>(xp[1], g.ax[1]);
+    if (D == 3) ci[2] = cell_fld<R>(xp[2], g.ax[2]);
 }
 
 // Weights of the 3^D window of a particle.  Returns false if the particle is
@@ -125,21 +177,29 @@ __device__ __forceinline__ bool particle_weights(const double *xp, const GDev<R>
         if (c < 0 || c >= g.ax[a].nc) { bad = true; c = clampi(c, 0, g.ax[a].nc - 1); }
         if (axis_weights<R>(xp[a], c, g.ax[a], w[a])) bad = true;
     }
+    if (D == 2) w[2].base = 0;
     if (bad) {
+        // out-of-grid particle: no weight, and a window at the grid origin so
+        // that any address formed from it stays inside the node arrays
 #pragma unroll
-        for (int a = 0; a < D; ++a)
+        for (int a = 0; a < D; ++a) {
+            w[a].base = 0;
 #pragma unroll
             for (int k = 0; k < 3; ++k) { w[a].N[k] = R(0); w[a].dN[k] = R(0); }
+        }
     }
     return !bad;
 }
 
+// node index of the window corner; window node (a, b, c) is
+// n0 + a*nny + b + c*nnx*nny (3D) / n0 + a*nny + b (2D)
+template <int D, typename R> __device__ __forceinline__ int window_n0(const GDev<R> &g, const AxisW<R> *w) {
+    return D == 2 ? w[0].base * g.nny + w[1].base : (w[2].base * g.nnx + w[0].base) * g.nny + w[1].base;
+}
+
 template <int D, typename R>
 __device__ __forceinline__ int window_node(const GDev<R> &g, const AxisW<R> *w, int a, int b, int c) {
-    int ix = clampi(w[0].base + a, 0, g.nnx - 1);
-    int iy = clampi(w[1].base + b, 0, g.nny - 1);
-    int iz = D == 3 ? clampi(w[2].base + c, 0, g.nnz - 1) : 0;
-    return node_id<D>(ix, iy, iz, g.nnx, g.nny);
+    return window_n0<D, R>(g, w) + a * g.nny + b + (D == 3 ? c * g.nnx * g.nny : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -151,7 +211,9 @@ template <int D, typename R>
 __device__ __forceinline__ void p2g_scatter(const GDev<R> &g, const AxisW<R> *w, R m, R vol,
                                             const R *v, const R *s, R G) {
     mark_blocks<D, R>(g, w);
-    R p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : R(0)};
+    const R p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : R(0)};
+    const int n0 = window_n0<D, R>(g, w);
+    const int plane = g.nnx * g.nny;
     constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
     for (int c = 0; c < NC; ++c)
@@ -159,35 +221,38 @@ __device__ __forceinline__ void p2g_scatter(const GDev<R> &g, const AxisW<R> *w,
         for (int a = 0; a < 3; ++a)
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                R Nz = D == 3 ? w[2].N[c] : R(1);
-                R N = D == 3 ? w[0].N[a] * w[1].N[b] * Nz : w[0].N[a] * w[1].N[b];
-                if (N == R(0)) continue;
-                int n = window_node<D, R>(g, w, a, b, c);
-                R NiM = m * N;
+                const R Nz = D == 3 ? w[2].N[c] : R(1);
+                const R N = D == 3 ? w[0].N[a] * w[1].N[b] * Nz : w[0].N[a] * w[1].N[b];
+                Node8<R> *q = g.acc + (n0 + a * g.nny + b + c * plane);
+                const R NiM = m * N;
                 if (D == 2) {
-                    R gx = w[0].dN[a] * w[1].N[b];
-                    R gy = w[1].dN[b] * w[0].N[a];
-                    R fx = -vol * (gx * s[0] + gy * s[3]);
-                    R fy = -vol * (gy * s[1] + gx * s[3]) + NiM * G;
-                    red_add4(&g.acc0[n], NiM, N * p[0], N * p[1], R(0));
-                    red_add4(&g.acc1[n], fx, fy, R(0), R(0));
+                    const R gx = w[0].dN[a] * w[1].N[b];
+                    const R gy = w[1].dN[b] * w[0].N[a];
+                    const R fx = -vol * (gx * s[0] + gy * s[3]);
+                    const R fy = -vol * (gy * s[1] + gx * s[3]) + NiM * G;
+                    if (N != R(0)) {
+                        red_add4(&q->a, NiM, N * p[0], N * p[1], R(0));
+                        red_add4(&q->b, fx, fy, R(0), R(0));
+                    }
                 } else {
-                    R gx = w[0].dN[a] * w[1].N[b] * Nz;
-                    R gy = w[1].dN[b] * w[0].N[a] * Nz;
-                    R gz = w[2].dN[c] * w[0].N[a] * w[1].N[b];
-                    R fx = -vol * (gx * s[0] + gy * s[3] + gz * s[5]);
-                    R fy = -vol * (gy * s[1] + gx * s[3] + gz * s[4]);
-                    R fz = -vol * (gz * s[2] + gx * s[5] + gy * s[4]) + NiM * G;
-                    red_add4(&g.acc0[n], NiM, N * p[0], N * p[1], N * p[2]);
-                    red_add4(&g.acc1[n], fx, fy, fz, R(0));
+                    const R gx = w[0].dN[a] * w[1].N[b] * Nz;
+                    const R gy = w[1].dN[b] * w[0].N[a] * Nz;
+                    const R gz = w[2].dN[c] * w[0].N[a] * w[1].N[b];
+                    const R fx = -vol * (gx * s[0] + gy * s[3] + gz * s[5]);
+                    const R fy = -vol * (gy * s[1] + gx * s[3] + gz * s[4]);
+                    const R fz = -vol * (gz * s[2] + gx * s[5] + gy * s[4]) + NiM * G;
+                    if (N != R(0)) {
+                        red_add4(&q->a, NiM, N * p[0], N * p[1], N * p[2]);
+                        red_add4(&q->b, fx, fy, fz, R(0));
+                    }
                 }
             }
 }
 
 template <int D, typename R>
 __device__ __forceinline__ void load_x(const PDev<D, R> &P, int64_t i, double *x) {
-    x[0] = P.x[0][i]; x[1] = P.x[1][i];
-    x[2] = D == 3 ? P.x[2][i] : 0.0;
+    x[0] = ldcs(P.x[0] + i); x[1] = ldcs(P.x[1] + i);
+    x[2] = D == 3 ? ldcs(P.x[2] + i) : 0.0;
 }
 
 // Standalone P2G (first step after an upload; per-stage checks).
@@ -216,16 +281,18 @@ __global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
     int i = block_node<D, R>(g, blockIdx.x, threadIdx.x);
     if (i < 0) return;
     using T4 = typename Vec<R>::T4;
-    T4 a0 = g.acc0[i];
-    T4 a1 = g.acc1[i];
+    Node8<R> A = g.acc[i];
+    const T4 a0 = A.a, a1 = A.b;
     if (a0.x == R(0) && a0.y == R(0) && a0.z == R(0) && a0.w == R(0) && a1.x == R(0) && a1.y == R(0) &&
         a1.z == R(0)) {
         // untouched node: every derived quantity is 0 (ms_denom = 0); the BC
         // can only write its value, which is 0 unless bcval is present.
         if (g.bcval == nullptr || g.bcmask[i] == 0) {
-            g.gvT[i] = mk4<R>(0, 0, 0, 0);
-            g.gas[i] = mk4<R>(0, 0, 0, 0);
-            if (sp.need_vs) g.gvs[i] = mk4<R>(0, 0, 0, 0);
+            Node8<R> z;
+            z.a = mk4<R>(0, 0, 0, 0);
+            z.b = z.a;
+            g.gat[i] = z;
+            if (sp.need_vs) g.gvs[i] = z.a;
             return;
         }
     }
@@ -264,11 +331,14 @@ __global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
         }
     }
     if (D == 2) { vs[2] = vT[2] = as[2] = R(0); }
-    g.gvT[i] = mk4<R>(vT[0], vT[1], vT[2], 0);
-    g.gas[i] = mk4<R>(as[0], as[1], as[2], 0);
+    Node8<R> G;
+    G.a = mk4<R>(vT[0], vT[1], vT[2], 0);
+    G.b = mk4<R>(as[0], as[1], as[2], 0);
+    g.gat[i] = G;
     if (sp.need_vs) g.gvs[i] = mk4<R>(vs[0], vs[1], vs[2], 0);
-    g.acc0[i] = mk4<R>(m, 0, 0, 0);
-    g.acc1[i] = mk4<R>(0, 0, 0, 0);
+    A.a = mk4<R>(m, 0, 0, 0);
+    A.b = mk4<R>(0, 0, 0, 0);
+    g.acc[i] = A;
 }
 
 // ---------------------------------------------------------------------------
@@ -278,14 +348,20 @@ __global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
 // carried out by k_g2p, which gathers the same ΣN·vsT with the same weights.
 // ---------------------------------------------------------------------------
 template <int D, typename R>
-__global__ void __launch_bounds__(256) k_dmap(PDev<D, R> P, GDev<R> g, StepParams sp) {
+__global__ void __launch_bounds__(256, MPM_P_MINB) k_dmap(PDev<D, R> P, GDev<R> g, StepParams sp) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= sp.np) return;
     using T4 = typename Vec<R>::T4;
     double x[3];
     load_x<D, R>(P, i, x);
+    R vo[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) vo[d] = ldcs(P.v[d] + i);
+    const R m = ldcs(P.m + i);
     AxisW<R> w[3];
     particle_weights<D, R>(x, g, w);   // out-of-grid particles get zero weights
+    const int n0 = window_n0<D, R>(g, w);
+    const int plane = g.nnx * g.nny;
     R tT[3] = {0, 0, 0}, ta[3] = {0, 0, 0}, tv[3] = {0, 0, 0};
     constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
@@ -295,30 +371,24 @@ __global__ void __launch_bounds__(256) k_dmap(PDev<D, R> P, GDev<R> g, StepParam
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 R N = D == 3 ? w[0].N[a] * w[1].N[b] * w[2].N[c] : w[0].N[a] * w[1].N[b];
-                if (N == R(0)) continue;
-                int n = window_node<D, R>(g, w, a, b, c);
-                T4 vT = g.gvT[n];
-                tT[0] += N * vT.x; tT[1] += N * vT.y; tT[2] += N * vT.z;
-                if (sp.va == 0) {
-                    T4 as = g.gas[n];
-                    ta[0] += N * as.x; ta[1] += N * as.y; ta[2] += N * as.z;
-                }
+                const int n = n0 + a * g.nny + b + c * plane;
+                const Node8<R> q = g.gat[n];   // every valid window lies inside the grid
+                tT[0] += N * q.a.x; tT[1] += N * q.a.y; tT[2] += N * q.a.z;
+                ta[0] += N * q.b.x; ta[1] += N * q.b.y; ta[2] += N * q.b.z;
                 if (sp.need_vs) {
                     T4 vs = g.gvs[n];
                     tv[0] += N * vs.x; tv[1] += N * vs.y; tv[2] += N * vs.z;
                 }
             }
     const R dt = (R)sp.dt, FLIP = (R)sp.FLIP, PIC = (R)sp.PIC;
-    R vn[3];
+    R vn[3] = {0, 0, 0};
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        R vo = P.v[d][i];
-        if (sp.va == 0) vn[d] = FLIP * vo + PIC * tv[d] + ta[d] * dt;
-        else vn[d] = FLIP * (vo + (tT[d] - tv[d])) + PIC * tT[d];
-        P.v[d][i] = vn[d];
+        if (sp.va == 0) vn[d] = FLIP * vo[d] + PIC * tv[d] + ta[d] * dt;
+        else vn[d] = FLIP * (vo[d] + (tT[d] - tv[d])) + PIC * tT[d];
+        stcs(P.v[d] + i, vn[d]);
     }
-    R m = P.m[i];
-    R p[3] = {m * vn[0], m * vn[1], D == 3 ? m * vn[2] : R(0)};
+    const R p[3] = {m * vn[0], m * vn[1], D == 3 ? m * vn[2] : R(0)};
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -326,14 +396,14 @@ __global__ void __launch_bounds__(256) k_dmap(PDev<D, R> P, GDev<R> g, StepParam
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 R N = D == 3 ? w[0].N[a] * w[1].N[b] * w[2].N[c] : w[0].N[a] * w[1].N[b];
-                if (N == R(0)) continue;
-                int n = window_node<D, R>(g, w, a, b, c);
-                red_add4(&g.acc0[n], R(0), p[0] * N, p[1] * N, p[2] * N);
+                const int n = n0 + a * g.nny + b + c * plane;
+                if (N != R(0)) red_add4(&g.acc[n].a, R(0), p[0] * N, p[1] * N, p[2] * N);
             }
 }
 
 // doublemapping3_OS!, utils_OS.jl:968-1016: grid velocity from the re-mapped
-// momentum, BC, Δus = vs·ΔT.  Clears mass and momentum for the next P2G.
+// momentum, BC, Δus = vs·ΔT (into the second half of the gather record).
+// Clears mass and momentum for the next P2G.
 template <int D, typename R>
 __global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
     if (g.bflag[blockIdx.x] == 0) return;
@@ -342,11 +412,11 @@ __global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
     int i = block_node<D, R>(g, blockIdx.x, threadIdx.x);
     if (i < 0) return;
     using T4 = typename Vec<R>::T4;
-    T4 a0 = g.acc0[i];
+    const T4 a0 = g.acc[i].a;
     uint8_t bm = g.bcmask[i];
     if (a0.x == R(0) && a0.y == R(0) && a0.z == R(0) && a0.w == R(0) &&
         (g.bcval == nullptr || bm == 0)) {
-        g.gdu[i] = mk4<R>(0, 0, 0, 0);
+        g.gat[i].b = mk4<R>(0, 0, 0, 0);
         return;
     }
     const R eps = sizeof(R) == 8 ? R(2.220446049250313e-16) : R(1.1920929e-7);
@@ -362,56 +432,17 @@ __global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
         if (bm & (1 << d)) vs = bv[d];
         du[d] = vs * dt;
     }
-    g.gdu[i] = mk4<R>(du[0], du[1], du[2], 0);
-    g.acc0[i] = mk4<R>(0, 0, 0, 0);
+    g.gat[i].b = mk4<R>(du[0], du[1], du[2], 0);
+    g.acc[i].a = mk4<R>(0, 0, 0, 0);
 }
 
-// ---------------------------------------------------------------------------
-// G2P_OS! (utils_OS.jl:1025-1153) + the position update of DM1 + liE! +
-// dpP!/mcP!.  With FUSE, the next step's P2G scatters the updated particle
-// (resetmpstatus_OS! + P2G_OS! at the new position, gravity sp.G).
-// ---------------------------------------------------------------------------
-template <int D, typename R, bool FUSE>
-__global__ void __launch_bounds__(256) k_g2p(PDev<D, R> P, GDev<R> g, StepParams sp) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= sp.np) return;
-    using T4 = typename Vec<R>::T4;
+// Everything of G2P_OS! after the gathers, plus liE! and dpP!/mcP! and the
+// DM1 position update: x (in/out, FP64), tT = ΣN·vsT, dF = ΣΔu⊗∇N.  Stores
+// the particle and returns the new stress s and volume vol for the next P2G.
+template <int D, typename R>
+__device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp,
+                                                int64_t i, double *x, const R *tT, const R *dF, R *s, R &vol) {
     constexpr int NV = PDev<D, R>::NV, NF = PDev<D, R>::NF;
-    double x[3];
-    load_x<D, R>(P, i, x);
-    AxisW<R> w[3];
-    particle_weights<D, R>(x, g, w);
-    R tT[3] = {0, 0, 0};
-    R dF[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    constexpr int NC = D == 3 ? 3 : 1;
-#pragma unroll
-    for (int c = 0; c < NC; ++c)
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                R Nz = D == 3 ? w[2].N[c] : R(1);
-                R N = D == 3 ? w[0].N[a] * w[1].N[b] * Nz : w[0].N[a] * w[1].N[b];
-                if (N == R(0)) continue;
-                int n = window_node<D, R>(g, w, a, b, c);
-                T4 vT = g.gvT[n];
-                T4 du = g.gdu[n];
-                tT[0] += N * vT.x; tT[1] += N * vT.y;
-                if (D == 3) tT[2] += N * vT.z;
-                if (D == 2) {
-                    R gx = w[0].dN[a] * w[1].N[b];
-                    R gy = w[1].dN[b] * w[0].N[a];
-                    dF[0] += du.x * gx; dF[1] += du.x * gy;
-                    dF[2] += du.y * gx; dF[3] += du.y * gy;
-                } else {
-                    R gx = w[0].dN[a] * w[1].N[b] * Nz;
-                    R gy = w[1].dN[b] * w[0].N[a] * Nz;
-                    R gz = w[2].dN[c] * w[0].N[a] * w[1].N[b];
-                    dF[0] += du.x * gx; dF[1] += du.x * gy; dF[2] += du.x * gz;
-                    dF[3] += du.y * gx; dF[4] += du.y * gy; dF[5] += du.y * gz;
-                    dF[6] += du.z * gx; dF[7] += du.z * gy; dF[8] += du.z * gz;
-                }
-            }
     // position: ξ += ΔT·ΣN·vsT, accumulated in FP64
 #pragma unroll
     for (int d = 0; d < D; ++d) x[d] += (double)tT[d] * sp.dt;
@@ -431,16 +462,18 @@ __global__ void __launch_bounds__(256) k_g2p(PDev<D, R> P, GDev<R> g, StepParams
     }
     // strain
     if (D == 2) {
-        P.eps[0][i] += de[0]; P.eps[1][i] += de[1]; P.eps[3][i] += de[3];
+        stcs(P.eps[0] + i, ldcs(P.eps[0] + i) + de[0]);
+        stcs(P.eps[1] + i, ldcs(P.eps[1] + i) + de[1]);
+        stcs(P.eps[3] + i, ldcs(P.eps[3] + i) + de[3]);
     } else {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) P.eps[k][i] += de[k];
+        for (int k = 0; k < 6; ++k) stcs(P.eps[k] + i, ldcs(P.eps[k] + i) + de[k]);
     }
-    P.epsv[i] = ev;
+    stcs(P.epsv + i, ev);
     // F <- (I + ΔF) F; J = det F in FP64; Ω = J Ω0
     R f[9], fn[9];
 #pragma unroll
-    for (int k = 0; k < NF; ++k) f[k] = P.F[k][i];
+    for (int k = 0; k < NF; ++k) f[k] = ldcs(P.F[k] + i);
     double J;
     if (D == 2) {
         fn[0] = (dF[0] + R(1)) * f[0] + dF[1] * f[2];
@@ -463,37 +496,89 @@ __global__ void __launch_bounds__(256) k_g2p(PDev<D, R> P, GDev<R> g, StepParams
         J = g0 * g4 * g8 + g1 * g5 * g6 + g2 * g3 * g7 - g6 * g4 * g2 - g7 * g5 * g0 - g8 * g3 * g1;
     }
 #pragma unroll
-    for (int k = 0; k < NF; ++k) P.F[k][i] = fn[k];
-    R vol = (R)(J * (double)P.vol0[i]);
-    P.vol[i] = vol;
+    for (int k = 0; k < NF; ++k) stcs(P.F[k] + i, fn[k]);
+    vol = (R)(J * (double)ldcs(P.vol0 + i));
+    stcs(P.vol + i, vol);
     // stress: liE! then dpP! / mcP! (OS_MUSL.jl:82-96)
-    const Mat<R> M = g.mat[P.mat[i]];
-    R s[6], srot[6];
+    const Mat<R> M = g.mat[ldcs(P.mat + i)];
+    R srot[6];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) s[k] = P.sig[k][i];
+    for (int k = 0; k < NV; ++k) s[k] = ldcs(P.sig[k] + i);
     lin_elastic<D, R>(s, dF, de, M, srot);
-    R eq = P.epsq[i], ek = P.epsk[i];
-    if (sp.plastic) {
-        if (sp.constitutive == 1) {
-            drucker_prager<D, R>(s, eq, ek, M);
-            P.epsq[i] = eq; P.epsk[i] = ek;
-        } else if (sp.constitutive == 2 && D == 2) {
-            mohr_coulomb_2d<R>(s, eq, ek, M);
-            P.epsq[i] = eq; P.epsk[i] = ek;
-        }
+    if (sp.plastic && (sp.constitutive == 1 || (sp.constitutive == 2 && D == 2))) {
+        R eq = ldcs(P.epsq + i), ek = ldcs(P.epsk + i);
+        if (sp.constitutive == 1) drucker_prager<D, R>(s, eq, ek, M);
+        else mohr_coulomb_2d<R>(s, eq, ek, M);
+        stcs(P.epsq + i, eq);
+        stcs(P.epsk + i, ek);
     }
 #pragma unroll
-    for (int k = 0; k < NV; ++k) P.sig[k][i] = s[k];
+    for (int k = 0; k < NV; ++k) stcs(P.sig[k] + i, s[k]);
 #pragma unroll
-    for (int d = 0; d < D; ++d) P.x[d][i] = x[d];
+    for (int d = 0; d < D; ++d) stcs(P.x[d] + i, x[d]);
     bool bad = !(J > 0.0);
     bool nan = !isfinite(x[0]) || !isfinite(x[1]) || !isfinite((double)s[0]) || !isfinite((double)s[1]);
     if (bad) atomicOr(g.err, ERR_J);
     if (nan) atomicOr(g.err, ERR_NAN);
+}
+
+// ---------------------------------------------------------------------------
+// G2P_OS! (utils_OS.jl:1025-1153) + the position update of DM1 + liE! +
+// dpP!/mcP!.  With FUSE, the next step's P2G scatters the updated particle
+// (resetmpstatus_OS! + P2G_OS! at the new position, gravity sp.G).
+// ---------------------------------------------------------------------------
+template <int D, typename R, bool FUSE>
+__global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    double x[3];
+    load_x<D, R>(P, i, x);
+    AxisW<R> w[3];
+    particle_weights<D, R>(x, g, w);
+    const int n0 = window_n0<D, R>(g, w);
+    const int plane = g.nnx * g.nny;
+    R tT[3] = {0, 0, 0};
+    R dF[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    constexpr int NC = D == 3 ? 3 : 1;
+    // ΣΔu⊗∇N = Σ(Δu - Δu_c)⊗∇N since Σ∇N = 0 (uGIMP partition of unity); the
+    // window-centre node's Δu_c is subtracted before the products, which keeps
+    // the FP32 sum from cancelling when the motion is mostly a translation.
+    const auto duc = g.gat[n0 + g.nny + 1 + (D == 3 ? plane : 0)].b;
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                R Nz = D == 3 ? w[2].N[c] : R(1);
+                R N = D == 3 ? w[0].N[a] * w[1].N[b] * Nz : w[0].N[a] * w[1].N[b];
+                const Node8<R> q = g.gat[n0 + a * g.nny + b + c * plane];
+                const R ux = q.b.x - duc.x, uy = q.b.y - duc.y, uz = q.b.z - duc.z;
+                tT[0] += N * q.a.x; tT[1] += N * q.a.y;
+                if (D == 3) tT[2] += N * q.a.z;
+                if (D == 2) {
+                    R gx = w[0].dN[a] * w[1].N[b];
+                    R gy = w[1].dN[b] * w[0].N[a];
+                    dF[0] += ux * gx; dF[1] += ux * gy;
+                    dF[2] += uy * gx; dF[3] += uy * gy;
+                } else {
+                    R gx = w[0].dN[a] * w[1].N[b] * Nz;
+                    R gy = w[1].dN[b] * w[0].N[a] * Nz;
+                    R gz = w[2].dN[c] * w[0].N[a] * w[1].N[b];
+                    dF[0] += ux * gx; dF[1] += ux * gy; dF[2] += ux * gz;
+                    dF[3] += uy * gx; dF[4] += uy * gy; dF[5] += uy * gz;
+                    dF[6] += uz * gx; dF[7] += uz * gy; dF[8] += uz * gz;
+                }
+            }
+    R s[6], vol;
+    update_particle<D, R>(P, g, sp, i, x, tT, dF, s, vol);
     if (FUSE) {
         if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
-        R v[3] = {P.v[0][i], P.v[1][i], D == 3 ? P.v[2][i] : R(0)};
-        p2g_scatter<D, R>(g, w, P.m[i], vol, v, s, (R)sp.G);
+        R v[3];
+#pragma unroll
+        for (int d = 0; d < D; ++d) v[d] = ldcs(P.v[d] + i);
+        if (D == 2) v[2] = R(0);
+        p2g_scatter<D, R>(g, w, ldcs(P.m + i), vol, v, s, (R)sp.G);
     }
 }
 

@@ -3,8 +3,9 @@
 //
 // Key: the particle's cell (the reference's p2c cell, Julia fld/cld rule)
 // renumbered tile-major: tiles of TX x TY x TZ cells, key = tile * CPT +
-// cell-in-tile.  Order: ascending key, ties by ascending original particle
-// index -- exactly a CPU std::stable_sort by (key, original index).
+// cell-in-tile.  Order: ascending tile; inside a tile ascending rank of the
+// particle within its cell (rank = position by original index), then
+// ascending cell-in-tile -- a CPU stable sort by (tile, rank, cell-in-tile).
 //
 // Counting sort: count per key, exclusive scan, scatter (atomic slot within
 // the bucket), then each bucket is ordered by original index (buckets hold the
@@ -194,6 +195,50 @@ __global__ void __launch_bounds__(512) k_sort_big(const uint32_t *off, const uin
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
             pairs[b + i] = make_uint2((uint32_t)(s[i] >> 32), (uint32_t)(s[i] & 0xffffffffu));
         __syncthreads();
+    }
+}
+
+// Rank-major order inside each tile: the particles of a tile, ordered by
+// (cell, original index) after the bucket sort, are regrouped as (rank within
+// the cell, cell): the first particle of every cell, then the second one of
+// every cell, ...  Adjacent threads then work on adjacent cells, so their
+// stencils hit different nodes at the same time (no same-address conflicts in
+// the shared-memory scatter) while loads stay coalesced.  One CTA of CPT
+// threads (one per cell) per tile.
+template <int CPT>
+__global__ void __launch_bounds__(CPT) k_tile_transpose(const uint32_t *off, const uint32_t *tiles,
+                                                        const uint32_t *ntiles, const uint2 *src, uint2 *dst) {
+    __shared__ uint32_t ws[CPT / 32 + 1];
+    __shared__ uint32_t s_max;
+    const uint32_t nt = *ntiles;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint32_t q = blockIdx.x; q < nt; q += gridDim.x) {
+        const uint32_t t = tiles[q];
+        const uint32_t k = t * CPT + threadIdx.x;
+        const uint32_t b = off[k], n = off[k + 1] - b;
+        const uint32_t tile_base = off[t * CPT];
+        if (threadIdx.x == 0) s_max = 0;
+        __syncthreads();
+        atomicMax(&s_max, n);
+        __syncthreads();
+        const uint32_t maxn = s_max;
+        uint32_t level = tile_base;
+        for (uint32_t r = 0; r < maxn; ++r) {
+            uint32_t f = n > r ? 1u : 0u;
+            uint32_t bal = __ballot_sync(0xffffffffu, f);
+            uint32_t pre = __popc(bal & ((1u << lane) - 1u));
+            if (lane == 0) ws[wid] = __popc(bal);
+            __syncthreads();
+            uint32_t before = 0, tot = 0;
+            for (int w = 0; w < CPT / 32; ++w) {
+                uint32_t c = ws[w];
+                if (w < wid) before += c;
+                tot += c;
+            }
+            if (f) dst[level + before + pre] = src[b + r];
+            level += tot;
+            __syncthreads();
+        }
     }
 }
 

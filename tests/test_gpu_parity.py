@@ -24,9 +24,18 @@ def tol_stress(tol):
     return TOL32_STRESS if tol == TOL32 else tol
 
 
-def run_both(pkg, orc, case, nsteps, mask=None):
+def run_both(pkg, orc, case, nsteps, tiled=False):
+    import os
     lib = pkg._lib
-    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+    old = os.environ.get("MPM_B200_TILED")
+    os.environ["MPM_B200_TILED"] = "1" if tiled else "0"
+    try:
+        dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+    finally:
+        if old is None:
+            del os.environ["MPM_B200_TILED"]
+        else:
+            os.environ["MPM_B200_TILED"] = old
     dev.step(case.dt, 0.0, nsteps)
     out = fresh_particles(pkg, case.mp)
     dev.download(lib.F_REFERENCE | lib.F_F, out)
@@ -78,6 +87,38 @@ def test_steps_3d(pkg, orc, gpu_lib, prec, tol, model):
     case = small3d(pkg, constitutive=model, gpu_precision=prec)
     out, o = run_both(pkg, orc, case, 8)
     check_fields(out, o, case.mp, tol, tol_stress(tol))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_tiled_path(pkg, orc, gpu_lib, dim, prec, tol):
+    """The shared-memory tiled particle passes compute the same step."""
+    mk = small2d if dim == 2 else small3d
+    case = mk(pkg, constitutive="druckerprager", gpu_precision=prec)
+    out, o = run_both(pkg, orc, case, 8, tiled=True)
+    check_fields(out, o, case.mp, tol, tol_stress(tol))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", 1e-3)])
+def test_drift_beyond_tile_margin(pkg, orc, gpu_lib, prec, tol):
+    """No re-sort for 120 steps while the column translates by > 2 cells: the
+    particles leaving their tile's window take the global path.  Mixed mode is
+    checked on the kinematics only: the elastic velocities (~1e-3 m/s) ride on
+    a 3 m/s translation, and FP32 nodal velocities resolve them to ~1e-3, so
+    the stresses they integrate differ from FP64 by up to ~10 % -- the same
+    limit the reference has in its FP32 mode."""
+    case = small3d(pkg, constitutive="linearelastic", gpu_precision=prec, sort_every=100000,
+                   domain=(0.4, 0.12, 0.16))
+    case.mp.xi[:, 0] += 0.05          # away from the fixed wall
+    case.mp.vs[:, 0] = 3.0
+    out, o = run_both(pkg, orc, case, 120, tiled=True)
+    moved = np.abs(o.xi[:, 0] - case.mp.xi[:, 0]).max() / case.grid.dx
+    assert moved > 2.0
+    if prec == "fp64":
+        check_fields(out, o, case.mp, tol)
+    else:
+        assert rel(out.xi - case.mp.xi, o.xi - case.mp.xi) < tol
+        assert rel(out.vs, o.vs) < tol
 
 
 @pytest.mark.parametrize("dim", [2, 3])
@@ -191,7 +232,15 @@ def test_sort_bit_exact(pkg, orc, gpu_lib, dim):
     dev.close()
     o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc)
     key = host_key(o.p2c(case.mp.xi), case.grid, dim)
-    expect = np.lexsort((np.arange(case.mp.np), key))
+    cpt = 128 if dim == 3 else 64
+    # rank of each particle within its cell, by original index
+    by_cell = np.lexsort((np.arange(case.mp.np), key))
+    rank = np.empty(case.mp.np, np.int64)
+    ks = key[by_cell]
+    start = np.r_[0, np.flatnonzero(np.diff(ks)) + 1]
+    lens = np.diff(np.r_[start, len(ks)])
+    rank[by_cell] = np.arange(len(ks)) - np.repeat(start, lens)
+    expect = np.lexsort((key % cpt, rank, key // cpt))
     assert np.array_equal(order, expect)
 
 
