@@ -189,6 +189,34 @@ int mpm_sort(mpm_handle *h);
 int mpm_run_stages(mpm_handle *h, double dt, double Ti, uint32_t stage_mask);
 int mpm_download_grid(mpm_handle *h, int32_t field, double *out);
 
+/* ---- cell ordering without allocation ----
+ * No counterpart in the reference (which never reorders particles).  For
+ * callers that cannot allocate device memory -- a host runtime that owns all
+ * device memory through its own pool, code running while a CUDA graph is
+ * being captured, a real-time loop that must not hit the allocator's implicit
+ * synchronisation -- this computes what mpm_compute_p2c() and mpm_sort() +
+ * mpm_download_order() compute for particles in their original order:
+ * p2c_out[i] (1-based, the reference's formula) and order_out[k] (0-based
+ * index of the k-th particle in the library's cell-sorted order).  All five
+ * pointers are caller-owned DEVICE buffers (x, y, z: np FP64 coordinates; z is
+ * unused in 2D; order_out, p2c_out: np int64).  The grid and np come from
+ * `d` (the other descriptor fields are ignored).  The work runs on `stream`
+ * (a cudaStream_t; NULL = default stream) and the call returns after it.
+ *
+ * The scratch is a fixed static device array of MPM_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading the library holds until process exit; np above
+ * MPM_NOALLOC_MAX_PARTICLES or a grid above MPM_NOALLOC_MAX_KEYS cell keys
+ * (cells rounded up to whole 4x8x4 / 8x8 tiles) is rejected with MPM_E_ARG.
+ * The first call on each device looks up the scratch's device address (with
+ * that device current); make it before any stream capture.  All calls share
+ * the one scratch array, so calls whose work overlaps on the GPU race: issue
+ * them on one stream or serialise them.  Errors: mpm_last_error(NULL). */
+#define MPM_NOALLOC_MAX_PARTICLES (1 << 19)
+#define MPM_NOALLOC_MAX_KEYS (1 << 19)
+#define MPM_NOALLOC_SCRATCH_BYTES 14731264
+int mpm_cell_order_noalloc(const mpm_desc *d, const double *x, const double *y, const double *z,
+                           int64_t *order_out, int64_t *p2c_out, void *stream);
+
 /* ---- diagnostics ---- */
 /* sizeof(mpm_desc), sizeof(mpm_view), sizeof(mpm_host_views), sizeof(mpm_stats):
  * lets a binding verify its struct layouts against the library's. */

@@ -34,8 +34,10 @@ EXPORTS = [
     "mpm_create", "mpm_upload", "mpm_destroy", "mpm_step", "mpm_step_async", "mpm_sync",
     "mpm_download", "mpm_compute_p2c", "mpm_download_order", "mpm_sort", "mpm_run_stages",
     "mpm_download_grid", "mpm_get_stats", "mpm_last_error", "mpm_peak_bandwidth",
-    "mpm_set_profiling", "mpm_get_kernel_times", "mpm_abi_sizes",
+    "mpm_set_profiling", "mpm_get_kernel_times", "mpm_abi_sizes", "mpm_cell_order_noalloc",
 ]
+NOALLOC_MAX_PARTICLES = 1 << 19
+NOALLOC_MAX_KEYS = 1 << 19
 
 
 class Desc(C.Structure):
@@ -92,7 +94,8 @@ def build(force=False, verbose=False):
             and all(os.path.getmtime(LIB_PATH) >= os.path.getmtime(s) for s in srcs)):
         return LIB_PATH
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB_PATH, os.path.join(CSRC, "mpm_b200.cu")]
+    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB_PATH, os.path.join(CSRC, "mpm_b200.cu"),
+                                 os.path.join(CSRC, "mpm_noalloc.cu")]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)
@@ -132,6 +135,7 @@ def lib():
     L.mpm_get_kernel_times.argtypes = [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
                                        C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]
     L.mpm_abi_sizes.argtypes = [C.POINTER(C.c_int64)] * 4
+    L.mpm_cell_order_noalloc.argtypes = [C.POINTER(Desc)] + [C.c_void_p] * 6
     sizes = [C.c_int64() for _ in range(4)]
     L.mpm_abi_sizes(*[C.byref(x) for x in sizes])
     mine = [C.sizeof(Desc), C.sizeof(View), C.sizeof(HostViews), C.sizeof(Stats)]

@@ -770,6 +770,10 @@ thread_local std::string g_create_error;
 
 }  // namespace
 
+namespace mpm_detail {
+__attribute__((visibility("hidden"))) void set_global_error(const std::string &m) { g_create_error = m; }
+}
+
 // =====================================================================================
 // C ABI
 // =====================================================================================

@@ -81,7 +81,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *tot) {
     return base + x - v;
 }
 
-__global__ void __launch_bounds__(SCAN_T) k_scan_reduce(const uint32_t *in, uint32_t n, uint32_t *bsum) {
+static __global__ void __launch_bounds__(SCAN_T) k_scan_reduce(const uint32_t *in, uint32_t n, uint32_t *bsum) {
     uint32_t base = blockIdx.x * SCAN_CHUNK;
     uint32_t s = 0;
 #pragma unroll
@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_reduce(const uint32_t *in, uint
     if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
 }
 
-__global__ void __launch_bounds__(SCAN_T) k_scan_top(uint32_t *bsum, uint32_t nb) {
+static __global__ void __launch_bounds__(SCAN_T) k_scan_top(uint32_t *bsum, uint32_t nb) {
     uint32_t carry = 0;
     for (uint32_t base = 0; base < nb; base += SCAN_T) {
         uint32_t i = base + threadIdx.x;
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_top(uint32_t *bsum, uint32_t nb
 }
 
 // off[i] = exclusive prefix of in; off[n] = total
-__global__ void __launch_bounds__(SCAN_T) k_scan_down(const uint32_t *in, uint32_t n, const uint32_t *bsum,
+static __global__ void __launch_bounds__(SCAN_T) k_scan_down(const uint32_t *in, uint32_t n, const uint32_t *bsum,
                                                       uint32_t *off) {
     uint32_t base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_IT;
     uint32_t v[SCAN_IT];
@@ -144,7 +144,7 @@ __global__ void k_sort_scatter(PDev<D, R> P, int64_t np, const uint32_t *keys, c
 constexpr int BUCKET_SMALL = 32;
 constexpr int BUCKET_MAX = 4096;
 
-__global__ void k_sort_buckets(const uint32_t *off, uint32_t nk, uint2 *pairs, uint32_t *big,
+static __global__ void k_sort_buckets(const uint32_t *off, uint32_t nk, uint2 *pairs, uint32_t *big,
                                uint32_t *nbig, uint32_t big_cap, int *err) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nk) return;
@@ -167,7 +167,7 @@ __global__ void k_sort_buckets(const uint32_t *off, uint32_t nk, uint2 *pairs, u
 }
 
 // bitonic sort of one large bucket in shared memory (one CTA per bucket)
-__global__ void __launch_bounds__(512) k_sort_big(const uint32_t *off, const uint32_t *big, const uint32_t *nbig,
+static __global__ void __launch_bounds__(512) k_sort_big(const uint32_t *off, const uint32_t *big, const uint32_t *nbig,
                                                   uint32_t big_cap, uint2 *pairs) {
     __shared__ unsigned long long s[BUCKET_MAX];
     uint32_t nb = *nbig;
@@ -196,6 +196,13 @@ __global__ void __launch_bounds__(512) k_sort_big(const uint32_t *off, const uin
             pairs[b + i] = make_uint2((uint32_t)(s[i] >> 32), (uint32_t)(s[i] & 0xffffffffu));
         __syncthreads();
     }
+}
+
+// list of the tiles that hold particles after a sort
+static __global__ void k_tile_list(const uint32_t *off, uint32_t ntile, uint32_t cpt, uint32_t *tiles, uint32_t *ntiles) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntile) return;
+    if (off[(t + 1) * cpt] > off[t * cpt]) tiles[atomicAdd(ntiles, 1u)] = t;
 }
 
 // Rank-major order inside each tile: the particles of a tile, ordered by

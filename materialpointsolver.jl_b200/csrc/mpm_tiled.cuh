@@ -37,11 +37,6 @@ struct TileList {
     SortGeom sg;
 };
 
-__global__ void k_tile_list(const uint32_t *off, uint32_t ntile, uint32_t cpt, uint32_t *tiles, uint32_t *ntiles) {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntile) return;
-    if (off[(t + 1) * cpt] > off[t * cpt]) tiles[atomicAdd(ntiles, 1u)] = t;
-}
 
 template <int D> struct TileGeo {
     int c0[3];   // first cell of the tile
