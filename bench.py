@@ -105,6 +105,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+def max_over_ranks(x, device):
+    """Max of a per-rank scalar over all ranks of the default process group."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, npart, steps, t_max_ms):
+    """Whole-job particle-updates/s of `world` independent replicas, each
+    stepping `npart` particles `steps` times, timed by the slowest rank."""
+    return world * npart * steps / (t_max_ms * 1e-3)
+
+
 def make_case(mc3d):
     import __graft_entry__ as g
     pkg = g.load_package()
@@ -186,12 +201,8 @@ def run_b200(args):
     launches = st.launches - launches0
     na = st.active_nodes
     Ti += K * dt
-    t_max = ms
-    if use_dist:
-        tt = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = world * npart * K / (t_max * 1e-3)
+    t_max = max_over_ranks(ms, f"cuda:{local}") if use_dist else ms
+    value = replica_value(world, npart, K, t_max)
 
     # ---- per-kernel device times (events on the library stream) ----
     dev.set_profiling(True)
