@@ -397,6 +397,7 @@ template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, do
     sp.zeta = h->d.zeta_s;
     sp.plastic = Ti >= h->d.Te;
     sp.constitutive = h->d.constitutive;
+    sp.mc3d = h->d.mc3d == MPM_MC3D_RESTATED ? 1 : 0;
     sp.va = h->d.va;
     sp.need_vs = (h->d.PIC != 0.0 || h->d.va == MPM_VA_V) ? 1 : 0;
     sp.np = h->d.np;
@@ -432,6 +433,7 @@ template <int D, typename R> const TiledCfg &tiled_cfg(mpm_handle *h, int need_v
     cc.smem_g2p = (size_t)6 * W::WN * sizeof(R);
     CK(cudaFuncSetAttribute(k_dmap_tile<D, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cc.smem_dm));
     CK(cudaFuncSetAttribute(k_g2p_tile<D, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cc.smem_g2p));
+    CK(cudaFuncSetAttribute(k_g2p_tile<D, R, D == 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cc.smem_g2p));
     int a = 0, b = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_dmap_tile<D, R>, 256, cc.smem_dm));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_g2p_tile<D, R>, 256, cc.smem_g2p));
@@ -460,17 +462,24 @@ template <int D, typename R> void run_steps(mpm_handle *h, double dt, double Ti0
         PDev<D, R> P = pdev_from<D, R>(h, 0);
         GDev<R> g = gdev_from<R>(h);
         StepParams sp = make_params<D, R>(h, dt, Ti, gravity_at(h->d, Tn));
+        const bool mc3 = sp.mc3d && sp.constitutive == MPM_MOHRCOULOMB;
         L.run("solve", [&] { k_solve<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         if (h->tiled) {
             TileList tl{h->tiles, h->ntiles, h->off, h->sg};
             const TiledCfg &c = tiled_cfg<D, R>(h, sp.need_vs);
             if (np) L.run("dmap", [&] { k_dmap_tile<D, R><<<c.grid_dm, 256, c.smem_dm, h->stream>>>(P, g, sp, tl); });
             L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-            if (np) L.run("g2p_p2g", [&] { k_g2p_tile<D, R><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl); });
+            if (np) L.run("g2p_p2g", [&] {
+                if (mc3) k_g2p_tile<D, R, D == 3><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
+                else k_g2p_tile<D, R><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
+            });
         } else {
             if (np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
             L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-            if (np) L.run("g2p_p2g", [&] { k_g2p<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+            if (np) L.run("g2p_p2g", [&] {
+                if (mc3) k_g2p<D, R, true, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                else k_g2p<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            });
         }
         Ti = Tn;
         h->since_sort++;
@@ -711,7 +720,11 @@ template <int D, typename R> struct Stages {
         if (mask & 2u) L.run("solve", [&] { k_solve<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         if ((mask & 4u) && np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
         if (mask & 8u) L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-        if ((mask & 16u) && np) L.run("g2p", [&] { k_g2p<D, R, false><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        const bool mc3 = sp.mc3d && sp.constitutive == MPM_MOHRCOULOMB;
+        if ((mask & 16u) && np) L.run("g2p", [&] {
+            if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_g2p<D, R, false><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+        });
         h->acc_valid = false;
     }
 };
@@ -799,8 +812,7 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
             throw Err{MPM_E_ARG, "particle size must satisfy 0 < lp <= h (at most 3 uGIMP nodes per axis)"};
         if (d->constitutive < 0 || d->constitutive > 2) throw Err{MPM_E_UNSUPPORTED, "constitutive model not provided (hyperelastic is out of scope)"};
         if (d->mvl) throw Err{MPM_E_UNSUPPORTED, "MVL volumetric-locking mitigation is not provided by this backend"};
-        if (d->dim == 3 && d->constitutive == MPM_MOHRCOULOMB && d->mc3d == MPM_MC3D_RESTATED)
-            throw Err{MPM_E_UNSUPPORTED, "restated 3D Mohr-Coulomb is not provided on the device"};
+        if (d->mc3d != MPM_MC3D_LITERAL && d->mc3d != MPM_MC3D_RESTATED) throw Err{MPM_E_ARG, "mc3d must be 0 or 1"};
         h->d = *d;
         if (h->d.dim == 2) { h->d.nnz = 1; h->d.z1 = 0; h->d.dz = 1; h->d.lpz = 1; }
         h->fp64 = d->precision == MPM_PREC_FP64;

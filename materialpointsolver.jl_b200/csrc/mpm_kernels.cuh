@@ -23,6 +23,7 @@
 // reads or reduces one sector.
 #pragma once
 #include "mpm_device.cuh"
+#include "mpm_mc3d.cuh"
 
 // resident CTAs of 256 threads per SM the particle passes are register-capped for
 #ifndef MPM_P_MINB
@@ -148,6 +149,7 @@ struct StepParams {
     int constitutive;
     int va;          // 0 = :a, 1 = :v
     int need_vs;     // DM gathers grid vs
+    int mc3d;        // 3D Mohr-Coulomb: 0 elastic predictor only (literal), 1 restated return
     int64_t np;
 };
 
@@ -439,7 +441,7 @@ __global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
 // Everything of G2P_OS! after the gathers, plus liE! and dpP!/mcP! and the
 // DM1 position update: x (in/out, FP64), tT = ΣN·vsT, dF = ΣΔu⊗∇N.  Stores
 // the particle and returns the new stress s and volume vol for the next P2G.
-template <int D, typename R>
+template <int D, typename R, bool MC3 = false>
 __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp,
                                                 int64_t i, double *x, const R *tT, const R *dF, R *s, R &vol) {
     constexpr int NV = PDev<D, R>::NV, NF = PDev<D, R>::NF;
@@ -511,6 +513,19 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
         else mohr_coulomb_2d<R>(s, eq, ek, M);
         stcs(P.epsq + i, eq);
         stcs(P.epsk + i, ek);
+    } else if (MC3 && D == 3 && sp.plastic && sp.constitutive == 2) {
+        // restated 3D Mohr-Coulomb, FP64 (mohrcoulomb.jl:152-455, commented out there)
+        double sd[6], s0d[6], ded[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) { sd[k] = s[k]; s0d[k] = srot[k]; ded[k] = de[k]; }
+        const mc3d::Par mp = {(double)M.K, (double)M.G, (double)M.c, (double)M.phi, (double)M.psi,
+                              (double)M.sigt, (double)M.sphi, (double)M.cphi, (double)M.tphi, (double)M.tpsi};
+        double eq = ldcs(P.epsq + i);
+        if (mc3d::mohr_coulomb_3d(sd, s0d, ded, eq, mp)) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) s[k] = (R)sd[k];
+            stcs(P.epsq + i, (R)eq);
+        }
     }
 #pragma unroll
     for (int k = 0; k < NV; ++k) stcs(P.sig[k] + i, s[k]);
@@ -527,7 +542,7 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
 // dpP!/mcP!.  With FUSE, the next step's P2G scatters the updated particle
 // (resetmpstatus_OS! + P2G_OS! at the new position, gravity sp.G).
 // ---------------------------------------------------------------------------
-template <int D, typename R, bool FUSE>
+template <int D, typename R, bool FUSE, bool MC3 = false>
 __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g, StepParams sp) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= sp.np) return;
@@ -571,7 +586,7 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
                 }
             }
     R s[6], vol;
-    update_particle<D, R>(P, g, sp, i, x, tT, dF, s, vol);
+    update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol);
     if (FUSE) {
         if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
         R v[3];

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_dmap_tile(PDev<D, R> P, GDe
 // Tiled G2P + stress + position update, fused with the next step's P2G.
 // smem: vsT and Δu of the window, structure of arrays.
 // ---------------------------------------------------------------------------
-template <int D, typename R>
+template <int D, typename R, bool MC3 = false>
 __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p_tile(PDev<D, R> P, GDev<R> g, StepParams sp, TileList tl) {
     using W = Win<D>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p_tile(PDev<D, R> P, GDev
             if (inw) g2p_gather<D, R, true>(g, w, lb, n0, s_vT, s_du, tT, dF);
             else g2p_gather<D, R, false>(g, w, lb, n0, s_vT, s_du, tT, dF);
             R s[6], vol;
-            update_particle<D, R>(P, g, sp, i, x, tT, dF, s, vol);
+            update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol);
             // next step's P2G at the new position, straight into the node records
             if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); continue; }
             R v[3];

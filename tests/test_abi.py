@@ -116,7 +116,7 @@ def _desc(pkg, **over):
     (dict(lpx=0.05), -1, b"particle size"),      # lp > h: more than 3 uGIMP nodes per axis
     (dict(constitutive=3), -8, b"constitutive"),
     (dict(mvl=1), -8, b"MVL"),
-    (dict(mc3d=1, constitutive=2), -8, b"Mohr-Coulomb"),
+    (dict(mc3d=5), -1, b"mc3d"),
 ])
 def test_create_rejects_bad_descriptors(pkg, L, over, code, msg):
     """Validation runs before any CUDA call, so it is exercised without a GPU."""

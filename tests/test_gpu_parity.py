@@ -90,6 +90,23 @@ def test_steps_3d(pkg, orc, gpu_lib, prec, tol, model):
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+def test_mc3d_restated(pkg, orc, gpu_lib, prec, tol):
+    """The restated 3D Mohr-Coulomb return (FP64 on the device in both modes)
+    against the oracle's restatement, over steps where most particles yield."""
+    case = small3d(pkg, constitutive="mohrcoulomb", mc3d="restated", gpu_precision=prec)
+    out, o = run_both(pkg, orc, case, 20)
+    assert (o.epsq > 0).mean() > 0.5
+    check_fields(out, o, case.mp, tol, tol_stress(tol))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+def test_mc3d_restated_tiled(pkg, orc, gpu_lib, prec, tol):
+    case = small3d(pkg, constitutive="mohrcoulomb", mc3d="restated", gpu_precision=prec)
+    out, o = run_both(pkg, orc, case, 20, tiled=True)
+    check_fields(out, o, case.mp, tol, tol_stress(tol))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_tiled_path(pkg, orc, gpu_lib, dim, prec, tol):
     """The shared-memory tiled particle passes compute the same step."""
