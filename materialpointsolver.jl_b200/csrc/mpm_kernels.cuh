@@ -208,6 +208,12 @@ __device__ __forceinline__ int window_node(const GDev<R> &g, const AxisW<R> *w, 
 // P2G scatter of one particle (P2G_OS!, utils_OS.jl:424-496): nodal mass,
 // momentum and force; gravity on the last axis.  Nodes with N == 0 are skipped
 // like the reference's `if Ni ≠ 0`.
+//
+// The weights are separable, N = Nx·Ny·Nz and ∇N = (dNx·Ny·Nz, Nx·dNy·Nz,
+// Nx·Ny·dNz), so the terms that do not depend on the y index are formed once
+// per (x, z) column of the window: with σv = -Ω·σ,
+//   f_k(node) = Ny·X_k + dNy·Y_k,  X_k = σv_kx·dNx·Nz + σv_kz·Nx·dNz (+ m·Nx·Nz·g
+//   on the gravity axis), Y_k = σv_ky·Nx·Nz;  m·N = Ny·(m·Nx·Nz), p·N likewise.
 // ---------------------------------------------------------------------------
 template <int D, typename R>
 __device__ __forceinline__ void p2g_scatter(const GDev<R> &g, const AxisW<R> *w, R m, R vol,
@@ -216,39 +222,53 @@ __device__ __forceinline__ void p2g_scatter(const GDev<R> &g, const AxisW<R> *w,
     const R p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : R(0)};
     const int n0 = window_n0<D, R>(g, w);
     const int plane = g.nnx * g.nny;
-    constexpr int NC = D == 3 ? 3 : 1;
+    if (D == 2) {
+        // σv rows: (xx, xy), (xy, yy)
+        const R sxx = -vol * s[0], syy = -vol * s[1], sxy = -vol * s[3];
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a) {
+            const R wx = w[0].N[a], gx = w[0].dN[a];
+            if (wx == R(0)) continue;
+            const R M = m * wx, P0 = p[0] * wx, P1 = p[1] * wx;
+            const R X0 = sxx * gx, X1 = sxy * gx + M * G;
+            const R Y0 = sxy * wx, Y1 = syy * wx;
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                const R Nz = D == 3 ? w[2].N[c] : R(1);
-                const R N = D == 3 ? w[0].N[a] * w[1].N[b] * Nz : w[0].N[a] * w[1].N[b];
-                Node8<R> *q = g.acc + (n0 + a * g.nny + b + c * plane);
-                const R NiM = m * N;
-                if (D == 2) {
-                    const R gx = w[0].dN[a] * w[1].N[b];
-                    const R gy = w[1].dN[b] * w[0].N[a];
-                    const R fx = -vol * (gx * s[0] + gy * s[3]);
-                    const R fy = -vol * (gy * s[1] + gx * s[3]) + NiM * G;
-                    if (N != R(0)) {
-                        red_add4(&q->a, NiM, N * p[0], N * p[1], R(0));
-                        red_add4(&q->b, fx, fy, R(0), R(0));
-                    }
-                } else {
-                    const R gx = w[0].dN[a] * w[1].N[b] * Nz;
-                    const R gy = w[1].dN[b] * w[0].N[a] * Nz;
-                    const R gz = w[2].dN[c] * w[0].N[a] * w[1].N[b];
-                    const R fx = -vol * (gx * s[0] + gy * s[3] + gz * s[5]);
-                    const R fy = -vol * (gy * s[1] + gx * s[3] + gz * s[4]);
-                    const R fz = -vol * (gz * s[2] + gx * s[5] + gy * s[4]) + NiM * G;
-                    if (N != R(0)) {
-                        red_add4(&q->a, NiM, N * p[0], N * p[1], N * p[2]);
-                        red_add4(&q->b, fx, fy, fz, R(0));
-                    }
+                const R wy = w[1].N[b], gy = w[1].dN[b];
+                if (wy == R(0)) continue;
+                Node8<R> *q = g.acc + (n0 + a * g.nny + b);
+                red_add4(&q->a, M * wy, P0 * wy, P1 * wy, R(0));
+                red_add4(&q->b, wy * X0 + gy * Y0, wy * X1 + gy * Y1, R(0), R(0));
+            }
+        }
+    } else {
+        const R sv[6] = {-vol * s[0], -vol * s[1], -vol * s[2], -vol * s[3], -vol * s[4], -vol * s[5]};
+        // Voigt xx yy zz xy yz zx: rows x = (0, 3, 5), y = (3, 1, 4), z = (5, 4, 2)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const R wz = w[2].N[c], gz = w[2].dN[c];
+            if (wz == R(0)) continue;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const R wx = w[0].N[a];
+                if (wx == R(0)) continue;
+                const R wxz = wx * wz, gxz = w[0].dN[a] * wz, xdz = wx * gz;
+                const R M = m * wxz, P0 = p[0] * wxz, P1 = p[1] * wxz, P2 = p[2] * wxz;
+                const R X0 = sv[0] * gxz + sv[5] * xdz;
+                const R X1 = sv[3] * gxz + sv[4] * xdz;
+                const R X2 = sv[5] * gxz + sv[2] * xdz + M * G;
+                const R Y0 = sv[3] * wxz, Y1 = sv[1] * wxz, Y2 = sv[4] * wxz;
+                Node8<R> *col = g.acc + (n0 + a * g.nny + c * plane);
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const R wy = w[1].N[b], gy = w[1].dN[b];
+                    if (wy == R(0)) continue;
+                    red_add4(&col[b].a, M * wy, P0 * wy, P1 * wy, P2 * wy);
+                    red_add4(&col[b].b, wy * X0 + gy * Y0, wy * X1 + gy * Y1, wy * X2 + gy * Y2, R(0));
                 }
             }
+        }
+    }
 }
 
 template <int D, typename R>
@@ -366,41 +386,69 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_dmap(PDev<D, R> P, GDev<R> 
     const int plane = g.nnx * g.nny;
     R tT[3] = {0, 0, 0}, ta[3] = {0, 0, 0}, tv[3] = {0, 0, 0};
     constexpr int NC = D == 3 ? 3 : 1;
+    const bool va_v = sp.va != 0, need_vs = sp.need_vs != 0;
+    // ΣN·q = Σ_(x,z) Nx·Nz·(Σ_y Ny·q): inner sums along the contiguous y run
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
+    for (int c = 0; c < NC; ++c) {
+        const R wz = D == 3 ? w[2].N[c] : R(1);
+        if (wz == R(0)) continue;
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a) {
+            const R wx = w[0].N[a];
+            if (wx == R(0)) continue;
+            const int col = n0 + a * g.nny + c * plane;
+            R sT[3] = {0, 0, 0}, sa[3] = {0, 0, 0}, sv[3] = {0, 0, 0};
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                R N = D == 3 ? w[0].N[a] * w[1].N[b] * w[2].N[c] : w[0].N[a] * w[1].N[b];
-                const int n = n0 + a * g.nny + b + c * plane;
-                const Node8<R> q = g.gat[n];   // every valid window lies inside the grid
-                tT[0] += N * q.a.x; tT[1] += N * q.a.y; tT[2] += N * q.a.z;
-                ta[0] += N * q.b.x; ta[1] += N * q.b.y; ta[2] += N * q.b.z;
-                if (sp.need_vs) {
-                    T4 vs = g.gvs[n];
-                    tv[0] += N * vs.x; tv[1] += N * vs.y; tv[2] += N * vs.z;
+                const R wy = w[1].N[b];
+                if (wy == R(0)) continue;
+                const T4 qb = g.gat[col + b].b;   // every valid window lies inside the grid
+                sa[0] += wy * qb.x; sa[1] += wy * qb.y; sa[2] += wy * qb.z;
+                if (va_v) {
+                    const T4 qa = g.gat[col + b].a;
+                    sT[0] += wy * qa.x; sT[1] += wy * qa.y; sT[2] += wy * qa.z;
+                }
+                if (need_vs) {
+                    const T4 vs = g.gvs[col + b];
+                    sv[0] += wy * vs.x; sv[1] += wy * vs.y; sv[2] += wy * vs.z;
                 }
             }
+            const R wxz = wx * wz;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ta[d] += wxz * sa[d];
+                tT[d] += wxz * sT[d];
+                tv[d] += wxz * sv[d];
+            }
+        }
+    }
     const R dt = (R)sp.dt, FLIP = (R)sp.FLIP, PIC = (R)sp.PIC;
     R vn[3] = {0, 0, 0};
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        if (sp.va == 0) vn[d] = FLIP * vo[d] + PIC * tv[d] + ta[d] * dt;
+        if (!va_v) vn[d] = FLIP * vo[d] + PIC * tv[d] + ta[d] * dt;
         else vn[d] = FLIP * (vo[d] + (tT[d] - tv[d])) + PIC * tT[d];
         stcs(P.v[d] + i, vn[d]);
     }
     const R p[3] = {m * vn[0], m * vn[1], D == 3 ? m * vn[2] : R(0)};
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
+    for (int c = 0; c < NC; ++c) {
+        const R wz = D == 3 ? w[2].N[c] : R(1);
+        if (wz == R(0)) continue;
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a) {
+            const R wxz = w[0].N[a] * wz;
+            if (wxz == R(0)) continue;
+            const R P0 = p[0] * wxz, P1 = p[1] * wxz, P2 = p[2] * wxz;
+            Node8<R> *col = g.acc + (n0 + a * g.nny + c * plane);
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                R N = D == 3 ? w[0].N[a] * w[1].N[b] * w[2].N[c] : w[0].N[a] * w[1].N[b];
-                const int n = n0 + a * g.nny + b + c * plane;
-                if (N != R(0)) red_add4(&g.acc[n].a, R(0), p[0] * N, p[1] * N, p[2] * N);
+                const R wy = w[1].N[b];
+                if (wy == R(0)) continue;
+                red_add4(&col[b].a, R(0), P0 * wy, P1 * wy, P2 * wy);
             }
+        }
+    }
 }
 
 // doublemapping3_OS!, utils_OS.jl:968-1016: grid velocity from the re-mapped
@@ -520,11 +568,11 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
         for (int k = 0; k < 6; ++k) { sd[k] = s[k]; s0d[k] = srot[k]; ded[k] = de[k]; }
         const mc3d::Par mp = {(double)M.K, (double)M.G, (double)M.c, (double)M.phi, (double)M.psi,
                               (double)M.sigt, (double)M.sphi, (double)M.cphi, (double)M.tphi, (double)M.tpsi};
-        double eq = ldcs(P.epsq + i);
-        if (mc3d::mohr_coulomb_3d(sd, s0d, ded, eq, mp)) {
+        const mc3d::Ret r = mc3d::mohr_coulomb_3d(sd, s0d, ded, mp);
+        if (r.yielded) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) s[k] = (R)sd[k];
-            stcs(P.epsq + i, (R)eq);
+            stcs(P.epsq + i, (R)((double)ldcs(P.epsq + i) + r.dq));
         }
     }
 #pragma unroll
@@ -558,33 +606,47 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
     // ΣΔu⊗∇N = Σ(Δu - Δu_c)⊗∇N since Σ∇N = 0 (uGIMP partition of unity); the
     // window-centre node's Δu_c is subtracted before the products, which keeps
     // the FP32 sum from cancelling when the motion is mostly a translation.
+    // Separable sums: per (x, z) column, A = ΣNy·Δu', B = ΣdNy·Δu', T = ΣNy·vsT;
+    // then ∂/∂x += dNx·Nz·A, ∂/∂y += Nx·Nz·B, ∂/∂z += Nx·dNz·A, tT += Nx·Nz·T.
     const auto duc = g.gat[n0 + g.nny + 1 + (D == 3 ? plane : 0)].b;
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
+    for (int c = 0; c < NC; ++c) {
+        const R wz = D == 3 ? w[2].N[c] : R(1);
+        const R gz = D == 3 ? w[2].dN[c] : R(0);
+        if (wz == R(0)) continue;
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a) {
+            const R wx = w[0].N[a];
+            if (wx == R(0)) continue;
+            const int col = n0 + a * g.nny + c * plane;
+            R T[3] = {0, 0, 0}, A[3] = {0, 0, 0}, B[3] = {0, 0, 0};
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                R Nz = D == 3 ? w[2].N[c] : R(1);
-                R N = D == 3 ? w[0].N[a] * w[1].N[b] * Nz : w[0].N[a] * w[1].N[b];
-                const Node8<R> q = g.gat[n0 + a * g.nny + b + c * plane];
-                const R ux = q.b.x - duc.x, uy = q.b.y - duc.y, uz = q.b.z - duc.z;
-                tT[0] += N * q.a.x; tT[1] += N * q.a.y;
-                if (D == 3) tT[2] += N * q.a.z;
-                if (D == 2) {
-                    R gx = w[0].dN[a] * w[1].N[b];
-                    R gy = w[1].dN[b] * w[0].N[a];
-                    dF[0] += ux * gx; dF[1] += ux * gy;
-                    dF[2] += uy * gx; dF[3] += uy * gy;
-                } else {
-                    R gx = w[0].dN[a] * w[1].N[b] * Nz;
-                    R gy = w[1].dN[b] * w[0].N[a] * Nz;
-                    R gz = w[2].dN[c] * w[0].N[a] * w[1].N[b];
-                    dF[0] += ux * gx; dF[1] += ux * gy; dF[2] += ux * gz;
-                    dF[3] += uy * gx; dF[4] += uy * gy; dF[5] += uy * gz;
-                    dF[6] += uz * gx; dF[7] += uz * gy; dF[8] += uz * gz;
+                const R wy = w[1].N[b], gy = w[1].dN[b];
+                if (wy == R(0)) continue;
+                const Node8<R> q = g.gat[col + b];
+                const R u[3] = {q.b.x - duc.x, q.b.y - duc.y, q.b.z - duc.z};
+                T[0] += wy * q.a.x; T[1] += wy * q.a.y; T[2] += wy * q.a.z;
+#pragma unroll
+                for (int k = 0; k < D; ++k) { A[k] += wy * u[k]; B[k] += gy * u[k]; }
+            }
+            const R wxz = wx * wz, gxz = w[0].dN[a] * wz;
+#pragma unroll
+            for (int k = 0; k < D; ++k) tT[k] += wxz * T[k];
+            if (D == 2) {
+                dF[0] += gxz * A[0]; dF[1] += wxz * B[0];
+                dF[2] += gxz * A[1]; dF[3] += wxz * B[1];
+            } else {
+                const R xdz = wx * gz;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    dF[3 * k + 0] += gxz * A[k];
+                    dF[3 * k + 1] += wxz * B[k];
+                    dF[3 * k + 2] += xdz * A[k];
                 }
             }
+        }
+    }
     R s[6], vol;
     update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol);
     if (FUSE) {

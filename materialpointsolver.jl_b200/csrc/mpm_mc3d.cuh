@@ -32,7 +32,7 @@ struct Inv {
     double dev[6];
 };
 
-__device__ __forceinline__ void invariants(const double *s, Inv &v) {
+__host__ __device__ __forceinline__ void invariants(const double *s, Inv &v) {
     const double sm = (s[0] + s[1] + s[2]) / 3.0;
     v.sm = sm;
     const double d0 = s[0] - sm, d1 = s[1] - sm, d2 = s[2] - sm;
@@ -57,7 +57,7 @@ struct Par {
     double sphi, cphi, tphi, tpsi;
 };
 
-__device__ __forceinline__ int yield(const Inv &v, const Par &p, double &ft, double &fs) {
+__host__ __device__ __forceinline__ int yield(const Inv &v, const Par &p, double &ft, double &fs) {
     const double r23 = sqrt(2.0 / 3.0), r15 = sqrt(1.5), r3 = sqrt(3.0);
     ft = r23 * cos(v.theta) * v.rho + v.epsilon / r3 - p.st;
     fs = r15 * v.rho * (sin(v.theta + PI / 3.0) / (r3 * p.cphi) + cos(v.theta + PI / 3.0) * p.tphi / 3.0) +
@@ -76,7 +76,7 @@ __device__ __forceinline__ int yield(const Inv &v, const Par &p, double &ft, dou
 }
 
 // df/dsigma, dg/dsigma (Voigt, engineering shear) and dg/dq for the given mode.
-__device__ __forceinline__ void gradients(int type, const Inv &v, const Par &p, double *df, double *dg,
+__host__ __device__ __forceinline__ void gradients(int type, const Inv &v, const Par &p, double *df, double *dg,
                                           double &dg_dq) {
     const double r23 = sqrt(2.0 / 3.0), r15 = sqrt(1.5), r3 = sqrt(3.0);
     const double th = v.theta, rho = v.rho;
@@ -166,7 +166,7 @@ __device__ __forceinline__ void gradients(int type, const Inv &v, const Par &p, 
 }
 
 // y = D_e x, isotropic elasticity with engineering shear
-__device__ __forceinline__ void De_mul(const Par &p, const double *x, double *y) {
+__host__ __device__ __forceinline__ void De_mul(const Par &p, const double *x, double *y) {
     const double Dt = p.K + 4.0 / 3.0 * p.G, Dd = p.K - 2.0 / 3.0 * p.G;
     y[0] = Dt * x[0] + Dd * x[1] + Dd * x[2];
     y[1] = Dd * x[0] + Dt * x[1] + Dd * x[2];
@@ -174,20 +174,24 @@ __device__ __forceinline__ void De_mul(const Par &p, const double *x, double *y)
     y[3] = p.G * x[3]; y[4] = p.G * x[4]; y[5] = p.G * x[5];
 }
 
-__device__ __forceinline__ double dot6(const double *a, const double *b) {
+__host__ __device__ __forceinline__ double dot6(const double *a, const double *b) {
     return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3] + a[4] * b[4] + a[5] * b[5];
 }
 
 // s: trial stress (in/out); s0: rotated pre-increment stress; de: strain
-// increment (engineering shear); epsq: accumulated plastic shear strain.
-// Returns whether the trial stress yielded (s and epsq changed).
-static __device__ __noinline__ bool mohr_coulomb_3d(double *s, const double *s0, const double *de, double &epsq,
-                                             const Par p) {
+// increment (engineering shear).  Returns whether the trial stress yielded
+// (s changed) and the increment of the accumulated plastic shear strain epsq.
+struct Ret {
+    double dq;
+    int yielded;
+};
+static __host__ __device__ __noinline__ Ret mohr_coulomb_3d(double *s, const double *s0, const double *de,
+                                                            const Par p) {
     Inv v;
     double ft, fs;
     invariants(s, v);
     const int type_tr = yield(v, p, ft, fs);
-    if (type_tr == ELASTIC) return false;
+    if (type_tr == ELASTIC) return Ret{0.0, 0};
     double df[6], dg[6], Ddf[6], Ddg[6], dq;
     gradients(type_tr, v, p, df, dg, dq);
     De_mul(p, df, Ddf);
@@ -233,8 +237,7 @@ static __device__ __noinline__ bool mohr_coulomb_3d(double *s, const double *s0,
     }
 #pragma unroll
     for (int k = 0; k < 6; ++k) s[k] = u[k];
-    epsq += dpq;
-    return true;
+    return Ret{dpq, 1};
 }
 
 }  // namespace mc3d

@@ -88,7 +88,7 @@ def column_collapse_2d(*, h=0.005, ppc=2, seed=1001, jitter=0.1, width=0.2, heig
 def column_collapse_3d(*, h=0.005, ppc=2, seed=1002, jitter=0.1, column=(0.5, 0.2, 0.4),
                        domain=(1.2, 0.4, 0.6), pad=2, precision="FP64", constitutive="mohrcoulomb",
                        E=1.0e6, nu=0.3, rho=2650.0, phi_deg=30.0, c=0.0, psi_deg=0.0, gravity=-9.81,
-                       Ttol=1.0, cfl=0.2, gpu_precision="mixed", mc3d="literal", project_path="/tmp",
+                       Ttol=1.0, cfl=0.2, gpu_precision="mixed", mc3d="literal", project_path="/tmp", sigt=0.0,
                        **extra):
     """3D granular column collapse.  Defaults: domain 1.2 x 0.4 x 0.6 m
     (z up), h = 5 mm, 2x2x2 particles per cell in a 0.5 x 0.2 x 0.4 m column
@@ -115,7 +115,7 @@ def column_collapse_3d(*, h=0.005, ppc=2, seed=1002, jitter=0.1, column=(0.5, 0.
                       NIC=27)
     mp = UserParticle3D(ϵ=precision, NIC=27, dx=lp, dy=lp, dz=lp, ξ=pts, ρs=np.full(npart, rho))
     attr = UserProperty(ϵ=precision, nid=np.ones(npart, np.int64), ν=[nu], Es=[E], Gs=[G], Ks=[K],
-                        σt=[0.0], ϕ=[math.radians(phi_deg)], ϕr=[0.0], ψ=[math.radians(psi_deg)],
+                        σt=[sigt], ϕ=[math.radians(phi_deg)], ϕr=[0.0], ψ=[math.radians(psi_deg)],
                         c=[c], cr=[0.0], Hp=[0.0])
     # boundary flags per node, built from the node coordinates without forming grid.ξ
     nnx, nny, nnz = grid.nnx, grid.nny, grid.nnz

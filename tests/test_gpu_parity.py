@@ -89,21 +89,44 @@ def test_steps_3d(pkg, orc, gpu_lib, prec, tol, model):
     check_fields(out, o, case.mp, tol, tol_stress(tol))
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
-def test_mc3d_restated(pkg, orc, gpu_lib, prec, tol):
+def mc3d_case(pkg, prec):
+    """Cohesive Mohr-Coulomb column (c = 500 Pa, σt = 200 Pa) with a seeded
+    compressive prestress near the yield surface, so that almost every particle
+    yields in the first steps, away from the cone apex.  (For c = 0 and σt = 0
+    the restated return is singular at the apex, ρ -> 0 with a zero-offset
+    tension potential: particles at the free surface then get arbitrary plastic
+    multipliers in the oracle as well, so that case carries no parity.)"""
+    case = small3d(pkg, constitutive="mohrcoulomb", mc3d="restated", gpu_precision=prec, c=500.0, sigt=200.0)
+    rng = np.random.default_rng(77)
+    n = case.mp.np
+    case.mp.sig[:, :3] = rng.normal(-4000.0, 1500.0, (n, 3))
+    case.mp.sig[:, 3:] = rng.normal(0.0, 1000.0, (n, 3))
+    return case
+
+
+# The restated return is discontinuous at the yield surface: its first
+# corrector takes the multiplier from the pre-increment stress when that stress
+# is within 0.1 Pa of the surface, else from the trial stress, and the two
+# land on different points of the surface.  A returned stress stored in FP32
+# (as the mixed mode stores every particle stress) moves by ~1e-4 Pa and flips
+# that choice for a fraction of the particles on their next yielding step:
+# returning a seeded set of on-surface states once from the FP64 value and once
+# from its FP32 rounding gives next-step stresses that differ by 9e-4 relative
+# on average and up to 0.29 at worst.  The mixed mode is therefore held to
+# 2e-2 on this case; the FP64 mode shows the device return itself is exact.
+MC3D_MIXED_TOL = 2e-2
+
+
+@pytest.mark.parametrize("tiled", [False, True])
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", MC3D_MIXED_TOL)])
+def test_mc3d_restated(pkg, orc, gpu_lib, prec, tol, tiled):
     """The restated 3D Mohr-Coulomb return (FP64 on the device in both modes)
-    against the oracle's restatement, over steps where most particles yield."""
-    case = small3d(pkg, constitutive="mohrcoulomb", mc3d="restated", gpu_precision=prec)
-    out, o = run_both(pkg, orc, case, 20)
-    assert (o.epsq > 0).mean() > 0.5
-    check_fields(out, o, case.mp, tol, tol_stress(tol))
-
-
-@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
-def test_mc3d_restated_tiled(pkg, orc, gpu_lib, prec, tol):
-    case = small3d(pkg, constitutive="mohrcoulomb", mc3d="restated", gpu_precision=prec)
-    out, o = run_both(pkg, orc, case, 20, tiled=True)
-    check_fields(out, o, case.mp, tol, tol_stress(tol))
+    against the oracle's restatement, over steps where almost all particles
+    yield."""
+    case = mc3d_case(pkg, prec)
+    out, o = run_both(pkg, orc, case, 20, tiled=tiled)
+    assert (o.epsq > 0).mean() > 0.9
+    check_fields(out, o, case.mp, tol, tol)
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
