@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mc3d", default="literal", choices=["literal", "restated"])
+    ap.add_argument("--workload", default="column3d", choices=["column3d", "slope3d"],
+                    help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
+                         "3D slope with a lognormal cohesion field")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W warm-up + K device steps (the command profilers wrap)")
     return ap.parse_args()
@@ -120,10 +123,20 @@ def replica_value(world, npart, steps, t_max_ms):
     return world * npart * steps / (t_max_ms * 1e-3)
 
 
-def make_case(mc3d):
+WORKLOADS = {
+    "column3d": {"workload": "3D granular column collapse, uGIMP, MUSL va=:a", "constitutive": "mohrcoulomb"},
+    "slope3d": {"workload": "3D slope failure with a lognormal cohesion field, uGIMP, MUSL va=:a",
+                "constitutive": "druckerprager"},
+}
+
+
+def make_case(mc3d, workload="column3d"):
     import __graft_entry__ as g
     pkg = g.load_package()
-    case = pkg.workloads.column_collapse_3d(mc3d=mc3d)
+    if workload == "slope3d":
+        case = pkg.workloads.slope_3d()
+    else:
+        case = pkg.workloads.column_collapse_3d(mc3d=mc3d)
     return pkg, case
 
 
@@ -146,7 +159,9 @@ def pin_particles(mp):
         setattr(mp, name, b)
 
 
-# algorithmic bytes (SURVEY-style accounting)
+G2P_TRAFFIC_PER_PARTICLE = 242.9   # B, dram__bytes_read.sum + dram__bytes_write.sum / np
+
+# algorithmic bytes per particle / per active node
 BP_STEP_3D = 212       # particle state read + written once per step
 BN_STEP_3D = 156       # compulsory grid traffic per active node per step
 BP_G2P_3D = 200        # fused G2P+stress+P2G kernel: its own particle bytes
@@ -155,7 +170,7 @@ BN_G2P_3D = 40         # Δu read (3 floats) + m, p, f written (7 floats)
 
 def run_b200(args):
     rank, world, local = dist_env()
-    pkg, case = make_case(args.mc3d)
+    pkg, case = make_case(args.mc3d, args.workload)
     lib = pkg._lib
     use_dist = world > 1
     if use_dist:
@@ -223,26 +238,20 @@ def run_b200(args):
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
     step_bytes = npart * BP_STEP_3D + na * BN_STEP_3D
     step_achieved = step_bytes / (ms * 1e-3 / K) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "g2p_p2g_traffic.json")
-    if os.path.exists(tp):
-        try:
-            tj = json.load(open(tp))
-            traffic = tj["bytes_per_particle"] * npart + tj.get("bytes_per_active_node", 0) * na
-        except (OSError, KeyError, ValueError):
-            traffic = None
+    # DRAM bytes (read + write) per launch of the fused kernel from one ncu
+    # capture of this workload (profiles/k_g2p_column3d_2.56M.md), per particle
+    traffic = G2P_TRAFFIC_PER_PARTICLE * npart if args.workload == "column3d" else None
 
     result = {
         "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": t_max / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded lattice + jitter, seed 1002)",
-        "config": {"workload": "3D granular column collapse, uGIMP, MUSL va=:a",
-                   "particles": npart, "nodes": case.grid.ni, "active_nodes": na,
-                   "h": case.meta["h"], "constitutive": "mohrcoulomb", "mc3d": args.mc3d,
-                   "precision": "FP32 bulk, FP64 positions and det(F)",
-                   "sort_every": 8, "l2": "particle state 0.5 GB > 126 MB L2 (no flush needed)",
-                   "parallelism": f"replicas x{world}"},
+        "data": f"synthetic (seeded lattice + jitter, seed {case.meta['seed']})",
+        "config": dict(WORKLOADS[args.workload],
+                       particles=npart, nodes=case.grid.ni, active_nodes=na, h=case.meta["h"],
+                       mc3d=args.mc3d, precision="FP32 bulk, FP64 positions and det(F)", sort_every=8,
+                       l2=f"particle state {npart * 212 / 1e9:.2f} GB > 126 MB L2 (no flush needed)",
+                       parallelism=f"replicas x{world}"),
         "gpu_launches": launches,
         "kernel_ms": {k: v[0] for k, v in kt.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,

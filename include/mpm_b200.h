@@ -217,6 +217,17 @@ int mpm_download_grid(mpm_handle *h, int32_t field, double *out);
 int mpm_cell_order_noalloc(const mpm_desc *d, const double *x, const double *y, const double *z,
                            int64_t *order_out, int64_t *p2c_out, void *stream);
 
+/* ---- random fields (grf_gc! / grf_ec!, src/toolkits/randomfield.jl:57-96, 112-150) ----
+ * Evaluates the randomised-spectral sum of those functions on the device, FP64:
+ *   out[i] = scale * sum_j ( a_j sin(V_j . p_i) + b_j cos(V_j . p_i) ),
+ * p_i = (x[i], y[i], z[i]) (z may be NULL: 0), harm = nh rows of
+ * (V1, V2, V3, a, b), row-major.  The caller draws the harmonics (the
+ * reference's rand/randn loop) and applies the final rescaling.  x, y, z,
+ * harm and out are HOST arrays; the call is synchronous.  Errors:
+ * mpm_last_error(NULL). */
+int mpm_grf_eval(int32_t device, const double *x, const double *y, const double *z, int64_t np,
+                 const double *harm, int64_t nh, double scale, double *out);
+
 /* ---- diagnostics ---- */
 /* sizeof(mpm_desc), sizeof(mpm_view), sizeof(mpm_host_views), sizeof(mpm_stats):
  * lets a binding verify its struct layouts against the library's. */

@@ -8,6 +8,7 @@ from .types import (Args2D, Args3D, Grid2D, Grid3D, Particle2D, Particle3D, Prop
                     UserParticle2D, UserParticle3D, UserProperty, UserVBoundary2D,
                     UserVBoundary3D, meshbuilder, jl_range)
 from . import workloads
+from . import randomfield
 from . import _lib
 from .solver import (DeviceModel, host2device, device2host, clean_device, procedure,
                      materialpointsolver, time_sequence)

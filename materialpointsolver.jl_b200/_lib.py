@@ -35,6 +35,7 @@ EXPORTS = [
     "mpm_download", "mpm_compute_p2c", "mpm_download_order", "mpm_sort", "mpm_run_stages",
     "mpm_download_grid", "mpm_get_stats", "mpm_last_error", "mpm_peak_bandwidth",
     "mpm_set_profiling", "mpm_get_kernel_times", "mpm_abi_sizes", "mpm_cell_order_noalloc",
+    "mpm_grf_eval",
 ]
 NOALLOC_MAX_PARTICLES = 1 << 19
 NOALLOC_MAX_KEYS = 1 << 19
@@ -82,6 +83,9 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
               "-Xcompiler", "-fPIC", "-shared"]
 
 
+TRANSLATION_UNITS = ["mpm_b200.cu", "mpm_noalloc.cu", "mpm_grf.cu"]
+
+
 def sources():
     return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
             if f.endswith((".cu", ".cuh"))] + [os.path.join(INCLUDE, "mpm_b200.h")]
@@ -94,8 +98,7 @@ def build(force=False, verbose=False):
             and all(os.path.getmtime(LIB_PATH) >= os.path.getmtime(s) for s in srcs)):
         return LIB_PATH
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB_PATH, os.path.join(CSRC, "mpm_b200.cu"),
-                                 os.path.join(CSRC, "mpm_noalloc.cu")]
+    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB_PATH] + [os.path.join(CSRC, f) for f in TRANSLATION_UNITS]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)
@@ -136,6 +139,8 @@ def lib():
                                        C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]
     L.mpm_abi_sizes.argtypes = [C.POINTER(C.c_int64)] * 4
     L.mpm_cell_order_noalloc.argtypes = [C.POINTER(Desc)] + [C.c_void_p] * 6
+    L.mpm_grf_eval.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                               C.c_double, C.c_void_p]
     sizes = [C.c_int64() for _ in range(4)]
     L.mpm_abi_sizes(*[C.byref(x) for x in sizes])
     mine = [C.sizeof(Desc), C.sizeof(View), C.sizeof(HostViews), C.sizeof(Stats)]

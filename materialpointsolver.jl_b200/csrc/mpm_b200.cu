@@ -56,6 +56,7 @@ struct mpm_handle {
     int dev = 0;
     bool fp64 = false;
     bool uploaded = false;
+    bool coh_mode = false;   // per-particle cohesion (materials differ only in c)
     bool acc_valid = false;     // grid accumulators hold the P2G of the current particles
     double acc_Ti = 0.0;
     int64_t steps_done = 0, sorts_done = 0, since_sort = 1 << 30;
@@ -127,6 +128,8 @@ template <int D, typename R> PDev<D, R> pdev_from(mpm_handle *h, int which) {
     P.vol = (R *)take(sizeof(R));
     P.mat = (uint32_t *)take(4);
     P.orig = (uint32_t *)take(4);
+    R *coh = (R *)take(sizeof(R));
+    P.coh = h->coh_mode ? coh : nullptr;
     return P;
 }
 
@@ -140,7 +143,7 @@ size_t pbuf_bytes(int D, bool fp64, int64_t np) {
     add(R, NV);
     add(R, D * D);
     add(R, NV);
-    add(R, 6);
+    add(R, 7);
     add(4, 2);
     return per;
 }
@@ -292,7 +295,7 @@ void download_col(mpm_handle *h, const S *src, const uint32_t *orig, const mpm_v
 
 // ---- materials ---------------------------------------------------------------------
 template <typename R> void build_materials(mpm_handle *h, const mpm_host_views *v) {
-    const int64_t nm = h->d.nmat;
+    const int64_t nm = h->coh_mode ? 1 : h->d.nmat;
     std::vector<Mat<R>> M(nm);
     auto get = [&](const mpm_view &vw, int64_t i) { return vw.ptr ? view_get(vw, i, 0) : 0.0; };
     for (int64_t i = 0; i < nm; ++i) {
@@ -316,6 +319,7 @@ template <typename R> void build_materials(mpm_handle *h, const mpm_host_views *
         m.dq = (R)std::sqrt(0.333333 + 0.222222 * qpsi * qpsi);
         m.sphi = (R)std::sin(phi); m.cphi = (R)std::cos(phi); m.tphi = (R)std::tan(phi);
         m.spsi = (R)std::sin(psi); m.tpsi = (R)std::tan(psi);
+        m.kc = (R)((6.0 * std::cos(phi)) / (1.732051 * (3.0 + std::sin(phi))));
     }
     CK(cudaMemcpy(h->mat, M.data(), nm * sizeof(Mat<R>), cudaMemcpyHostToDevice));
 }
@@ -524,6 +528,21 @@ template <int D, typename R> struct Upload {
         req(v->Omega, "Omega");
         req(v->rho, "rho");
         req(v->nid, "nid");
+        // Materials that differ only in cohesion (the reference's way of
+        // giving every particle its own random-field cohesion: nid = 1:np,
+        // property.jl:62-63) are stored as one record plus a per-particle c.
+        h->coh_mode = false;
+        if (h->d.nmat > 1 && v->c.ptr) {
+            bool same = true;
+            const mpm_view *others[] = {&v->Ks, &v->Gs, &v->phi, &v->psi, &v->sigt, &v->Hp, &v->cr};
+            for (const mpm_view *o : others) {
+                if (!o->ptr) continue;
+                const double a0 = view_get(*o, 0, 0);
+                for (int64_t k = 1; k < h->d.nmat && same; ++k) same = view_get(*o, k, 0) == a0;
+            }
+            h->coh_mode = same;
+        }
+        P = pdev_from<D, R>(h, 0);
         if (np) {
             for (int d = 0; d < D; ++d) upload_col<double>(h, v->xi, d, P.x[d], np);
             for (int d = 0; d < D; ++d) upload_col<R>(h, v->vs, d, P.v[d], np);
@@ -555,6 +574,13 @@ template <int D, typename R> struct Upload {
                     int64_t q = view_geti(v->nid, i);
                     if (q < 1 || q > h->d.nmat) throw Err{MPM_E_ARG, "nid out of range 1..nmat"};
                     mid[i] = (uint32_t)(q - 1);
+                }
+                if (h->coh_mode) {
+                    // one shared material record; the cohesion travels with the particle
+                    std::vector<R> coh(np);
+                    for (int64_t i = 0; i < np; ++i) coh[i] = (R)view_get(v->c, mid[i], 0);
+                    CK(cudaMemcpy(P.coh, coh.data(), np * sizeof(R), cudaMemcpyHostToDevice));
+                    std::fill(mid.begin(), mid.end(), 0u);
                 }
                 CK(cudaMemcpy(P.mat, mid.data(), np * 4, cudaMemcpyHostToDevice));
             }

@@ -187,7 +187,8 @@ template <typename R> struct Mat {
     R c, phi, psi, sigt, Hp, cr;
     R kphi, qphi, qpsi, st, ab, tb, dq;   // Drucker-Prager (druckerprager.jl:39-44, 59)
     R sphi, cphi, tphi, spsi, tpsi;       // Mohr-Coulomb
-    R pad[2];
+    R kc;                                 // kphi per unit cohesion
+    R pad;
 };
 
 // liE!, src/materials/linearelastic.jl:22-69 (2D) / :78-140 (3D).  s: Voigt

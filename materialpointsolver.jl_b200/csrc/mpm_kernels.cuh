@@ -44,6 +44,7 @@ template <int D, typename R> struct PDev {
     R *epsq, *epsk, *epsv;
     R *m, *vol0, *vol;
     uint32_t *mat, *orig;
+    R *coh;   // per-particle cohesion (random-field materials), else NULL
 };
 
 template <typename R> struct alignas(2 * sizeof(typename Vec<R>::T4)) Node8 {
@@ -550,7 +551,16 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
     vol = (R)(J * (double)ldcs(P.vol0 + i));
     stcs(P.vol + i, vol);
     // stress: liE! then dpP! / mcP! (OS_MUSL.jl:82-96)
-    const Mat<R> M = g.mat[ldcs(P.mat + i)];
+    Mat<R> M = g.mat[ldcs(P.mat + i)];
+    if (P.coh) {
+        // one material per particle differing only in cohesion (a random
+        // field): the cohesion-dependent constants of druckerprager.jl:39-44
+        const R c = ldcs(P.coh + i);
+        M.c = c;
+        M.kphi = c * M.kc;
+        M.st = fmin(M.sigt, M.kphi / M.qphi);
+        M.tb = M.kphi - M.qphi * M.st;
+    }
     R srot[6];
 #pragma unroll
     for (int k = 0; k < NV; ++k) s[k] = ldcs(P.sig[k] + i);

@@ -266,6 +266,7 @@ __global__ void k_permute(PDev<D, R> src, PDev<D, R> dst, const uint2 *pairs, in
     dst.epsq[k] = src.epsq[o]; dst.epsk[k] = src.epsk[o]; dst.epsv[k] = src.epsv[o];
     dst.m[k] = src.m[o]; dst.vol0[k] = src.vol0[o]; dst.vol[k] = src.vol[o];
     dst.mat[k] = src.mat[o];
+    if (src.coh) dst.coh[k] = src.coh[o];
     dst.orig[k] = pr.x;
 }
 

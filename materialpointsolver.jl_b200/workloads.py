@@ -144,3 +144,84 @@ def small_column_3d(**kw):
     base = dict(h=0.02, column=(0.2, 0.1, 0.16), domain=(0.4, 0.16, 0.24), seed=1002)
     base.update(kw)
     return column_collapse_3d(**base)
+
+
+def slope_points_3d(h, ppc, height, crest, slope_deg, width, rng, jitter=0.1):
+    """Lattice particles (lp = h/ppc, seeded jitter) filling a slope of the given
+    height against the x = 0 wall: a crest of length `crest`, then a face at
+    `slope_deg` down to the toe, over the full width in y (z up)."""
+    lp = h / ppc
+    tb = math.tan(math.radians(slope_deg))
+    x_toe = crest + height / tb
+    xs = jl_range(lp / 2, lp, x_toe - lp / 2)
+    ys = jl_range(lp / 2, lp, width - lp / 2)
+    zs = jl_range(lp / 2, lp, height - lp / 2)
+    pts = meshbuilder(xs, ys, zs)
+    keep = pts[:, 0] <= crest + (height - pts[:, 2]) / tb
+    pts = pts[keep]
+    pts += rng.uniform(-jitter * h, jitter * h, size=pts.shape)
+    return pts
+
+
+def slope_3d(*, h=0.1, ppc=2, seed=1003, jitter=0.1, domain=(100.0, 20.0, 40.0), height=6.0, crest=4.05,
+             slope_deg=35.0, pad=2, precision="FP64", E=20.0e6, nu=0.3, rho=2000.0, phi_deg=25.0, psi_deg=0.0,
+             c_mean=10.0e3, c_cov=0.3, corr_len=2.0, nh=5000, k_m=100.0, field=True, gravity=-9.81,
+             Ttol=10.0, Te=1.0, cfl=0.2, gpu_precision="mixed", project_path="/tmp", device=0, **extra):
+    """3D slope failure: a 35° slope of height 6 m and crest 4.05 m against the
+    x = 0 wall, 20 m wide, in a 100 x 20 x 40 m domain at h = 0.1 m with 2x2x2
+    particles per cell (8 000 particles per m^3): 50 m^2 x 20 m = 1 000 m^3, so
+    about 8.0 M particles.  Drucker-Prager φ = 25°, ψ = 0, E = 20 MPa, ν = 0.3,
+    ρ = 2000, gravity ramped over Te = 1 s, 10 s simulated.  Cohesion is a
+    lognormal random field (mean 10 kPa, CoV 0.3) over a Gaussian-covariance
+    field of correlation length 2 m (grf_gc's randomised spectral method with
+    5 000 harmonics, standardised to N(0, 1)), one material per particle like
+    the reference expresses a random field (nid = 1:np).  field=False gives the
+    uniform mean cohesion instead.  Boundaries: floor fixed, x and y walls
+    free-slip."""
+    from . import randomfield
+    K, G = elastic_constants(E, nu)
+    dt = cfl_dt(h, K, G, rho, cfl)
+    lp = h / ppc
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pts = slope_points_3d(h, ppc, height, crest, slope_deg, domain[1], rng, jitter)
+    npart = pts.shape[0]
+    if field:
+        Z = randomfield.grf_gc(np.empty(npart), pts, 0.0, 1.0, If=corr_len, k_m=k_m, Nh=nh, seed=seed,
+                               rescale="standard", device=device)
+        coh = randomfield.lognormal(Z, c_mean, c_cov)
+        nid = np.arange(1, npart + 1, dtype=np.int64)
+    else:
+        coh = np.array([c_mean])
+        nid = np.ones(npart, np.int64)
+    nm = coh.shape[0]
+
+    def full(v):
+        return np.full(nm, v, dtype=np.float64)
+
+    akw = dict(Ttol=Ttol, Te=Te, ΔT=dt, FLIP=1, PIC=0, constitutive="druckerprager", basis="uGIMP",
+               device="B200", coupling="OS", scheme="MUSL", va="a", gravity=gravity, ζs=0,
+               project_name="slope3d", project_path=project_path, ϵ=precision, gpu_precision=gpu_precision,
+               make_project_dir=False)
+    akw.update(extra)
+    args = UserArgs3D(**akw)
+    grid = UserGrid3D(ϵ=precision, x1=-pad * h, x2=domain[0] + pad * h, y1=-pad * h, y2=domain[1] + pad * h,
+                      z1=-pad * h, z2=domain[2] + pad * h, dx=h, dy=h, dz=h, NIC=27)
+    mp = UserParticle3D(ϵ=precision, NIC=27, dx=lp, dy=lp, dz=lp, ξ=pts, ρs=np.full(npart, rho))
+    attr = UserProperty(ϵ=precision, nid=nid, ν=full(nu), Es=full(E), Gs=full(G), Ks=full(K), σt=full(0.0),
+                        ϕ=full(math.radians(phi_deg)), ϕr=full(0.0), ψ=full(math.radians(psi_deg)), c=coh,
+                        cr=full(0.0), Hp=full(0.0))
+    nnx, nny, nnz = grid.nnx, grid.nny, grid.nnz
+    eps = 1e-9 * h
+    vx, vy, vz = grid._vx, grid._vy, grid._vz
+    bx = ((vx <= eps) | (vx >= domain[0] - eps))
+    by = ((vy <= eps) | (vy >= domain[1] - eps))
+    bz = (vz <= eps)
+    fx = np.broadcast_to(bx[None, :, None] | bz[:, None, None], (nnz, nnx, nny)).ravel().astype(np.int64)
+    fy = np.broadcast_to(by[None, None, :] | bz[:, None, None], (nnz, nnx, nny)).ravel().astype(np.int64)
+    fz = np.broadcast_to(bz[:, None, None], (nnz, nnx, nny)).ravel().astype(np.int64)
+    zeros = np.zeros(grid.ni)
+    bc = UserVBoundary3D(ϵ=precision, vx_s_idx=fx, vx_s_val=zeros, vy_s_idx=fy, vy_s_val=zeros,
+                         vz_s_idx=fz, vz_s_val=zeros)
+    nsteps = int(math.ceil(Ttol / dt))
+    return Case("slope_3d", args, grid, mp, attr, bc, dt, nsteps,
+                dict(np=npart, h=h, K=K, G=G, seed=seed, cohesion=coh if field else None))

@@ -316,3 +316,17 @@ def test_entry_point_matches_oracle(pkg, orc, gpu_lib):
     assert rel(case.mp.xi - mp0.xi, o.xi - mp0.xi) < TOL64
     assert rel(case.mp.sig, o.sig) < TOL64
     assert rel(case.mp.ms, o.ms) < 1e-12
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+def test_slope_random_cohesion(pkg, orc, gpu_lib, prec, tol):
+    """3D slope with one material per particle whose cohesion is a lognormal
+    random field (the reference's nid = 1:np form).  The library stores it as
+    one material record plus a per-particle cohesion that travels through the
+    cell sort; the oracle keeps the 3 184 material records."""
+    case = pkg.workloads.slope_3d(h=0.5, domain=(20.0, 4.0, 10.0), height=3.0, crest=2.0, corr_len=1.0, nh=500,
+                                  Te=0.0, gpu_precision=prec, seed=31, sort_every=4)
+    assert len(case.attr.c) == case.mp.np and np.ptp(case.attr.c) > 0
+    out, o = run_both(pkg, orc, case, 20)
+    assert (o.epsq > 0).mean() > 0.05
+    check_fields(out, o, case.mp, tol, tol_stress(tol))
