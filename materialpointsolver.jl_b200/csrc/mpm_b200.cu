@@ -49,6 +49,15 @@ struct KTimer {
 
 }  // namespace
 
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    double dt = 0;
+    void *pbuf0 = nullptr;
+    int sort_every = 0;
+    bool tiled = false;
+    int64_t launches = 0, steps = 0, sorts = 0;
+};
+
 struct mpm_handle {
     mpm_desc d{};
     std::string last_error;
@@ -57,6 +66,9 @@ struct mpm_handle {
     bool fp64 = false;
     bool uploaded = false;
     bool coh_mode = false;   // per-particle cohesion (materials differ only in c)
+    bool use_graphs = true;  // replay captured step blocks (MPM_B200_GRAPHS=0 turns it off)
+    GraphCache graph;
+    int64_t graph_launches = 0;
     bool acc_valid = false;     // grid accumulators hold the P2G of the current particles
     double acc_Ti = 0.0;
     int64_t steps_done = 0, sorts_done = 0, since_sort = 1 << 30;
@@ -71,7 +83,9 @@ struct mpm_handle {
     void *acc = nullptr, *gat = nullptr, *gvs = nullptr;   // node records (see mpm_kernels.cuh)
     uint8_t *bcmask = nullptr;
     void *bcval = nullptr;
-    uint8_t *bflag = nullptr;
+    uint32_t *bflag = nullptr;   // per node block: touched by a particle window
+    uint32_t *blist = nullptr;   // list of the flagged blocks
+    uint32_t *bcount = nullptr;  // its length
     int nbx = 1, nby = 1, nbz = 1;
     int64_t ni = 0;
     void *mat = nullptr;
@@ -182,6 +196,8 @@ template <typename R> GDev<R> gdev_from(mpm_handle *h) {
     g.mat = (const Mat<R> *)h->mat;
     g.err = h->err;
     g.bflag = h->bflag;
+    g.blist = h->blist;
+    g.bcount = h->bcount;
     g.nbx = h->nbx;
     g.nby = h->nby;
     g.nbz = h->nbz;
@@ -412,7 +428,8 @@ template <int D, typename R> void standalone_p2g(mpm_handle *h, double Ti, Launc
     const int64_t np = h->d.np;
     using T4 = typename Vec<R>::T4;
     CK(cudaMemsetAsync(h->acc, 0, h->ni * sizeof(Node8<R>), h->stream));
-    CK(cudaMemsetAsync(h->bflag, 0, (size_t)h->nbx * h->nby * h->nbz, h->stream));
+    CK(cudaMemsetAsync(h->bflag, 0, (size_t)h->nbx * h->nby * h->nbz * 4, h->stream));
+    CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
     PDev<D, R> P = pdev_from<D, R>(h, 0);
     GDev<R> g = gdev_from<R>(h);
     StepParams sp = make_params<D, R>(h, 0.0, Ti, gravity_at(h->d, Ti));
@@ -447,10 +464,91 @@ template <int D, typename R> const TiledCfg &tiled_cfg(mpm_handle *h, int need_v
     return cc;
 }
 
-template <int D, typename R> void run_steps(mpm_handle *h, double dt, double Ti0, int64_t nsteps) {
+// The launches of one step (solve, double mapping, DM3, fused G2P + next P2G).
+template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double dt, double Ti, double Tn) {
     const int64_t np = h->d.np;
-    Launcher L{h};
     const int nblk = h->nbx * h->nby * h->nbz;
+    const int ngrid = std::min(nblk, h->nsm * 16);   // node passes: grid-stride over the active-block list
+    if (h->since_sort >= h->sort_every) do_sort<D, R>(h);
+    PDev<D, R> P = pdev_from<D, R>(h, 0);
+    GDev<R> g = gdev_from<R>(h);
+    StepParams sp = make_params<D, R>(h, dt, Ti, gravity_at(h->d, Tn));
+    const bool mc3 = sp.mc3d && sp.constitutive == MPM_MOHRCOULOMB;
+    L.run("solve", [&] { k_solve<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+    if (h->tiled) {
+        TileList tl{h->tiles, h->ntiles, h->off, h->sg};
+        const TiledCfg &c = tiled_cfg<D, R>(h, sp.need_vs);
+        if (np) L.run("dmap", [&] { k_dmap_tile<D, R><<<c.grid_dm, 256, c.smem_dm, h->stream>>>(P, g, sp, tl); });
+        L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+        CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
+        if (np) L.run("g2p_p2g", [&] {
+            if (mc3) k_g2p_tile<D, R, D == 3><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
+            else k_g2p_tile<D, R><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
+        });
+    } else {
+        if (np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+        CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
+        if (np) L.run("g2p_p2g", [&] {
+            if (mc3) k_g2p<D, R, true, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_g2p<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+        });
+    }
+    h->since_sort++;
+    h->steps_done++;
+}
+
+// Steps after the gravity ramp (Ti >= Te) all launch with the same parameters,
+// so a block of two sort periods -- sort, S steps, sort, S steps, after which
+// the ping-pong particle buffers are back in place -- is captured once into a
+// CUDA graph and replayed.  The capture is keyed on everything baked into the
+// launches; the host bookkeeping of a replay repeats what the capture did.
+template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double Ti) {
+    GraphCache &gc = h->graph;
+    const int S = h->sort_every;
+    const bool match = gc.exec && gc.dt == dt && gc.pbuf0 == h->pbuf[0] && gc.sort_every == S &&
+                       gc.tiled == h->tiled;
+    if (!match) {
+        if (gc.exec) { cudaGraphExecDestroy(gc.exec); gc.exec = nullptr; }
+        if (h->tiled) {   // kernel attributes are set outside the capture
+            tiled_cfg<D, R>(h, 0);
+            tiled_cfg<D, R>(h, 1);
+        }
+        const int64_t l0 = h->launches, s0 = h->steps_done, q0 = h->sorts_done;
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        Launcher L{h};
+        try {
+            for (int k = 0; k < 2 * S; ++k) issue_step<D, R>(h, L, dt, Ti, Ti + dt);
+        } catch (...) {
+            cudaStreamEndCapture(h->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        CK(cudaStreamEndCapture(h->stream, &graph));
+        cudaError_t e = cudaGraphInstantiate(&gc.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) throw Err{MPM_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)};
+        gc.dt = dt;
+        gc.pbuf0 = h->pbuf[0];
+        gc.sort_every = S;
+        gc.tiled = h->tiled;
+        gc.launches = h->launches - l0;
+        gc.steps = h->steps_done - s0;
+        gc.sorts = h->sorts_done - q0;
+        // the capture recorded the work without running it
+    } else {
+        h->launches += gc.launches;
+        h->steps_done += gc.steps;
+        h->sorts_done += gc.sorts;
+    }
+    CK(cudaGraphLaunch(gc.exec, h->stream));
+    h->graph_launches++;
+    return true;
+}
+
+template <int D, typename R> void run_steps(mpm_handle *h, double dt, double Ti0, int64_t nsteps) {
+    Launcher L{h};
     auto next_t = [&](double t) {
         return h->d.time_f32 ? (double)((float)t + (float)dt) : t + dt;
     };
@@ -460,34 +558,19 @@ template <int D, typename R> void run_steps(mpm_handle *h, double dt, double Ti0
         standalone_p2g<D, R>(h, Ti0, L);
     }
     double Ti = Ti0;
-    for (int64_t s = 0; s < nsteps; ++s) {
-        double Tn = next_t(Ti);
-        if (h->since_sort >= h->sort_every) do_sort<D, R>(h);
-        PDev<D, R> P = pdev_from<D, R>(h, 0);
-        GDev<R> g = gdev_from<R>(h);
-        StepParams sp = make_params<D, R>(h, dt, Ti, gravity_at(h->d, Tn));
-        const bool mc3 = sp.mc3d && sp.constitutive == MPM_MOHRCOULOMB;
-        L.run("solve", [&] { k_solve<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-        if (h->tiled) {
-            TileList tl{h->tiles, h->ntiles, h->off, h->sg};
-            const TiledCfg &c = tiled_cfg<D, R>(h, sp.need_vs);
-            if (np) L.run("dmap", [&] { k_dmap_tile<D, R><<<c.grid_dm, 256, c.smem_dm, h->stream>>>(P, g, sp, tl); });
-            L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-            if (np) L.run("g2p_p2g", [&] {
-                if (mc3) k_g2p_tile<D, R, D == 3><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
-                else k_g2p_tile<D, R><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
-            });
-        } else {
-            if (np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
-            L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-            if (np) L.run("g2p_p2g", [&] {
-                if (mc3) k_g2p<D, R, true, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                else k_g2p<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-            });
+    const int64_t block = 2 * (int64_t)h->sort_every;
+    for (int64_t s = 0; s < nsteps;) {
+        if (h->use_graphs && !h->profiling && Ti >= h->d.Te && h->since_sort >= h->sort_every &&
+            nsteps - s >= block) {
+            graph_block<D, R>(h, dt, Ti);
+            for (int64_t k = 0; k < block; ++k) Ti = next_t(Ti);
+            s += block;
+            continue;
         }
+        double Tn = next_t(Ti);
+        issue_step<D, R>(h, L, dt, Ti, Tn);
         Ti = Tn;
-        h->since_sort++;
-        h->steps_done++;
+        ++s;
     }
     h->acc_valid = true;
     h->acc_Ti = Ti;
@@ -739,13 +822,17 @@ template <int D, typename R> struct Stages {
         const int64_t np = h->d.np;
         Launcher L{h};
         const int nblk = h->nbx * h->nby * h->nbz;
+        const int ngrid = std::min(nblk, h->nsm * 16);
         if (mask & 1u) standalone_p2g<D, R>(h, Ti, L);
         PDev<D, R> P = pdev_from<D, R>(h, 0);
         GDev<R> g = gdev_from<R>(h);
         StepParams sp = make_params<D, R>(h, dt, Ti, gravity_at(h->d, Ti));
-        if (mask & 2u) L.run("solve", [&] { k_solve<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+        if (mask & 2u) L.run("solve", [&] { k_solve<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         if ((mask & 4u) && np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
-        if (mask & 8u) L.run("dm3", [&] { k_dm3<D, R><<<nblk, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+        if (mask & 8u) {
+            L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+            CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
+        }
         const bool mc3 = sp.mc3d && sp.constitutive == MPM_MOHRCOULOMB;
         if ((mask & 16u) && np) L.run("g2p", [&] {
             if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
@@ -868,8 +955,11 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
             h->nbx = (int)cdiv(d->nnx, Blk<2>::BX); h->nby = (int)cdiv(d->nny, Blk<2>::BY); h->nbz = 1;
         }
         size_t nblk = (size_t)h->nbx * h->nby * h->nbz;
-        h->bflag = (uint8_t *)dalloc(h, nblk);
-        CK(cudaMemset(h->bflag, 0, nblk));
+        h->bflag = (uint32_t *)dalloc(h, nblk * 4);
+        CK(cudaMemset(h->bflag, 0, nblk * 4));
+        h->blist = (uint32_t *)dalloc(h, nblk * 4);
+        h->bcount = (uint32_t *)dalloc(h, 4);
+        CK(cudaMemset(h->bcount, 0, 4));
         size_t msz = h->fp64 ? sizeof(Mat<double>) : sizeof(Mat<float>);
         h->mat = dalloc(h, d->nmat * msz);
         h->err = (int *)dalloc(h, 4);
@@ -907,6 +997,9 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         // same step.  The per-particle kernels are the faster ones on B200, where
         // shared-memory float atomics are the tiled passes' limiter.
         if (const char *e = getenv("MPM_B200_TILED")) h->tiled = (e[0] == '1');
+        // MPM_B200_GRAPHS=0 issues every step's launches directly instead of
+        // replaying captured blocks of steps.
+        if (const char *e = getenv("MPM_B200_GRAPHS")) h->use_graphs = (e[0] != '0');
         *out = h;
         return MPM_OK;
     } catch (const Err &e) {
@@ -1030,6 +1123,7 @@ int mpm_destroy(mpm_handle *h) {
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (void *p : h->allocs) cudaFree(p);
+    if (h->graph.exec) cudaGraphExecDestroy(h->graph.exec);
     for (auto e : h->kev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);

@@ -62,7 +62,9 @@ template <typename R> struct GDev {
     const T4 *bcval;        // fixed values (NULL when all zero)
     const Mat<R> *mat;
     int *err;
-    uint8_t *bflag;         // per node block: 1 if some particle window touched it
+    uint32_t *bflag;        // per node block: 1 if some particle window touched it
+    uint32_t *blist;        // the flagged blocks, in the order they were flagged
+    uint32_t *bcount;       // number of entries in blist
     int nbx, nby, nbz;      // node blocks per axis (blocks of BX x BY x BZ nodes)
 };
 
@@ -94,6 +96,11 @@ template <int D, typename R> __device__ __forceinline__ void block_range(const G
     }
 }
 
+// Flag node block b and append it to the active-block list the first time.
+template <typename R> __device__ __forceinline__ void mark_block(const GDev<R> &g, int b) {
+    if (g.bflag[b] == 0u && atomicExch(&g.bflag[b], 1u) == 0u) g.blist[atomicAdd(g.bcount, 1u)] = (uint32_t)b;
+}
+
 // Flag the node blocks covered by the windows of the calling lanes.  The
 // active lanes of a warp (neighbouring particles after the cell sort) mark the
 // bounding box of their windows together; a box wider than 64 blocks (lanes
@@ -116,15 +123,13 @@ __device__ __forceinline__ void mark_blocks(const GDev<R> &g, const AxisW<R> *w)
         const int rank = __popc(mask & ((1u << lane) - 1u)), cnt = __popc(mask);
         for (int k = rank; k < total; k += cnt) {
             int by = blo[1] + k % ny, r = k / ny, bx = blo[0] + r % nx, bz = blo[2] + r / nx;
-            int b = (bz * g.nbx + bx) * g.nby + by;
-            if (g.bflag[b] == 0) g.bflag[b] = 1;
+            mark_block<R>(g, (bz * g.nbx + bx) * g.nby + by);
         }
     } else {
         for (int bz = lo[2]; bz <= hi[2]; ++bz)
             for (int bx = lo[0]; bx <= hi[0]; ++bx)
                 for (int by = lo[1]; by <= hi[1]; ++by) {
-                    int b = (bz * g.nbx + bx) * g.nby + by;
-                    if (g.bflag[b] == 0) g.bflag[b] = 1;
+                    mark_block<R>(g, (bz * g.nbx + bx) * g.nby + by);
                 }
     }
 }
@@ -299,10 +304,7 @@ __global__ void __launch_bounds__(256) k_p2g(PDev<D, R> P, GDev<R> g, StepParams
 // (va = :v, utils_OS.jl:507-535, 650-687).  Clears momentum and force.
 // ---------------------------------------------------------------------------
 template <int D, typename R>
-__global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
-    if (g.bflag[blockIdx.x] == 0) return;
-    int i = block_node<D, R>(g, blockIdx.x, threadIdx.x);
-    if (i < 0) return;
+__device__ __forceinline__ void solve_node(const GDev<R> &g, const StepParams &sp, int i) {
     using T4 = typename Vec<R>::T4;
     Node8<R> A = g.acc[i];
     const T4 a0 = A.a, a1 = A.b;
@@ -362,6 +364,16 @@ __global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
     A.a = mk4<R>(m, 0, 0, 0);
     A.b = mk4<R>(0, 0, 0, 0);
     g.acc[i] = A;
+}
+
+// One CTA per active node block, grid-stride over the active-block list.
+template <int D, typename R>
+__global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
+    const uint32_t n = *g.bcount;
+    for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const int i = block_node<D, R>(g, (int)g.blist[k], threadIdx.x);
+        if (i >= 0) solve_node<D, R>(g, sp, i);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -456,12 +468,7 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_dmap(PDev<D, R> P, GDev<R> 
 // momentum, BC, Δus = vs·ΔT (into the second half of the gather record).
 // Clears mass and momentum for the next P2G.
 template <int D, typename R>
-__global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
-    if (g.bflag[blockIdx.x] == 0) return;
-    __syncthreads();
-    if (threadIdx.x == 0) g.bflag[blockIdx.x] = 0;   // re-armed by the next scatter
-    int i = block_node<D, R>(g, blockIdx.x, threadIdx.x);
-    if (i < 0) return;
+__device__ __forceinline__ void dm3_node(const GDev<R> &g, const StepParams &sp, int i) {
     using T4 = typename Vec<R>::T4;
     const T4 a0 = g.acc[i].a;
     uint8_t bm = g.bcmask[i];
@@ -485,6 +492,19 @@ __global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
     }
     g.gat[i].b = mk4<R>(du[0], du[1], du[2], 0);
     g.acc[i].a = mk4<R>(0, 0, 0, 0);
+}
+
+// Clears each processed block's flag (re-armed by the next scatter); the list
+// count is reset by the host right after this launch.
+template <int D, typename R>
+__global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
+    const uint32_t n = *g.bcount;
+    for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const int b = (int)g.blist[k];
+        const int i = block_node<D, R>(g, b, threadIdx.x);
+        if (i >= 0) dm3_node<D, R>(g, sp, i);
+        if (threadIdx.x == 0) g.bflag[b] = 0u;
+    }
 }
 
 // Everything of G2P_OS! after the gathers, plus liE! and dpP!/mcP! and the

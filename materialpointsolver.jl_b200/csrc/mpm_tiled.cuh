@@ -88,8 +88,7 @@ __device__ __forceinline__ void mark_window(const GDev<R> &g, const TileGeo<D> &
     int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
     for (int k = threadIdx.x; k < nx * ny * nz; k += blockDim.x) {
         int by = y0 + k % ny, r = k / ny, bx = x0 + r % nx, bz = z0 + r / nx;
-        int b = (bz * g.nbx + bx) * g.nby + by;
-        if (g.bflag[b] == 0) g.bflag[b] = 1;
+        mark_block<R>(g, (bz * g.nbx + bx) * g.nby + by);
     }
 }
 

@@ -106,27 +106,54 @@ def mc3d_case(pkg, prec):
 
 # The restated return is discontinuous at the yield surface: its first
 # corrector takes the multiplier from the pre-increment stress when that stress
-# is within 0.1 Pa of the surface, else from the trial stress, and the two
-# land on different points of the surface.  A returned stress stored in FP32
-# (as the mixed mode stores every particle stress) moves by ~1e-4 Pa and flips
-# that choice for a fraction of the particles on their next yielding step:
-# returning a seeded set of on-surface states once from the FP64 value and once
-# from its FP32 rounding gives next-step stresses that differ by 9e-4 relative
-# on average and up to 0.29 at worst.  The mixed mode is therefore held to
-# 2e-2 on this case; the FP64 mode shows the device return itself is exact.
-MC3D_MIXED_TOL = 2e-2
+# is within 0.1 Pa of the surface, else from the trial stress, and the two land
+# on different points of the surface.  A returned stress stored in FP32 (as the
+# mixed mode stores every particle stress) moves by ~1e-4 Pa and flips that
+# choice for a fraction of the yielding particles on their next step.  The
+# oracle itself shows it: rounding its stresses to FP32 after every step moves
+# its 20-step result by 4e-3 in displacement and 8e-2 in stress.  The mixed
+# mode is held to twice that self-difference of the oracle, field by field;
+# the FP64 mode shows the device return itself is exact.
+MC3D_FIELDS = ("vs", "sig", "eps", "F", "Omega", "sigm", "epsv", "epsq")
+
+
+def oracle_fp32_stress_spread(pkg, orc, case_fn, nsteps):
+    """Per-field relative difference between the FP64 oracle and the same
+    oracle with its particle stresses rounded to FP32 after every step."""
+    a, b = case_fn(), case_fn()
+    oa = orc.Oracle(a.args, a.grid, a.mp, a.attr, a.bc)
+    oa.run(a.dt, 0.0, nsteps)
+    ob = orc.Oracle(b.args, b.grid, b.mp, b.attr, b.bc)
+    ob.sig[:] = ob.sig.astype(np.float32)
+    Ti = 0.0
+    for _ in range(nsteps):
+        ob.procedure(b.dt, Ti)
+        Ti += b.dt
+        ob.sig[:] = ob.sig.astype(np.float32)
+    spread = {f: rel(getattr(ob, f), getattr(oa, f)) for f in MC3D_FIELDS}
+    spread["disp"] = rel(ob.xi - b.mp.xi, oa.xi - a.mp.xi)
+    return spread
 
 
 @pytest.mark.parametrize("tiled", [False, True])
-@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", MC3D_MIXED_TOL)])
-def test_mc3d_restated(pkg, orc, gpu_lib, prec, tol, tiled):
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_mc3d_restated(pkg, orc, gpu_lib, prec, tiled):
     """The restated 3D Mohr-Coulomb return (FP64 on the device in both modes)
     against the oracle's restatement, over steps where almost all particles
     yield."""
+    nsteps = 20
     case = mc3d_case(pkg, prec)
-    out, o = run_both(pkg, orc, case, 20, tiled=tiled)
+    out, o = run_both(pkg, orc, case, nsteps, tiled=tiled)
     assert (o.epsq > 0).mean() > 0.9
-    check_fields(out, o, case.mp, tol, tol)
+    if prec == "fp64":
+        check_fields(out, o, case.mp, TOL64)
+        return
+    spread = oracle_fp32_stress_spread(pkg, orc, lambda: mc3d_case(pkg, "fp64"), nsteps)
+    got = {f: rel(getattr(out, f), getattr(o, f)) for f in MC3D_FIELDS}
+    got["disp"] = rel(out.xi - case.mp.xi, o.xi - case.mp.xi)
+    for f, err in got.items():
+        bound = max(TOL32, 2.0 * spread[f])
+        assert err < bound, (f, err, bound, spread[f])
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
@@ -325,8 +352,36 @@ def test_slope_random_cohesion(pkg, orc, gpu_lib, prec, tol):
     one material record plus a per-particle cohesion that travels through the
     cell sort; the oracle keeps the 3 184 material records."""
     case = pkg.workloads.slope_3d(h=0.5, domain=(20.0, 4.0, 10.0), height=3.0, crest=2.0, corr_len=1.0, nh=500,
-                                  Te=0.0, gpu_precision=prec, seed=31, sort_every=4)
+                                  Te=0.0, gpu_precision=prec, seed=31, sort_every=4, c_mean=1.0e3)
     assert len(case.attr.c) == case.mp.np and np.ptp(case.attr.c) > 0
     out, o = run_both(pkg, orc, case, 20)
-    assert (o.epsq > 0).mean() > 0.05
+    assert (o.epsq > 1e-9).mean() > 0.2
     check_fields(out, o, case.mp, tol, tol_stress(tol))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_graph_replay_matches_direct_launches(pkg, orc, gpu_lib, dim, monkeypatch):
+    """Steps after the gravity ramp are replayed from captured CUDA graphs in
+    blocks of two sort periods; the same 40 steps issued launch by launch give
+    the same state (FP64 mode: only the order of atomic additions differs), and
+    both match the oracle."""
+    mk = small2d if dim == 2 else small3d
+    outs, stats = [], []
+    for graphs in ("1", "0"):
+        monkeypatch.setenv("MPM_B200_GRAPHS", graphs)
+        case = mk(pkg, constitutive="druckerprager", gpu_precision="fp64")
+        dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+        dev.step(case.dt, 0.0, 40)
+        out = fresh_particles(pkg, case.mp)
+        dev.download(pkg._lib.F_REFERENCE | pkg._lib.F_F, out)
+        stats.append(dev.stats())
+        dev.close()
+        outs.append(out)
+    assert stats[0].steps_done == stats[1].steps_done == 40
+    assert stats[0].sorts_done == stats[1].sorts_done
+    assert stats[0].launches == stats[1].launches
+    for f in ("xi", "vs", "sig", "F"):
+        assert rel(getattr(outs[0], f), getattr(outs[1], f)) < 1e-12, f
+    o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc)
+    o.run(case.dt, 0.0, 40)
+    check_fields(outs[0], o, case.mp, TOL64)
