@@ -41,9 +41,10 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mc3d", default="literal", choices=["literal", "restated"])
-    ap.add_argument("--workload", default="column3d", choices=["column3d", "slope3d"],
+    ap.add_argument("--workload", default="column3d", choices=["column3d", "slope3d", "batch2d"],
                     help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
-                         "3D slope with a lognormal cohesion field")
+                         "3D slope with a lognormal cohesion field; batch2d: 256 independent 2D slopes "
+                         "(15.5 M particles) advanced together, autotuned during warm-up")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W warm-up + K device steps (the command profilers wrap)")
     return ap.parse_args()
@@ -127,6 +128,8 @@ WORKLOADS = {
     "column3d": {"workload": "3D granular column collapse, uGIMP, MUSL va=:a", "constitutive": "mohrcoulomb"},
     "slope3d": {"workload": "3D slope failure with a lognormal cohesion field, uGIMP, MUSL va=:a",
                 "constitutive": "druckerprager"},
+    "batch2d": {"workload": "256 independent 2D slopes in one grid, uGIMP, MUSL va=:a",
+                "constitutive": "druckerprager"},
 }
 
 
@@ -135,6 +138,8 @@ def make_case(mc3d, workload="column3d"):
     pkg = g.load_package()
     if workload == "slope3d":
         case = pkg.workloads.slope_3d()
+    elif workload == "batch2d":
+        case = pkg.workloads.slope_batch_2d()
     else:
         case = pkg.workloads.column_collapse_3d(mc3d=mc3d)
     return pkg, case
@@ -166,6 +171,10 @@ BP_STEP_3D = 212       # particle state read + written once per step
 BN_STEP_3D = 156       # compulsory grid traffic per active node per step
 BP_G2P_3D = 200        # fused G2P+stress+P2G kernel: its own particle bytes
 BN_G2P_3D = 40         # Δu read (3 floats) + m, p, f written (7 floats)
+BP_STEP_2D = 132
+BN_STEP_2D = 108
+BP_G2P_2D = 128
+BN_G2P_2D = 28         # Δu read (2 floats) + m, p, f written (5 floats)
 
 
 def run_b200(args):
@@ -184,7 +193,10 @@ def run_b200(args):
 
     # ---- end to end through the public API: host arrays -> device -> host ----
     pin_particles(case.mp)
-    out = pkg.Particle3D(dx=case.mp.dx, dy=case.mp.dy, dz=case.mp.dz, xi=case.mp.xi, rho=case.mp.rho)
+    if case.grid.dim == 3:
+        out = pkg.Particle3D(dx=case.mp.dx, dy=case.mp.dy, dz=case.mp.dz, xi=case.mp.xi, rho=case.mp.rho)
+    else:
+        out = pkg.Particle2D(dx=case.mp.dx, dy=case.mp.dy, xi=case.mp.xi, rho=case.mp.rho)
     pin_particles(out)
 
     def e2e_once(nsteps):
@@ -198,13 +210,24 @@ def run_b200(args):
 
     e2e_once(W)                       # warm: context, module load, first allocations
     e2e_t = e2e_once(K)
-    h2d = npart * 8 * (3 + 3 + 6 + 6 + 3 + 4 + 9) + npart * 8   # uploaded particle columns (FP64) + nid
-    d2h = npart * 8 * (1 + 3 + 3 + 1 + 6 + 1 + 1 + 1 + 6 + 1)   # device2host! field set (FP64)
+    D = case.grid.dim
+    nv = 6 if D == 3 else 4
+    # uploaded particle columns (FP64: xi, vs, sig, eps, epsq/epsk/epsv, Omega/Omega0/rho/rho0, F) + nid
+    h2d = npart * 8 * (D + D + nv + nv + 3 + 4 + D * D) + npart * 8
+    # device2host! field set (FP64: sigm, vs, xi, Omega, sig, epsk, epsq, epsv, eps, ms)
+    d2h = npart * 8 * (1 + D + D + 1 + nv + 1 + 1 + 1 + nv + 1)
 
     # ---- device-timed region (inputs resident in HBM) ----
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
-    dev.step(dt, 0.0, W)
-    Ti = W * dt
+    tuning = None
+    Ti = 0.0
+    if args.workload == "batch2d":
+        # untimed: the autotuner's trials are real steps of the model
+        Ti, S, tiled, trial_ms = dev.autotune(dt, Ti, 16)
+        tuning = {"sort_every": S, "tiled": tiled, "trial_ms_per_step": trial_ms,
+                  "candidates": "sort period 4/8/16/32 x per-particle/tiled passes, 16 steps each"}
+    dev.step(dt, Ti, W)
+    Ti += W * dt
     if use_dist:
         dist.barrier()
     launches0 = dev.stats().launches
@@ -218,6 +241,8 @@ def run_b200(args):
     Ti += K * dt
     t_max = max_over_ranks(ms, f"cuda:{local}") if use_dist else ms
     value = replica_value(world, npart, K, t_max)
+
+    sort_used, tiled_used = dev.tuning()
 
     # ---- per-kernel device times (events on the library stream) ----
     dev.set_profiling(True)
@@ -234,9 +259,11 @@ def run_b200(args):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    alg_bytes = npart * BP_G2P_3D + na * BN_G2P_3D
+    bp_g2p, bn_g2p = (BP_G2P_3D, BN_G2P_3D) if D == 3 else (BP_G2P_2D, BN_G2P_2D)
+    bp_step, bn_step = (BP_STEP_3D, BN_STEP_3D) if D == 3 else (BP_STEP_2D, BN_STEP_2D)
+    alg_bytes = npart * bp_g2p + na * bn_g2p
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
-    step_bytes = npart * BP_STEP_3D + na * BN_STEP_3D
+    step_bytes = npart * bp_step + na * bn_step
     step_achieved = step_bytes / (ms * 1e-3 / K) / 1e9
     # DRAM bytes (read + write) per launch of the fused kernel from one ncu
     # capture of this workload (profiles/k_g2p_column3d_2.56M.md), per particle
@@ -249,9 +276,11 @@ def run_b200(args):
         "data": f"synthetic (seeded lattice + jitter, seed {case.meta['seed']})",
         "config": dict(WORKLOADS[args.workload],
                        particles=npart, nodes=case.grid.ni, active_nodes=na, h=case.meta["h"],
-                       mc3d=args.mc3d, precision="FP32 bulk, FP64 positions and det(F)", sort_every=8,
-                       l2=f"particle state {npart * 212 / 1e9:.2f} GB > 126 MB L2 (no flush needed)",
-                       parallelism=f"replicas x{world}"),
+                       mc3d=args.mc3d, precision="FP32 bulk, FP64 positions and det(F)", sort_every=sort_used,
+                       particle_passes="tiled" if tiled_used else "per-particle",
+                       l2=f"particle state {npart * bp_step / 1e9:.2f} GB > 126 MB L2 (no flush needed)",
+                       parallelism=f"replicas x{world}",
+                       **({"slopes": len(case.meta["slopes"]), "tuning": tuning} if tuning else {})),
         "gpu_launches": launches,
         "kernel_ms": {k: v[0] for k, v in kt.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,

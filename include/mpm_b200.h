@@ -172,6 +172,20 @@ int mpm_step(mpm_handle *h, double dt, double Ti0, int64_t nsteps, double *Ti_ou
 int mpm_step_async(mpm_handle *h, double dt, double Ti0, int64_t nsteps);
 int mpm_sync(mpm_handle *h);
 
+/* ---- tuning (no counterpart in the reference) ----
+ * Run-time choices of the step: the cell re-sort period (steps) and the
+ * particle-pass variant (0 = per-particle kernels with vector reductions into
+ * L2, 1 = shared-memory tiled kernels).  mpm_autotune times each of the sort
+ * periods 4, 8, 16, 32 with each variant on `steps_per_trial` REAL steps of
+ * the model (8 trials; they advance the simulation exactly like mpm_step, from
+ * Ti0, and *Ti_out receives the end time), keeps the fastest and reports it;
+ * trial_ms (optional, trial_cap entries) receives each trial's ms per step in
+ * the order variant-major, period-minor. */
+int mpm_set_tuning(mpm_handle *h, int32_t sort_every, int32_t tiled);
+int mpm_get_tuning(mpm_handle *h, int32_t *sort_every, int32_t *tiled);
+int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, double *Ti_out,
+                 int32_t *sort_every_out, int32_t *tiled_out, double *trial_ms, int32_t trial_cap);
+
 /* ---- results (device2host!) ---- */
 int mpm_download(mpm_handle *h, const mpm_host_views *v, uint32_t field_mask);
 /* p2c (1-based, the reference's formula) of the current positions, original order. */

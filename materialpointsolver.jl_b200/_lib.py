@@ -35,7 +35,7 @@ EXPORTS = [
     "mpm_download", "mpm_compute_p2c", "mpm_download_order", "mpm_sort", "mpm_run_stages",
     "mpm_download_grid", "mpm_get_stats", "mpm_last_error", "mpm_peak_bandwidth",
     "mpm_set_profiling", "mpm_get_kernel_times", "mpm_abi_sizes", "mpm_cell_order_noalloc",
-    "mpm_grf_eval",
+    "mpm_grf_eval", "mpm_set_tuning", "mpm_get_tuning", "mpm_autotune",
 ]
 NOALLOC_MAX_PARTICLES = 1 << 19
 NOALLOC_MAX_KEYS = 1 << 19
@@ -139,6 +139,10 @@ def lib():
                                        C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]
     L.mpm_abi_sizes.argtypes = [C.POINTER(C.c_int64)] * 4
     L.mpm_cell_order_noalloc.argtypes = [C.POINTER(Desc)] + [C.c_void_p] * 6
+    L.mpm_set_tuning.argtypes = [vp, C.c_int32, C.c_int32]
+    L.mpm_get_tuning.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.mpm_autotune.argtypes = [vp, C.c_double, C.c_double, C.c_int64, C.POINTER(C.c_double),
+                               C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32]
     L.mpm_grf_eval.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                C.c_double, C.c_void_p]
     sizes = [C.c_int64() for _ in range(4)]

@@ -1057,6 +1057,59 @@ int mpm_step(mpm_handle *h, double dt, double Ti0, int64_t nsteps, double *Ti_ou
     return rc;
 }
 
+int mpm_set_tuning(mpm_handle *h, int32_t sort_every, int32_t tiled) {
+    if (!h) return MPM_E_ARG;
+    if (sort_every < 1 || sort_every > 1024 || (tiled != 0 && tiled != 1)) {
+        h->last_error = "sort_every must be 1..1024 and tiled 0 or 1";
+        return MPM_E_ARG;
+    }
+    h->sort_every = sort_every;
+    h->tiled = tiled != 0;
+    return MPM_OK;
+}
+
+int mpm_get_tuning(mpm_handle *h, int32_t *sort_every, int32_t *tiled) {
+    if (!h) return MPM_E_ARG;
+    if (sort_every) *sort_every = h->sort_every;
+    if (tiled) *tiled = h->tiled ? 1 : 0;
+    return MPM_OK;
+}
+
+// Times every candidate (sort period x particle-pass variant) on steps_per_trial
+// real steps of the simulation, each trial starting with a fresh sort, and
+// keeps the fastest.  The trial steps advance the model like mpm_step does.
+int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, double *Ti_out,
+                 int32_t *sort_every_out, int32_t *tiled_out, double *trial_ms, int32_t trial_cap) {
+    static const int32_t periods[] = {4, 8, 16, 32};
+    if (!h) return MPM_E_ARG;
+    if (steps_per_trial < 1) {
+        h->last_error = "steps_per_trial must be >= 1";
+        return MPM_E_ARG;
+    }
+    double Ti = Ti0;
+    double best = 1e300;
+    int32_t best_s = h->sort_every, best_t = h->tiled ? 1 : 0;
+    int k = 0;
+    for (int32_t t = 0; t < 2; ++t) {
+        for (int32_t S : periods) {
+            int rc = mpm_set_tuning(h, S, t);
+            if (rc) return rc;
+            h->since_sort = 1 << 30;   // every trial starts with a sort
+            rc = mpm_step(h, dt, Ti, steps_per_trial, &Ti);
+            if (rc) return rc;
+            const double ms = h->last_step_ms / (double)steps_per_trial;
+            if (trial_ms && k < trial_cap) trial_ms[k] = ms;
+            ++k;
+            if (ms < best) { best = ms; best_s = S; best_t = t; }
+        }
+    }
+    mpm_set_tuning(h, best_s, best_t);
+    if (Ti_out) *Ti_out = Ti;
+    if (sort_every_out) *sort_every_out = best_s;
+    if (tiled_out) *tiled_out = best_t;
+    return MPM_OK;
+}
+
 int mpm_download(mpm_handle *h, const mpm_host_views *v, uint32_t mask) {
     if (!h || !v) return MPM_E_ARG;
     try {

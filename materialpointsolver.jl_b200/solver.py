@@ -151,6 +151,25 @@ class DeviceModel:
         _lib.check(_lib.lib().mpm_get_kernel_times(self.h, names, ms, nl, cap, C.byref(cnt)), self.h)
         return {names[i].decode(): (ms[i], nl[i]) for i in range(min(cnt.value, cap))}
 
+    # run-time tuning of the step (no counterpart in the reference)
+    def set_tuning(self, sort_every, tiled=False):
+        _lib.check(_lib.lib().mpm_set_tuning(self.h, int(sort_every), int(bool(tiled))), self.h)
+
+    def tuning(self):
+        s, t = C.c_int32(), C.c_int32()
+        _lib.check(_lib.lib().mpm_get_tuning(self.h, C.byref(s), C.byref(t)), self.h)
+        return s.value, bool(t.value)
+
+    def autotune(self, dt, Ti, steps_per_trial=32):
+        """Time every (sort period, particle-pass variant) candidate on real
+        steps of this model and keep the fastest.  Returns (Ti after the trial
+        steps, sort_every, tiled, per-trial ms per step)."""
+        Tout, s, t = C.c_double(), C.c_int32(), C.c_int32()
+        ms = (C.c_double * 8)()
+        _lib.check(_lib.lib().mpm_autotune(self.h, dt, Ti, steps_per_trial, C.byref(Tout), C.byref(s),
+                                           C.byref(t), ms, 8), self.h)
+        return Tout.value, s.value, bool(t.value), list(ms)
+
     # clean_device! (devicehelpfunc_cuda.jl:71-100)
     def close(self):
         if getattr(self, "h", None):

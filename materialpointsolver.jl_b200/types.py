@@ -204,17 +204,33 @@ class Grid2D(Grid):
         vy = _axis(self.y1, self.y2, self.dy)[::-1]
         self.nnx, self.nny = len(vx), len(vy)
         self.ni = self.nnx * self.nny
-        x = np.repeat(vx, self.nny)
-        y = np.tile(vy, self.nnx)
-        self.xi = _f(np.stack([x, y], axis=1), self.T2)
+        self._vx, self._vy = vx, vy   # vy descending, as stored
+        self._xi = None
         self.ncx, self.ncy = self.nnx - 1, self.nny - 1
         self.nc = self.ncx * self.ncy
         T2 = self.T2
         self.sigm = np.zeros(self.nc, T2)
         self.Omega = np.zeros(self.nc, T2)
-        self.ms = np.zeros(self.ni, T2)
-        for name in ("ps", "vs", "vsT", "as_", "fs", "dus"):
-            setattr(self, name, _f(np.zeros((self.ni, 2)), T2))
+
+    @property
+    def xi(self):
+        # node coordinates (ni x 2), built on first use
+        if self._xi is None:
+            x = np.repeat(self._vx, self.nny)
+            y = np.tile(self._vy, self.nnx)
+            self._xi = _f(np.stack([x, y], axis=1), self.T2)
+        return self._xi
+
+    def __getattr__(self, name):
+        # the reference's grid work arrays, allocated on first use
+        if name in ("ms",):
+            arr = np.zeros(self.ni, self.T2)
+        elif name in ("ps", "vs", "vsT", "as_", "fs", "dus"):
+            arr = _f(np.zeros((self.ni, 2)), self.T2)
+        else:
+            raise AttributeError(name)
+        object.__setattr__(self, name, arr)
+        return arr
 
 
 class Grid3D(Grid):

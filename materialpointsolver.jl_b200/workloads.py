@@ -225,3 +225,138 @@ def slope_3d(*, h=0.1, ppc=2, seed=1003, jitter=0.1, domain=(100.0, 20.0, 40.0),
     nsteps = int(math.ceil(Ttol / dt))
     return Case("slope_3d", args, grid, mp, attr, bc, dt, nsteps,
                 dict(np=npart, h=h, K=K, G=G, seed=seed, cohesion=coh if field else None))
+
+
+# ---------------------------------------------------------------------------
+# Batches of independent 2D slopes packed side by side into one grid
+# ---------------------------------------------------------------------------
+def draw_slope_specs(n, seed=1004, np_range=(1.0e4, 2.0e5), angle_deg=(25.0, 45.0), height=(5.0, 20.0),
+                     cohesion=(0.0, 20.0e3), friction_deg=(20.0, 35.0), h=0.05, ppc=2):
+    """Draw n slopes: particle count log-uniform in np_range, angle, height,
+    cohesion and friction uniform.  The cross-section area that holds the drawn
+    count is a triangle of the drawn height and angle plus a crest; when the
+    triangle alone is already larger, the height is lowered instead (same
+    angle, no crest)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    per_area = (ppc / h) ** 2
+    specs = []
+    for s in range(n):
+        target = float(np.exp(rng.uniform(math.log(np_range[0]), math.log(np_range[1]))))
+        beta = math.radians(rng.uniform(*angle_deg))
+        H = rng.uniform(*height)
+        c = rng.uniform(*cohesion)
+        phi = math.radians(rng.uniform(*friction_deg))
+        area = target / per_area
+        tri = H * H / (2.0 * math.tan(beta))
+        if area >= tri:
+            crest = (area - tri) / H
+        else:
+            H = math.sqrt(2.0 * area * math.tan(beta))
+            crest = 0.0
+        specs.append(dict(index=s, target_np=target, beta=beta, H=H, crest=crest, c=c, phi=phi,
+                          seed=int(rng.integers(1 << 62))))
+    return specs
+
+
+def slope_points_2d(spec, h, ppc=2, jitter=0.1):
+    """Lattice particles of one slope in its local frame (left wall x = 0, floor
+    y = 0), with the slope's own seeded jitter."""
+    lp = h / ppc
+    tb = math.tan(spec["beta"])
+    x_toe = spec["crest"] + spec["H"] / tb
+    xs = jl_range(lp / 2, lp, x_toe - lp / 2)
+    ys = jl_range(lp / 2, lp, spec["H"] - lp / 2)
+    pts = meshbuilder(xs, ys)
+    pts = pts[pts[:, 0] <= spec["crest"] + (spec["H"] - pts[:, 1]) / tb]
+    rng = np.random.Generator(np.random.PCG64(spec["seed"]))
+    return pts + rng.uniform(-jitter * h, jitter * h, size=pts.shape)
+
+
+def slope_batch_2d(*, n_slopes=256, seed=1004, specs=None, h=0.05, ppc=2, jitter=0.1, gap_cells=8, pad=2,
+                   runout_factor=3.0, precision="FP64", E=20.0e6, nu=0.3, rho=2000.0, psi_deg=0.0, gravity=-9.81,
+                   Ttol=5.0, Te=0.5, cfl=0.2, gpu_precision="mixed", project_path="/tmp", **extra):
+    """Independent 2D Drucker-Prager slopes advanced as one problem: each slope
+    gets its own region of one shared grid -- its wall at x0 (vx fixed), the
+    common floor y = 0 (fixed), a far wall at x0 + L (vx fixed) with L = crest +
+    run of the face + runout_factor x height -- and the regions are separated
+    by gap_cells empty cells, more than the uGIMP stencil reaches, so no node
+    is shared.  Every launch of the step then covers all slopes.  Each slope is
+    its own material (nid = slope + 1).  Offsets are whole cells, so a slope's
+    particles sit at the same place relative to the grid as when the slope is
+    run alone (slope_2d_single)."""
+    specs = specs if specs is not None else draw_slope_specs(n_slopes, seed, h=h, ppc=ppc)
+    K, G = elastic_constants(E, nu)
+    dt = cfl_dt(h, K, G, rho, cfl)
+    lp = h / ppc
+    x0 = 0.0
+    parts, nid, slopes = [], [], []
+    start = 0
+    for k, sp in enumerate(specs):
+        tb = math.tan(sp["beta"])
+        L = sp["crest"] + sp["H"] / tb + runout_factor * sp["H"]
+        L = math.ceil(L / h) * h
+        pts = slope_points_2d(sp, h, ppc, jitter)
+        toe0 = float(pts[:, 0].max())
+        pts = pts.copy()
+        pts[:, 0] += x0
+        parts.append(pts)
+        nid.append(np.full(len(pts), k + 1, np.int64))
+        slopes.append(dict(sp, x0=x0, L=L, np=len(pts), start=start, end=start + len(pts), toe0=toe0))
+        start += len(pts)
+        x0 = x0 + L + gap_cells * h
+    pts = np.concatenate(parts)
+    nid = np.concatenate(nid)
+    npart = len(pts)
+    width = x0 - gap_cells * h
+    top = max(s["H"] for s in slopes) + 1.0
+    akw = dict(Ttol=Ttol, Te=Te, ΔT=dt, FLIP=1, PIC=0, constitutive="druckerprager", basis="uGIMP",
+               device="B200", coupling="OS", scheme="MUSL", va="a", gravity=gravity, ζs=0,
+               project_name="slopes2d", project_path=project_path, ϵ=precision, gpu_precision=gpu_precision,
+               make_project_dir=False)
+    akw.update(extra)
+    args = UserArgs2D(**akw)
+    grid = UserGrid2D(ϵ=precision, x1=-pad * h, x2=width + pad * h, y1=-pad * h, y2=top + pad * h,
+                      dx=h, dy=h, NIC=9)
+    mp = UserParticle2D(ϵ=precision, NIC=9, dx=lp, dy=lp, ξ=pts, ρs=np.full(npart, rho))
+    ns = len(slopes)
+    attr = UserProperty(ϵ=precision, nid=nid, ν=np.full(ns, nu), Es=np.full(ns, E), Gs=np.full(ns, G),
+                        Ks=np.full(ns, K), σt=np.zeros(ns), ϕ=np.array([s["phi"] for s in slopes]),
+                        ϕr=np.zeros(ns), ψ=np.full(ns, math.radians(psi_deg)),
+                        c=np.array([s["c"] for s in slopes]), cr=np.zeros(ns), Hp=np.zeros(ns))
+    # boundary flags: node id = ix * nny + r, r = 0 at the top (y descending)
+    eps = 1e-9 * h
+    vx = grid._vx
+    vy = grid._vy
+    wall = np.zeros(len(vx), bool)
+    for s in slopes:
+        wall |= np.abs(vx - s["x0"]) <= eps
+        wall |= np.abs(vx - (s["x0"] + s["L"])) <= eps
+    floor = vy <= eps
+    fx = (wall[:, None] | floor[None, :]).ravel().astype(np.int64)
+    fy = np.broadcast_to(floor[None, :], (len(vx), len(vy))).ravel().astype(np.int64)
+    bc = UserVBoundary2D(ϵ=precision, vx_s_idx=fx, vx_s_val=np.zeros(grid.ni), vy_s_idx=fy,
+                         vy_s_val=np.zeros(grid.ni))
+    nsteps = int(math.ceil(Ttol / dt))
+    return Case("slope_batch_2d", args, grid, mp, attr, bc, dt, nsteps,
+                dict(np=npart, h=h, K=K, G=G, seed=seed, slopes=slopes))
+
+
+def slope_2d_single(batch_case, k, **kw):
+    """Slope k of a batch alone on its own grid (local frame), with the same
+    particles, material and boundary layout: the plain run the batched one is
+    compared with."""
+    s = batch_case.meta["slopes"][k]
+    a = batch_case.args
+    spec = {key: s[key] for key in ("index", "target_np", "beta", "H", "crest", "c", "phi", "seed")}
+    base = dict(h=batch_case.meta["h"], Ttol=a.Ttol, Te=a.Te, gpu_precision=a.gpu_precision)
+    base.update(kw)
+    return slope_batch_2d(specs=[spec], **base)
+
+
+def slope_runouts(case, xi):
+    """Per-slope run-out: the advance of the slope's farthest particle (toe)
+    from its initial position, in metres."""
+    out = []
+    for s in case.meta["slopes"]:
+        out.append(float(xi[s["start"]:s["end"], 0].max() - s["x0"] - s["toe0"]))
+    return np.array(out)
