@@ -242,6 +242,27 @@ int mpm_cell_order_noalloc(const mpm_desc *d, const double *x, const double *y, 
 int mpm_grf_eval(int32_t device, const double *x, const double *y, const double *z, int64_t np,
                  const double *harm, int64_t nh, double scale, double *out);
 
+/* ---- stress-return surrogate (no counterpart in the reference) ----
+ * A 15 -> 64 -> 64 -> 64 -> 6 GELU MLP standing in for the Drucker-Prager /
+ * Mohr-Coulomb return (druckerprager.jl:89-155), BF16 weights and FP32
+ * accumulation on the tensor cores (tcgen05).  params: mpm_mlp_nparams() FP32
+ * master values, per layer W[k][n] then b[n] with the input padded to 16 and
+ * the output to 16 (padding stays zero).  norm: 64 floats, input mean[16],
+ * input std[16], output mean[16], output std[16].  feat: n x 16 FP32 (15
+ * features + 1 pad), target / out: n x 6.  All arrays are DEVICE pointers, the
+ * work is queued on `stream` (a cudaStream_t, NULL = default); err (device int)
+ * gets bit 0 set if a tensor-core completion wait timed out. */
+int mpm_mlp_nparams(void);
+int mpm_mlp_forward(const float *params, const float *norm, const float *feat, float *out, int64_t n,
+                    int *err, void *stream);
+/* Adds the gradient of 1/2 * inv_btot * sum (MLP(x) - y)^2 (normalised units)
+ * over the n samples to grad, and that loss to *loss. */
+int mpm_mlp_grad(const float *params, const float *norm, const float *feat, const float *target, int64_t n,
+                 float inv_btot, float *grad, float *loss, int *err, void *stream);
+/* One Adam step (bias correction for step count `step` >= 1); zeroes grad. */
+int mpm_mlp_adam(float *params, float *grad, float *m, float *v, float lr, float b1, float b2, float eps,
+                 int64_t step, void *stream);
+
 /* ---- diagnostics ---- */
 /* sizeof(mpm_desc), sizeof(mpm_view), sizeof(mpm_host_views), sizeof(mpm_stats):
  * lets a binding verify its struct layouts against the library's. */

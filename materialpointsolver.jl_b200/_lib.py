@@ -36,6 +36,7 @@ EXPORTS = [
     "mpm_download_grid", "mpm_get_stats", "mpm_last_error", "mpm_peak_bandwidth",
     "mpm_set_profiling", "mpm_get_kernel_times", "mpm_abi_sizes", "mpm_cell_order_noalloc",
     "mpm_grf_eval", "mpm_set_tuning", "mpm_get_tuning", "mpm_autotune",
+    "mpm_mlp_nparams", "mpm_mlp_forward", "mpm_mlp_grad", "mpm_mlp_adam",
 ]
 NOALLOC_MAX_PARTICLES = 1 << 19
 NOALLOC_MAX_KEYS = 1 << 19
@@ -83,7 +84,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
               "-Xcompiler", "-fPIC", "-shared"]
 
 
-TRANSLATION_UNITS = ["mpm_b200.cu", "mpm_noalloc.cu", "mpm_grf.cu"]
+TRANSLATION_UNITS = ["mpm_b200.cu", "mpm_noalloc.cu", "mpm_grf.cu", "mpm_mlp.cu"]
 
 
 def sources():
@@ -143,6 +144,10 @@ def lib():
     L.mpm_get_tuning.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.mpm_autotune.argtypes = [vp, C.c_double, C.c_double, C.c_int64, C.POINTER(C.c_double),
                                C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32]
+    L.mpm_mlp_nparams.argtypes = []
+    L.mpm_mlp_forward.argtypes = [vp, vp, vp, vp, C.c_int64, vp, vp]
+    L.mpm_mlp_grad.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_float, vp, vp, vp, vp]
+    L.mpm_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int64, vp]
     L.mpm_grf_eval.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                C.c_double, C.c_void_p]
     sizes = [C.c_int64() for _ in range(4)]

@@ -1,0 +1,514 @@
+// mpm_mlp.cu -- the stress-return surrogate: a 15 -> 64 -> 64 -> 64 -> 6 GELU MLP
+// with BF16 weights and FP32 accumulation, run and trained on the sm_100a
+// tensor cores (tcgen05.mma, accumulators in TMEM, operands in shared memory).
+//
+// No counterpart in the reference, whose return mappings (dpP!,
+// src/materials/druckerprager.jl:89-155; mcP!, mohrcoulomb.jl) the network
+// stands in for.  Features (15, normalised by the caller's mean / std):
+// trial stress (6), strain increment (6), accumulated plastic strain, cohesion,
+// friction angle.  Output (6): the returned stress, normalised.
+//
+// Parameters: one FP32 vector (the master copy the optimiser updates), layer
+// by layer W[k][n] (k input, n output) then b[n]; the 15-wide input and the
+// 6-wide output are padded to 16 with rows / columns that stay zero.  Every
+// CTA converts them to BF16 in shared memory in the layouts the MMAs read.
+//
+// One CTA = 128 threads = one tile of 128 samples (thread t owns sample row t
+// and reads TMEM lane t); CTAs stride over the tiles.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/mpm_b200.h"
+#include "mpm_umma.cuh"
+
+namespace mpm_detail {
+void set_global_error(const std::string &m);
+}
+
+namespace {
+
+using namespace mpm::umma;
+
+constexpr int TILE = 128;
+constexpr int NL = 4;
+__host__ __device__ constexpr int lk(int l) { return l == 0 ? 16 : 64; }   // padded inputs of layer l
+__host__ __device__ constexpr int ln(int l) { return l == 3 ? 16 : 64; }   // padded outputs of layer l
+__host__ __device__ constexpr int ow(int l) {                               // offset of W_l
+    return l == 0 ? 0 : l == 1 ? 1088 : l == 2 ? 5248 : 9408;
+}
+__host__ __device__ constexpr int ob(int l) { return ow(l) + lk(l) * ln(l); }   // offset of b_l
+constexpr int NPAR = 10448;
+static_assert(ob(3) + 16 == NPAR, "parameter layout");
+
+// norm: in_mean[16], in_std[16], out_mean[16], out_std[16]
+constexpr int NORM = 64;
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.3989422804014327f * __expf(-0.5f * z * z);
+}
+
+__device__ __forceinline__ void st_bf16(uint8_t *base, uint32_t off, float v) {
+    *reinterpret_cast<__nv_bfloat16 *>(base + off) = __float2bfloat16_rn(v);
+}
+
+// W_l^T (n rows, k columns): B operand of the forward MMA
+__device__ void load_wT(uint8_t *dst, const float *P, int l) {
+    const int K = lk(l), N = ln(l);
+    for (int i = threadIdx.x; i < N * K; i += blockDim.x) {
+        const int n = i / K, k = i % K;
+        st_bf16(dst, kmajor_offset(n, k, K), P[ow(l) + k * N + n]);
+    }
+}
+// W_l (k rows, n columns): B operand of the backward MMA dY = dZ * W^T
+__device__ void load_w(uint8_t *dst, const float *P, int l) {
+    const int K = lk(l), N = ln(l);
+    for (int i = threadIdx.x; i < N * K; i += blockDim.x) {
+        const int k = i / N, n = i % N;
+        st_bf16(dst, kmajor_offset(k, n, N), P[ow(l) + k * N + n]);
+    }
+}
+
+struct Smem {
+    uint8_t *wT[NL];      // forward B operands
+    uint8_t *x;           // 128 x 16 inputs (A of layer 0)
+    uint8_t *a;           // 128 x 64 hidden activations (A of layers 1..3)
+    float *bias;          // 4 x 64
+    float *norm;          // 64
+    uint64_t *bar;
+    uint32_t *tslot;
+};
+
+__device__ uint8_t *carve(uint8_t *&p, size_t bytes) {
+    uint8_t *r = p;
+    p += (bytes + 127) & ~(size_t)127;
+    return r;
+}
+
+__device__ void setup_forward(Smem &S, uint8_t *&p, const float *P, const float *norm) {
+    for (int l = 0; l < NL; ++l) S.wT[l] = carve(p, (size_t)lk(l) * ln(l) * 2);
+    S.x = carve(p, TILE * 16 * 2);
+    S.a = carve(p, TILE * 64 * 2);
+    S.bias = reinterpret_cast<float *>(carve(p, 4 * 64 * 4));
+    S.norm = reinterpret_cast<float *>(carve(p, NORM * 4));
+    S.bar = reinterpret_cast<uint64_t *>(carve(p, 16));
+    S.tslot = reinterpret_cast<uint32_t *>(carve(p, 16));
+    for (int l = 0; l < NL; ++l) load_wT(S.wT[l], P, l);
+    for (int i = threadIdx.x; i < 4 * 64; i += blockDim.x) {
+        const int l = i / 64, n = i % 64;
+        S.bias[i] = n < ln(l) ? P[ob(l) + n] : 0.0f;
+    }
+    for (int i = threadIdx.x; i < NORM; i += blockDim.x) S.norm[i] = norm[i];
+    fence_proxy_async();   // the weights are read by the tensor core
+}
+
+// issue the MMAs of one layer: D[tmem_d] = A (128 x K, at a_saddr) * B^T (N x K)
+__device__ __forceinline__ void issue_layer(uint32_t tmem_d, uint32_t a_saddr, uint32_t b_saddr, int K, int N,
+                                            uint32_t bar) {
+    const uint32_t idesc = idesc_bf16_f32(TILE, N);
+    for (int j = 0; j < K / 16; ++j)
+        mma_bf16(tmem_d, kstep_desc(a_saddr, j, K), kstep_desc(b_saddr, j, K), idesc, j > 0 ? 1u : 0u);
+    commit(bar);
+}
+
+// Wait for the MMAs committed to `bar` (phase parity flips per use).  The
+// outcome is made CTA-uniform, so a timed-out wait takes every thread out of
+// the tile loop together.
+__device__ __forceinline__ bool layer_done(uint32_t bar, uint32_t &parity, int *err) {
+    const bool mine = mbar_wait(bar, parity);
+    parity ^= 1u;
+    const bool ok = __syncthreads_and(mine) != 0;
+    if (!ok && threadIdx.x == 0) atomicOr(err, 1);
+    fence_after_sync();
+    return ok;
+}
+
+// hidden-layer epilogue: bias + GELU of this thread's row -> BF16 row of `a`
+__device__ __forceinline__ void hidden_epilogue(uint32_t trow, const float *bias, uint8_t *a, float *zkeep) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < 64; c += 16) {
+        float z[16];
+        tmem_ld16(trow + c, z);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const float zz = z[i] + bias[c + i];
+            if (zkeep) zkeep[c + i] = zz;
+            st_bf16(a, kmajor_offset(t, c + i, 64), gelu(zz));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Inference: out[i, 0..5] = MLP(feat[i, 0..15]) in physical units.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TILE) k_mlp_forward(const float *__restrict__ P, const float *__restrict__ norm,
+                                                      const float *__restrict__ feat, float *__restrict__ out,
+                                                      int64_t n, int *err) {
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    uint8_t *p = smem_raw;
+    Smem S;
+    setup_forward(S, p, P, norm);
+    const int t = threadIdx.x, w = t >> 5;
+    const uint32_t bar = smem_u32(S.bar);
+    if (t == 0) mbar_init(bar, 1);
+    if (w == 0) tmem_alloc(smem_u32(S.tslot), 64);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *S.tslot;
+    const uint32_t trow = tmem + ((uint32_t)(w * 32) << 16);
+    uint32_t parity = 0;
+    bool ok = true;
+    const int64_t ntiles = (n + TILE - 1) / TILE;
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int64_t row = tile * TILE + t;
+        // inputs: normalise, BF16, canonical layout
+        float f[16];
+        if (row < n) {
+            const float4 *src = reinterpret_cast<const float4 *>(feat + row * 16);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 v = src[q];
+                f[4 * q] = v.x; f[4 * q + 1] = v.y; f[4 * q + 2] = v.z; f[4 * q + 3] = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) f[k] = S.norm[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const float xn = k < 15 ? (f[k] - S.norm[k]) / S.norm[16 + k] : 0.0f;
+            st_bf16(S.x, kmajor_offset(t, k, 16), xn);
+        }
+        fence_proxy_async();
+        __syncthreads();
+        // layer 0
+        if (t == 0) {
+            fence_after_sync();
+            issue_layer(tmem, smem_u32(S.x), smem_u32(S.wT[0]), 16, 64, bar);
+        }
+        ok = layer_done(bar, parity, err);
+        if (!ok) break;
+        hidden_epilogue(trow, S.bias, S.a, nullptr);
+        fence_before_sync();
+        fence_proxy_async();
+        __syncthreads();
+        // layers 1, 2 (input and output share `a`: the epilogue runs after the MMA completed)
+        for (int l = 1; l <= 2 && ok; ++l) {
+            if (t == 0) {
+                fence_after_sync();
+                issue_layer(tmem, smem_u32(S.a), smem_u32(S.wT[l]), 64, 64, bar);
+            }
+            ok = layer_done(bar, parity, err);
+            if (!ok) break;
+            hidden_epilogue(trow, S.bias + 64 * l, S.a, nullptr);
+            fence_before_sync();
+            fence_proxy_async();
+            __syncthreads();
+        }
+        if (!ok) break;
+        // layer 3: 16 (6 used) outputs
+        if (t == 0) {
+            fence_after_sync();
+            issue_layer(tmem, smem_u32(S.a), smem_u32(S.wT[3]), 64, 16, bar);
+        }
+        ok = layer_done(bar, parity, err);
+        if (!ok) break;
+        float z[16];
+        tmem_ld16(trow, z);
+        if (row < n) {
+#pragma unroll
+            for (int o = 0; o < 6; ++o) out[row * 6 + o] = (z[o] + S.bias[192 + o]) * S.norm[48 + o] + S.norm[32 + o];
+        }
+        fence_before_sync();
+        __syncthreads();
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    if (w == 0) tmem_dealloc(tmem, 64);
+}
+
+}  // namespace
+
+extern "C" int mpm_mlp_nparams(void) { return NPAR; }
+
+// Forward pass over n samples; all pointers are DEVICE arrays, work on `stream`.
+extern "C" int mpm_mlp_forward(const float *params, const float *norm, const float *feat, float *out, int64_t n,
+                               int *err, void *stream) {
+    if (!params || !norm || !err || n < 0 || (n > 0 && (!feat || !out))) {
+        mpm_detail::set_global_error("mpm_mlp_forward: invalid arguments");
+        return MPM_E_ARG;
+    }
+    if (n == 0) return MPM_OK;
+    const size_t smem = 60 * 1024;   // caps residency at 3 CTAs (192 of 512 TMEM columns) per SM
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t ntiles = (n + TILE - 1) / TILE;
+        const int grid = (int)(ntiles < 3 * nsm ? ntiles : 3 * nsm);
+        k_mlp_forward<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, out, n, err);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        mpm_detail::set_global_error(std::string("mpm_mlp_forward: ") + cudaGetErrorString(e));
+        return MPM_E_CUDA;
+    }
+    return MPM_OK;
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Training: gradient of L = 1/(2 btot) * sum over samples and the 6 outputs of
+// (MLP(x) - y)^2 (normalised units), accumulated into grad[NPAR] (FP32,
+// reductions from every CTA), and the loss into *loss.
+//
+// Per tile, forward with the pre-activations kept in TMEM (Z_l at column 64 l),
+// then for l = 3 .. 0:
+//   dW_l^T = dZ_l^T (128 x 128 samples) * Y_{l-1}            (TMEM column 384)
+//   dY_{l-1} = dZ_l (128 samples x N_l) * W_l^T               (TMEM column 256)
+//   dZ_{l-1} = dY_{l-1} .* GELU'(Z_{l-1} + b_{l-1})
+// Operands: Y_l^T and dZ^T are stored feature-major (samples contiguous) so that
+// the sample sum is the MMA's K dimension; rows of dZ^T beyond N_l are not read
+// back (row m of D only depends on row m of A).
+// ---------------------------------------------------------------------------
+constexpr uint32_t COL_DY = 256, COL_DW = 384, TCOLS = 512;
+
+struct TSmem {
+    uint8_t *w[NL];       // W_l (k rows x n), layers 1..3
+    uint8_t *xT;          // 16 x 128
+    uint8_t *yT[3];       // 64 x 128 each: Y_0..Y_2 feature-major
+    uint8_t *dz;          // 128 x N (sample-major)
+    uint8_t *dzT;         // 128 x 128 (feature-major, rows >= N unused)
+    float *dbias;         // 4 x 64
+};
+
+__device__ __forceinline__ void issue_gemm(uint32_t tmem_d, uint32_t a_saddr, uint32_t b_saddr, int K, int N) {
+    const uint32_t idesc = idesc_bf16_f32(TILE, N);
+    for (int j = 0; j < K / 16; ++j)
+        mma_bf16(tmem_d, kstep_desc(a_saddr, j, K), kstep_desc(b_saddr, j, K), idesc, j > 0 ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ P, const float *__restrict__ norm,
+                                                      const float *__restrict__ feat,
+                                                      const float *__restrict__ target, int64_t n, float inv_btot,
+                                                      float *__restrict__ grad, float *__restrict__ loss, int *err) {
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    uint8_t *p = smem_raw;
+    Smem S;
+    setup_forward(S, p, P, norm);
+    TSmem T;
+    T.w[0] = nullptr;
+    for (int l = 1; l < NL; ++l) T.w[l] = carve(p, (size_t)lk(l) * ln(l) * 2);
+    T.xT = carve(p, 16 * TILE * 2);
+    for (int l = 0; l < 3; ++l) T.yT[l] = carve(p, 64 * TILE * 2);
+    T.dz = carve(p, TILE * 64 * 2);
+    T.dzT = carve(p, TILE * TILE * 2);
+    T.dbias = reinterpret_cast<float *>(carve(p, 4 * 64 * 4));
+    for (int l = 1; l < NL; ++l) load_w(T.w[l], P, l);
+    for (int i = threadIdx.x; i < TILE * TILE; i += blockDim.x)
+        reinterpret_cast<__nv_bfloat16 *>(T.dzT)[i] = __float2bfloat16_rn(0.0f);
+    for (int i = threadIdx.x; i < 4 * 64; i += blockDim.x) T.dbias[i] = 0.0f;
+    fence_proxy_async();
+
+    const int t = threadIdx.x, w = t >> 5;
+    const uint32_t bar = smem_u32(S.bar);
+    if (t == 0) mbar_init(bar, 1);
+    if (w == 0) tmem_alloc(smem_u32(S.tslot), TCOLS);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *S.tslot;
+    const uint32_t trow = tmem + ((uint32_t)(w * 32) << 16);
+    uint32_t parity = 0;
+    bool ok = true;
+    float my_loss = 0.0f;
+    const int64_t ntiles = (n + TILE - 1) / TILE;
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int64_t row = tile * TILE + t;
+        const bool valid = row < n;
+        float f[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) f[k] = valid ? feat[row * 16 + k] : S.norm[k];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const float xn = k < 15 ? (f[k] - S.norm[k]) / S.norm[16 + k] : 0.0f;
+            st_bf16(S.x, kmajor_offset(t, k, 16), xn);
+            st_bf16(T.xT, kmajor_offset(k, t, TILE), xn);
+        }
+        fence_proxy_async();
+        __syncthreads();
+        // ---- forward, Z_l kept at column 64 l
+        for (int l = 0; l < 3 && ok; ++l) {
+            if (t == 0) {
+                fence_after_sync();
+                issue_layer(tmem + 64u * l, smem_u32(l == 0 ? S.x : S.a), smem_u32(S.wT[l]), lk(l), 64, bar);
+            }
+            ok = layer_done(bar, parity, err);
+            if (!ok) break;
+#pragma unroll
+            for (int c = 0; c < 64; c += 16) {
+                float z[16];
+                tmem_ld16(trow + 64u * l + c, z);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const float y = gelu(z[i] + S.bias[64 * l + c + i]);
+                    st_bf16(S.a, kmajor_offset(t, c + i, 64), y);
+                    st_bf16(T.yT[l], kmajor_offset(c + i, t, TILE), y);
+                }
+            }
+            fence_before_sync();
+            fence_proxy_async();
+            __syncthreads();
+        }
+        if (!ok) break;
+        if (t == 0) {
+            fence_after_sync();
+            issue_layer(tmem + 192u, smem_u32(S.a), smem_u32(S.wT[3]), 64, 16, bar);
+        }
+        ok = layer_done(bar, parity, err);
+        if (!ok) break;
+        // ---- output layer: dZ_3 = (yhat - y) / btot on the 6 outputs
+        {
+            float z[16];
+            tmem_ld16(trow + 192u, z);
+#pragma unroll
+            for (int o = 0; o < 16; ++o) {
+                float d = 0.0f;
+                if (valid && o < 6) {
+                    const float yh = z[o] + S.bias[192 + o];
+                    const float y = (target[row * 6 + o] - S.norm[32 + o]) / S.norm[48 + o];
+                    d = yh - y;
+                    my_loss += 0.5f * d * d * inv_btot;
+                    d *= inv_btot;
+                }
+                st_bf16(T.dz, kmajor_offset(t, o, 16), d);
+                st_bf16(T.dzT, kmajor_offset(o, t, TILE), d);
+                if (d != 0.0f) atomicAdd(&T.dbias[192 + o], d);
+            }
+        }
+        // ---- backward through layers 3, 2, 1 (dW_l and dY_{l-1}), then dW_0
+        for (int l = 3; l >= 0 && ok; --l) {
+            fence_before_sync();
+            fence_proxy_async();
+            __syncthreads();
+            if (t == 0) {
+                fence_after_sync();
+                issue_gemm(tmem + COL_DW, smem_u32(T.dzT), smem_u32(l == 0 ? T.xT : T.yT[l - 1]), TILE, lk(l));
+                if (l > 0) issue_gemm(tmem + COL_DY, smem_u32(T.dz), smem_u32(T.w[l]), ln(l), lk(l));
+                commit(bar);
+            }
+            ok = layer_done(bar, parity, err);
+            if (!ok) break;
+            // dW_l^T: lane = output unit n, columns = inputs k
+            const int N = ln(l), K = lk(l);
+            for (int c = 0; c < K; c += 16) {
+                float g[16];
+                tmem_ld16(trow + COL_DW + c, g);
+                if (t < N) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) atomicAdd(&grad[ow(l) + (c + i) * N + t], g[i]);
+                }
+            }
+            if (l == 0) break;
+            // dZ_{l-1} = dY_{l-1} .* GELU'(Z_{l-1} + b_{l-1})
+            const int lp = l - 1;
+#pragma unroll
+            for (int c = 0; c < 64; c += 16) {
+                float dy[16], z[16];
+                tmem_ld16(trow + COL_DY + c, dy);
+                tmem_ld16(trow + 64u * lp + c, z);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const float d = valid ? dy[i] * gelu_grad(z[i] + S.bias[64 * lp + c + i]) : 0.0f;
+                    st_bf16(T.dz, kmajor_offset(t, c + i, 64), d);
+                    st_bf16(T.dzT, kmajor_offset(c + i, t, TILE), d);
+                    if (d != 0.0f) atomicAdd(&T.dbias[64 * lp + c + i], d);
+                }
+            }
+        }
+        fence_before_sync();
+        __syncthreads();
+    }
+    // bias gradients and loss
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * 64; i += blockDim.x) {
+        const int l = i / 64, nn = i % 64;
+        if (nn < ln(l) && T.dbias[i] != 0.0f) atomicAdd(&grad[ob(l) + nn], T.dbias[i]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) my_loss += __shfl_xor_sync(0xffffffffu, my_loss, o);
+    if ((t & 31) == 0 && my_loss != 0.0f) atomicAdd(loss, my_loss);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    if (w == 0) tmem_dealloc(tmem, TCOLS);
+}
+
+// Adam on the FP32 master parameters; clears the gradient.
+__global__ void k_adam(float *P, float *G, float *M, float *V, int npar, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npar) return;
+    const float g = G[i];
+    const float m = b1 * M[i] + (1.0f - b1) * g;
+    const float v = b2 * V[i] + (1.0f - b2) * g * g;
+    M[i] = m;
+    V[i] = v;
+    P[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+    G[i] = 0.0f;
+}
+
+}  // namespace
+
+// Gradient of the loss over n samples (feat: n x 16, target: n x 6, DEVICE
+// arrays), ADDED to grad[mpm_mlp_nparams()]; the loss is added to *loss.
+// inv_btot scales both (1 / batch size for a mean).
+extern "C" int mpm_mlp_grad(const float *params, const float *norm, const float *feat, const float *target,
+                            int64_t n, float inv_btot, float *grad, float *loss, int *err, void *stream) {
+    if (!params || !norm || !grad || !loss || !err || n < 0 || (n > 0 && (!feat || !target))) {
+        mpm_detail::set_global_error("mpm_mlp_grad: invalid arguments");
+        return MPM_E_ARG;
+    }
+    if (n == 0) return MPM_OK;
+    const size_t smem = 200 * 1024;   // one CTA per SM: it holds all 512 TMEM columns
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t ntiles = (n + TILE - 1) / TILE;
+        const int grid = (int)(ntiles < nsm ? ntiles : nsm);
+        k_mlp_grad<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, target, n, inv_btot, grad, loss,
+                                                              err);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        mpm_detail::set_global_error(std::string("mpm_mlp_grad: ") + cudaGetErrorString(e));
+        return MPM_E_CUDA;
+    }
+    return MPM_OK;
+}
+
+// One Adam step (bias-corrected with the step count `step` >= 1); zeroes grad.
+extern "C" int mpm_mlp_adam(float *params, float *grad, float *m, float *v, float lr, float b1, float b2, float eps,
+                            int64_t step, void *stream) {
+    if (!params || !grad || !m || !v || step < 1) {
+        mpm_detail::set_global_error("mpm_mlp_adam: invalid arguments");
+        return MPM_E_ARG;
+    }
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    k_adam<<<(NPAR + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, grad, m, v, NPAR, lr, b1, b2, eps, c1, c2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        mpm_detail::set_global_error(std::string("mpm_mlp_adam: ") + cudaGetErrorString(e));
+        return MPM_E_CUDA;
+    }
+    return MPM_OK;
+}

@@ -1,0 +1,100 @@
+"""The stress-return surrogate's tensor-core kernels (csrc/mpm_mlp.cu).
+
+CPU: the parameter layout and normalisation helpers; the reference MLP's
+backward against finite differences.  GPU: the tcgen05 forward against the
+FP64 reference with the same BF16 roundings (tight) and without them (loose);
+the tcgen05 gradient against the FP64 gradient; training lowers the loss.
+"""
+import numpy as np
+import pytest
+
+import mlp_ref
+from helpers import rel
+
+
+def rand_case(pkg, n, seed=0):
+    S = pkg.surrogate
+    rng = np.random.default_rng(seed)
+    feat = rng.normal(0.0, 1.0, (n, 15)) * np.linspace(1.0, 3.0, 15) + np.linspace(-2.0, 2.0, 15)
+    target = np.column_stack([np.tanh(feat[:, :6] * 0.5) + 0.1 * feat[:, 6:12] * feat[:, 12:13]])
+    P = S.init_params(seed)
+    norm = S.make_norm(feat, target)
+    return S.pad_features(feat), target.astype(np.float32), P, norm
+
+
+def test_param_layout(pkg):
+    S = pkg.surrogate
+    P = S.init_params(3)
+    assert P.size == sum(k * n + n for k, n in S.LAYERS) == 10448
+    layers = S.unpack(P)
+    assert np.all(layers[0][0][15] == 0)          # padded input row
+    assert np.all(layers[3][0][:, 6:] == 0)       # padded outputs
+    assert all(np.all(b == 0) for _, b in layers)
+
+
+def test_reference_gradient_matches_finite_differences(pkg):
+    feat, target, P, norm = rand_case(pkg, 40, seed=1)
+    layers = [(W.astype(np.float64), b.astype(np.float64) + 0.01) for W, b in pkg.surrogate.unpack(P)]
+    grads, loss = mlp_ref.gradient(layers, norm, feat, target, 1.0 / 40)
+    rng = np.random.default_rng(2)
+    for li in range(4):
+        W, b = layers[li]
+        kmax = 15 if li == 0 else W.shape[0]
+        nmax = 6 if li == 3 else W.shape[1]
+        for _ in range(4):
+            k, n = rng.integers(kmax), rng.integers(nmax)
+            h = 1e-6
+            Wp = W.copy(); Wp[k, n] += h
+            Wm = W.copy(); Wm[k, n] -= h
+            lp = mlp_ref.gradient(layers[:li] + [(Wp, b)] + layers[li + 1:], norm, feat, target, 1.0 / 40)[1]
+            lm = mlp_ref.gradient(layers[:li] + [(Wm, b)] + layers[li + 1:], norm, feat, target, 1.0 / 40)[1]
+            assert grads[li][0][k, n] == pytest.approx((lp - lm) / (2 * h), rel=1e-5, abs=1e-9)
+
+
+def gpu_surrogate(pkg, P, norm):
+    return pkg.surrogate.Surrogate(params=P, norm=norm)
+
+
+@pytest.mark.gpu
+def test_forward_matches_reference(pkg, gpu_lib):
+    import torch
+    feat, target, P, norm = rand_case(pkg, 1000, seed=4)
+    P = P.copy()
+    for ow, ob in pkg.surrogate.offsets():   # nonzero biases
+        P[ob:ob + 16] = np.linspace(-0.1, 0.1, 16, dtype=np.float32)
+    layers = pkg.surrogate.unpack(P)
+    layers[3][1][6:] = 0
+    P[pkg.surrogate.offsets()[3][1] + 6:] = 0
+    sur = gpu_surrogate(pkg, P, norm)
+    out = sur.forward(torch.tensor(feat, device="cuda")).cpu().numpy()
+    emu, _ = mlp_ref.forward(layers, norm, feat, emulate_bf16=True)
+    exact, _ = mlp_ref.forward(layers, norm, feat, emulate_bf16=False)
+    assert rel(out, emu) < 2e-3, rel(out, emu)
+    assert rel(out, exact) < 3e-2, rel(out, exact)
+
+
+@pytest.mark.gpu
+def test_gradient_matches_reference(pkg, gpu_lib):
+    import torch
+    feat, target, P, norm = rand_case(pkg, 700, seed=5)   # 6 tiles, the last one partial
+    layers = pkg.surrogate.unpack(P)
+    sur = gpu_surrogate(pkg, P, norm)
+    G, loss = sur.gradient(torch.tensor(feat, device="cuda"), torch.tensor(target, device="cuda"))
+    ref, loss_ref = mlp_ref.gradient(layers, norm, feat, target, 1.0 / 700, emulate_bf16=True)
+    ex, _ = mlp_ref.gradient(layers, norm, feat, target, 1.0 / 700, emulate_bf16=False)
+    assert loss == pytest.approx(loss_ref, rel=2e-3)
+    gl = pkg.surrogate.unpack(G)
+    for li in range(4):
+        assert rel(gl[li][0], ref[li][0]) < 1e-2, (li, rel(gl[li][0], ref[li][0]))
+        assert rel(gl[li][1], ref[li][1]) < 1e-2, (li, rel(gl[li][1], ref[li][1]))
+        assert rel(gl[li][0], ex[li][0]) < 4e-2, (li, rel(gl[li][0], ex[li][0]))
+
+
+@pytest.mark.gpu
+def test_training_lowers_the_loss(pkg, gpu_lib):
+    import torch
+    feat, target, P, norm = rand_case(pkg, 20000, seed=6)
+    sur = gpu_surrogate(pkg, P, norm)
+    losses = sur.train(torch.tensor(feat, device="cuda"), torch.tensor(target, device="cuda"), epochs=15,
+                       batch=2048, lr=3e-3)
+    assert losses[-1] < 0.1 * losses[0], losses
