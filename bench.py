@@ -45,6 +45,9 @@ def parse():
                     help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
                          "3D slope with a lognormal cohesion field; batch2d: 256 independent 2D slopes "
                          "(15.5 M particles) advanced together, autotuned during warm-up")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="slope3d: train the stress-return surrogate on samples logged from plain steps "
+                         "(untimed) and time steps with it")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W warm-up + K device steps (the command profilers wrap)")
     return ap.parse_args()
@@ -133,11 +136,13 @@ WORKLOADS = {
 }
 
 
-def make_case(mc3d, workload="column3d"):
+def make_case(mc3d, workload="column3d", surrogate=False):
     import __graft_entry__ as g
     pkg = g.load_package()
     if workload == "slope3d":
-        case = pkg.workloads.slope_3d()
+        # with the surrogate the run starts in the plastic regime (no gravity
+        # ramp), so that the timed steps exercise the return it replaces
+        case = pkg.workloads.slope_3d(Te=0.0) if surrogate else pkg.workloads.slope_3d()
     elif workload == "batch2d":
         case = pkg.workloads.slope_batch_2d()
     else:
@@ -179,7 +184,7 @@ BN_G2P_2D = 28         # Δu read (2 floats) + m, p, f written (5 floats)
 
 def run_b200(args):
     rank, world, local = dist_env()
-    pkg, case = make_case(args.mc3d, args.workload)
+    pkg, case = make_case(args.mc3d, args.workload, args.surrogate)
     lib = pkg._lib
     use_dist = world > 1
     if use_dist:
@@ -226,6 +231,24 @@ def run_b200(args):
         Ti, S, tiled, trial_ms = dev.autotune(dt, Ti, 16)
         tuning = {"sort_every": S, "tiled": tiled, "trial_ms_per_step": trial_ms,
                   "candidates": "sort period 4/8/16/32 x per-particle/tiled passes, 16 steps each"}
+    surr_info = None
+    if args.surrogate:
+        if args.workload != "slope3d":
+            raise SystemExit("--surrogate applies to --workload slope3d")
+        # untimed: log samples of the plain return, train, switch the step over
+        t0 = time.perf_counter()
+        S = pkg.surrogate
+        feat, tgt, Ti = S.collect_samples(dev, dt, Ti, 60, 6_000_000, every=8, device=local)
+        sur = S.Surrogate(seed=1, device=local)
+        sur.set_norm(feat, tgt)
+        losses = sur.train(feat, tgt, epochs=6, batch=16384, lr=3e-3, lr_end=1e-4)
+        # the plain step on the same state, for comparison
+        dev.step(dt, Ti, 16)
+        plain_ms = dev.stats().last_step_ms / 16
+        Ti += 16 * dt
+        dev.set_surrogate(sur, tol=1e-3, sref=1e3)
+        surr_info = {"plain_ms_per_step_same_state": plain_ms,"train_samples": int(feat.shape[0]), "epochs": 6, "loss_first_last": [losses[0], losses[-1]],
+                     "setup_s": time.perf_counter() - t0, "tol": 1e-3, "sref_pa": 1e3}
     dev.step(dt, Ti, W)
     Ti += W * dt
     if use_dist:
@@ -243,6 +266,10 @@ def run_b200(args):
     value = replica_value(world, npart, K, t_max)
 
     sort_used, tiled_used = dev.tuning()
+    if surr_info is not None:
+        st_s = dev.stats()
+        surr_info["rows"] = int(st_s.surr_rows)
+        surr_info["accepted_fraction"] = 1.0 - st_s.surr_fallbacks / max(st_s.surr_rows, 1)
 
     # ---- per-kernel device times (events on the library stream) ----
     dev.set_profiling(True)
@@ -252,6 +279,10 @@ def run_b200(args):
     dev.close()
     dom = "g2p_p2g"
     dom_ms = kt.get(dom, (float("nan"), 0))[0]
+    if dom not in kt and "g2p" in kt and "p2g" in kt:
+        # surrogate steps run G2P and P2G as two passes around the MLP
+        dom = "g2p+p2g"
+        dom_ms = kt["g2p"][0] + kt["p2g"][0]
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -280,7 +311,8 @@ def run_b200(args):
                        particle_passes="tiled" if tiled_used else "per-particle",
                        l2=f"particle state {npart * bp_step / 1e9:.2f} GB > 126 MB L2 (no flush needed)",
                        parallelism=f"replicas x{world}",
-                       **({"slopes": len(case.meta["slopes"]), "tuning": tuning} if tuning else {})),
+                       **({"slopes": len(case.meta["slopes"]), "tuning": tuning} if tuning else {}),
+                       **({"surrogate": surr_info} if surr_info else {})),
         "gpu_launches": launches,
         "kernel_ms": {k: v[0] for k, v in kt.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,

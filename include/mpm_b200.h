@@ -156,6 +156,8 @@ typedef struct {
     int32_t kernels_per_step;  /* kernel launches per step */
     double last_step_ms;       /* device time of the last mpm_step call, ms */
     double device_bytes;       /* device memory held by the handle, bytes */
+    int64_t surr_rows;         /* returns handed to the surrogate so far */
+    int64_t surr_fallbacks;    /* of those, returns redone by the plain return */
 } mpm_stats;
 
 /* ---- lifecycle (host2device / clean_device!) ---- */
@@ -253,15 +255,32 @@ int mpm_grf_eval(int32_t device, const double *x, const double *y, const double 
  * work is queued on `stream` (a cudaStream_t, NULL = default); err (device int)
  * gets bit 0 set if a tensor-core completion wait timed out. */
 int mpm_mlp_nparams(void);
+#define MPM_MLP_RESIDUAL 1   /* flags: the network predicts out - feat[0..5] (the correction) */
 int mpm_mlp_forward(const float *params, const float *norm, const float *feat, float *out, int64_t n,
-                    int *err, void *stream);
+                    int32_t flags, int *err, void *stream);
 /* Adds the gradient of 1/2 * inv_btot * sum (MLP(x) - y)^2 (normalised units)
  * over the n samples to grad, and that loss to *loss. */
 int mpm_mlp_grad(const float *params, const float *norm, const float *feat, const float *target, int64_t n,
-                 float inv_btot, float *grad, float *loss, int *err, void *stream);
+                 float inv_btot, int32_t flags, float *grad, float *loss, int *err, void *stream);
 /* One Adam step (bias correction for step count `step` >= 1); zeroes grad. */
 int mpm_mlp_adam(float *params, float *grad, float *m, float *v, float lr, float b1, float b2, float eps,
                  int64_t step, void *stream);
+
+/* The surrogate inside the step (3D Drucker-Prager): with on = 1 every
+ * yielding particle's return is deferred, the MLP (params / norm: HOST arrays
+ * as above, copied) predicts it, and the prediction is kept when its yield
+ * residual |f| / max(kphi, |qphi sigma_m|, sref) is at most tol, else the plain
+ * return (dpP!) is used; plastic strains follow the plain return's closed-form
+ * multiplier.  Counts in mpm_stats.surr_rows / surr_fallbacks.  on = 0
+ * restores the plain return. */
+int mpm_set_surrogate(mpm_handle *h, const float *params, const float *norm, int32_t flags, float tol, float sref,
+                      int32_t on);
+/* Training samples from plain steps: one yielding particle in `every` (hashed
+ * by index and step) writes its 16 features (trial stress 6, strain increment
+ * 6, plastic strain, cohesion, friction, 0) to feat and the plain return's
+ * stress to target (DEVICE arrays of cap rows); *count (device) counts rows
+ * offered, rows beyond cap are dropped.  every = 0 stops logging. */
+int mpm_log_samples(mpm_handle *h, float *feat, float *target, uint32_t *count, uint32_t cap, uint32_t every);
 
 /* ---- diagnostics ---- */
 /* sizeof(mpm_desc), sizeof(mpm_view), sizeof(mpm_host_views), sizeof(mpm_stats):

@@ -36,7 +36,7 @@ EXPORTS = [
     "mpm_download_grid", "mpm_get_stats", "mpm_last_error", "mpm_peak_bandwidth",
     "mpm_set_profiling", "mpm_get_kernel_times", "mpm_abi_sizes", "mpm_cell_order_noalloc",
     "mpm_grf_eval", "mpm_set_tuning", "mpm_get_tuning", "mpm_autotune",
-    "mpm_mlp_nparams", "mpm_mlp_forward", "mpm_mlp_grad", "mpm_mlp_adam",
+    "mpm_mlp_nparams", "mpm_mlp_forward", "mpm_mlp_grad", "mpm_mlp_adam", "mpm_set_surrogate", "mpm_log_samples",
 ]
 NOALLOC_MAX_PARTICLES = 1 << 19
 NOALLOC_MAX_KEYS = 1 << 19
@@ -77,6 +77,7 @@ class Stats(C.Structure):
         ("launches", C.c_int64),
         ("error_flags", C.c_int32), ("kernels_per_step", C.c_int32),
         ("last_step_ms", C.c_double), ("device_bytes", C.c_double),
+        ("surr_rows", C.c_int64), ("surr_fallbacks", C.c_int64),
     ]
 
 
@@ -144,9 +145,11 @@ def lib():
     L.mpm_get_tuning.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.mpm_autotune.argtypes = [vp, C.c_double, C.c_double, C.c_int64, C.POINTER(C.c_double),
                                C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32]
+    L.mpm_set_surrogate.argtypes = [vp, vp, vp, C.c_int32, C.c_float, C.c_float, C.c_int32]
+    L.mpm_log_samples.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_uint32]
     L.mpm_mlp_nparams.argtypes = []
-    L.mpm_mlp_forward.argtypes = [vp, vp, vp, vp, C.c_int64, vp, vp]
-    L.mpm_mlp_grad.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_float, vp, vp, vp, vp]
+    L.mpm_mlp_forward.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_int32, vp, vp]
+    L.mpm_mlp_grad.argtypes = [vp, vp, vp, vp, C.c_int64, C.c_float, C.c_int32, vp, vp, vp, vp]
     L.mpm_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int64, vp]
     L.mpm_grf_eval.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                C.c_double, C.c_void_p]

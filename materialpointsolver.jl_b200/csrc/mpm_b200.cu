@@ -49,12 +49,19 @@ struct KTimer {
 
 }  // namespace
 
+namespace mpm_detail {
+cudaError_t mlp_forward_prepare();
+cudaError_t mlp_forward_dev(const float *P, const float *norm, const float *feat, float *out, int64_t cap,
+                            const uint32_t *n_dev, int residual, int *err, cudaStream_t st, int nsm);
+}
+
 struct GraphCache {
     cudaGraphExec_t exec = nullptr;
     double dt = 0;
     void *pbuf0 = nullptr;
     int sort_every = 0;
     bool tiled = false;
+    int surr_mode = 0;
     int64_t launches = 0, steps = 0, sorts = 0;
 };
 
@@ -69,6 +76,15 @@ struct mpm_handle {
     bool use_graphs = true;  // replay captured step blocks (MPM_B200_GRAPHS=0 turns it off)
     GraphCache graph;
     int64_t graph_launches = 0;
+    // stress-return surrogate: 1 = log samples into caller buffers, 2 = infer
+    int surr_mode = 0;
+    mpm::SurrCtx surr{};
+    float *surr_params = nullptr, *surr_norm = nullptr, *surr_out = nullptr, *surr_feat = nullptr;
+    uint32_t *surr_cnt = nullptr, *surr_list = nullptr;
+    unsigned long long *surr_stats = nullptr;   // rows deferred, fallbacks
+    int *surr_err = nullptr;
+    float surr_tol = 1e-3f, surr_sref = 1e3f;
+    int surr_residual = 0;   // the network predicts the correction to the trial stress
     bool acc_valid = false;     // grid accumulators hold the P2G of the current particles
     double acc_Ti = 0.0;
     int64_t steps_done = 0, sorts_done = 0, since_sort = 1 << 30;
@@ -421,6 +437,9 @@ template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, do
     sp.va = h->d.va;
     sp.need_vs = (h->d.PIC != 0.0 || h->d.va == MPM_VA_V) ? 1 : 0;
     sp.np = h->d.np;
+    sp.surr = h->surr;
+    sp.surr.mode = (D == 3 && h->d.constitutive == MPM_DRUCKERPRAGER) ? h->surr_mode : 0;
+    sp.surr.salt = (uint32_t)(h->steps_done * 0x9E3779B9ull);
     return sp;
 }
 
@@ -485,6 +504,25 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
             if (mc3) k_g2p_tile<D, R, D == 3><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
             else k_g2p_tile<D, R><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
         });
+    } else if (sp.surr.mode == 2 && sp.plastic && np) {
+        // surrogate: G2P + update with the yielding particles' returns deferred,
+        // the MLP over the deferred rows, accept-or-fallback, then the scatter
+        L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+        CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
+        CK(cudaMemsetAsync(h->surr_cnt, 0, 4, h->stream));
+        L.run("g2p", [&] { k_g2p<D, R, false><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("mlp", [&] {
+            CK(mpm_detail::mlp_forward_dev(h->surr_params, h->surr_norm, h->surr_feat, h->surr_out, np, h->surr_cnt,
+                                           h->surr_residual, h->surr_err, h->stream, h->nsm));
+        });
+        if constexpr (D == 3) {
+            L.run("surr_fix", [&] {
+                k_surr_fix<R><<<h->nsm * 8, 256, 0, h->stream>>>(P, g, sp.surr, h->surr_out, h->surr_tol, h->surr_sref,
+                                                              h->surr_stats);
+            });
+        }
+        L.run("p2g", [&] { k_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
     } else {
         if (np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
@@ -507,7 +545,7 @@ template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double T
     GraphCache &gc = h->graph;
     const int S = h->sort_every;
     const bool match = gc.exec && gc.dt == dt && gc.pbuf0 == h->pbuf[0] && gc.sort_every == S &&
-                       gc.tiled == h->tiled;
+                       gc.tiled == h->tiled && gc.surr_mode == h->surr_mode;
     if (!match) {
         if (gc.exec) { cudaGraphExecDestroy(gc.exec); gc.exec = nullptr; }
         if (h->tiled) {   // kernel attributes are set outside the capture
@@ -533,6 +571,7 @@ template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double T
         gc.pbuf0 = h->pbuf[0];
         gc.sort_every = S;
         gc.tiled = h->tiled;
+        gc.surr_mode = h->surr_mode;
         gc.launches = h->launches - l0;
         gc.steps = h->steps_done - s0;
         gc.sorts = h->sorts_done - q0;
@@ -560,7 +599,8 @@ template <int D, typename R> void run_steps(mpm_handle *h, double dt, double Ti0
     double Ti = Ti0;
     const int64_t block = 2 * (int64_t)h->sort_every;
     for (int64_t s = 0; s < nsteps;) {
-        if (h->use_graphs && !h->profiling && Ti >= h->d.Te && h->since_sort >= h->sort_every &&
+        // (logging mode draws a new sample of particles every step: no replay)
+        if (h->use_graphs && !h->profiling && h->surr_mode != 1 && Ti >= h->d.Te && h->since_sort >= h->sort_every &&
             nsteps - s >= block) {
             graph_block<D, R>(h, dt, Ti);
             for (int64_t k = 0; k < block; ++k) Ti = next_t(Ti);
@@ -889,6 +929,11 @@ int check_flags(mpm_handle *h) {
     if (f & ERR_J) throw Err{MPM_E_NONPOSITIVE_J, "det(F) <= 0 on some particle"};
     if (f & ERR_OOG) throw Err{MPM_E_OUT_OF_GRID, "a particle's uGIMP stencil left the grid (pad the grid by >= 2 cells)"};
     if (f & ERR_OVF) throw Err{MPM_E_CELL_OVERFLOW, "more than 4096 particles in one cell"};
+    if (h->surr_err) {
+        int se = 0;
+        CK(cudaMemcpy(&se, h->surr_err, 4, cudaMemcpyDeviceToHost));
+        if (se) throw Err{MPM_E_CUDA, "surrogate: a tensor-core completion wait timed out"};
+    }
     return 0;
 }
 
@@ -1057,6 +1102,73 @@ int mpm_step(mpm_handle *h, double dt, double Ti0, int64_t nsteps, double *Ti_ou
     return rc;
 }
 
+int mpm_set_surrogate(mpm_handle *h, const float *params, const float *norm, int32_t flags, float tol, float sref,
+                      int32_t on) {
+    if (!h) return MPM_E_ARG;
+    try {
+        CK(cudaSetDevice(h->dev));
+        if (!on) {
+            if (h->surr_mode == 2) h->surr_mode = 0;
+            return MPM_OK;
+        }
+        if (!params || !norm || !(tol > 0) || !(sref > 0)) throw Err{MPM_E_ARG, "surrogate: params, norm, tol > 0, sref > 0"};
+        if (h->d.dim != 3 || h->d.constitutive != MPM_DRUCKERPRAGER)
+            throw Err{MPM_E_UNSUPPORTED, "the surrogate replaces the 3D Drucker-Prager return"};
+        const int64_t np = h->d.np;
+        const int npar = mpm_mlp_nparams();
+        if (!h->surr_params) {
+            h->surr_params = (float *)dalloc(h, (size_t)npar * 4);
+            h->surr_norm = (float *)dalloc(h, 64 * 4);
+            h->surr_feat = (float *)dalloc(h, (size_t)std::max<int64_t>(np, 1) * 16 * 4);
+            h->surr_out = (float *)dalloc(h, (size_t)std::max<int64_t>(np, 1) * 6 * 4);
+            h->surr_list = (uint32_t *)dalloc(h, (size_t)std::max<int64_t>(np, 1) * 4);
+            h->surr_cnt = (uint32_t *)dalloc(h, 4);
+            h->surr_stats = (unsigned long long *)dalloc(h, 16);
+            h->surr_err = (int *)dalloc(h, 4);
+            CK(cudaMemset(h->surr_stats, 0, 16));
+            CK(cudaMemset(h->surr_err, 0, 4));
+            CK(cudaMemset(h->surr_cnt, 0, 4));
+        }
+        CK(cudaMemcpy(h->surr_params, params, (size_t)npar * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->surr_norm, norm, 64 * 4, cudaMemcpyHostToDevice));
+        CK(mpm_detail::mlp_forward_prepare());
+        h->surr_tol = tol;
+        h->surr_sref = sref;
+        h->surr_residual = flags & 1;
+        h->surr = mpm::SurrCtx{};
+        h->surr.cap = (uint32_t)np;
+        h->surr.feat = h->surr_feat;
+        h->surr.cnt = h->surr_cnt;
+        h->surr.list = h->surr_list;
+        h->surr_mode = 2;
+        return MPM_OK;
+    } catch (const Err &e) { return fail(h, e); }
+}
+
+int mpm_log_samples(mpm_handle *h, float *feat, float *target, uint32_t *count, uint32_t cap, uint32_t every) {
+    if (!h) return MPM_E_ARG;
+    if (every == 0) {
+        if (h->surr_mode == 1) { h->surr_mode = 0; h->surr = mpm::SurrCtx{}; }
+        return MPM_OK;
+    }
+    if (!feat || !target || !count || cap == 0) {
+        h->last_error = "mpm_log_samples: feat, target, count and cap > 0 are required";
+        return MPM_E_ARG;
+    }
+    if (h->d.dim != 3 || h->d.constitutive != MPM_DRUCKERPRAGER) {
+        h->last_error = "sample logging covers the 3D Drucker-Prager return";
+        return MPM_E_UNSUPPORTED;
+    }
+    h->surr = mpm::SurrCtx{};
+    h->surr.every = every;
+    h->surr.cap = cap;
+    h->surr.feat = feat;
+    h->surr.tgt = target;
+    h->surr.cnt = count;
+    h->surr_mode = 1;
+    return MPM_OK;
+}
+
 int mpm_set_tuning(mpm_handle *h, int32_t sort_every, int32_t tiled) {
     if (!h) return MPM_E_ARG;
     if (sort_every < 1 || sort_every > 1024 || (tiled != 0 && tiled != 1)) {
@@ -1199,6 +1311,13 @@ int mpm_get_stats(mpm_handle *h, mpm_stats *s) {
     s->kernels_per_step = h->kernels_per_step;
     s->last_step_ms = h->last_step_ms;
     s->device_bytes = (double)h->bytes;
+    if (h->surr_stats) {
+        unsigned long long st[2] = {0, 0};
+        if (cudaMemcpy(st, h->surr_stats, sizeof(st), cudaMemcpyDeviceToHost) == cudaSuccess) {
+            s->surr_rows = (int64_t)st[0];
+            s->surr_fallbacks = (int64_t)st[1];
+        }
+    }
     return MPM_OK;
 }
 

@@ -147,6 +147,23 @@ template <int D, typename R> __device__ __forceinline__ int block_node(const GDe
     return D == 2 ? ix * g.nny + iy : (iz * g.nnx + ix) * g.nny + iy;
 }
 
+// Stress-return surrogate hooks of the particle pass (3D Drucker-Prager).
+//   mode 1: run the plain return and log a sample of the yielding particles
+//           (features: trial stress 6, strain increment 6, plastic strain,
+//           cohesion, friction; target: returned stress 6);
+//   mode 2: defer every yielding particle: keep its trial stress, write its
+//           features and index to the work list (the surrogate and the
+//           fallback finish them before the scatter).
+struct SurrCtx {
+    int mode;
+    uint32_t every, salt;   // mode 1: keep a yielding particle if hash(i, salt) % every == 0
+    uint32_t cap;           // rows of feat / tgt / list
+    float *feat;            // cap x 16
+    float *tgt;             // cap x 6 (mode 1)
+    uint32_t *cnt;          // rows written (may exceed cap: extra rows are dropped)
+    uint32_t *list;         // mode 2: particle index of each row
+};
+
 struct StepParams {
     double dt;
     double G;        // gravity of the scatter (P2G) in this launch
@@ -156,6 +173,7 @@ struct StepParams {
     int va;          // 0 = :a, 1 = :v
     int need_vs;     // DM gathers grid vs
     int mc3d;        // 3D Mohr-Coulomb: 0 elastic predictor only (literal), 1 restated return
+    SurrCtx surr;
     int64_t np;
 };
 
@@ -507,6 +525,47 @@ __global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
     }
 }
 
+// Does the Drucker-Prager return change this trial stress (the shear or
+// tension branch of dpP!, druckerprager.jl:89-155)?
+// 0: elastic, 1: shear branch, 2: tension branch (3D)
+template <typename R> __device__ __forceinline__ int dp_branch(const R *s, const Mat<R> &M) {
+    const R sm = (s[0] + s[1] + s[2]) * R(0.333333);
+    const R d0 = s[0] - sm, d1 = s[1] - sm, d2 = s[2] - sm;
+    const R tau = sqrt(R(0.5) * (d0 * d0 + d1 * d1 + d2 * d2) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+    const R fs = tau + M.qphi * sm - M.kphi;
+    const R BF = (tau - M.tb) - (M.ab * (sm - M.st));
+    if ((sm < M.st) && (fs > R(0))) return 1;
+    if (sm >= M.st) return BF > R(0) ? 1 : 2;
+    return 0;
+}
+template <typename R> __device__ __forceinline__ bool dp_yielding(const R *s, const Mat<R> &M) {
+    return dp_branch<R>(s, M) != 0;
+}
+
+__device__ __forceinline__ bool hash_keep(int64_t i, uint32_t salt, uint32_t every) {
+    uint32_t x = (uint32_t)i * 0x9E3779B1u ^ salt;
+    x ^= x >> 16; x *= 0x85EBCA6Bu; x ^= x >> 13; x *= 0xC2B2AE35u; x ^= x >> 16;
+    return every <= 1 || x % every == 0;
+}
+
+// one row of surrogate features (and, when `out` is given, its target)
+template <typename R>
+__device__ __forceinline__ void surr_features(const SurrCtx &c, int64_t i, const R *trial, const R *de, R eq,
+                                              const Mat<R> &M, const R *out) {
+    const uint32_t r = atomicAdd(c.cnt, 1u);
+    if (r >= c.cap) return;
+    float4 *f = reinterpret_cast<float4 *>(c.feat + (size_t)r * 16);
+    f[0] = make_float4((float)trial[0], (float)trial[1], (float)trial[2], (float)trial[3]);
+    f[1] = make_float4((float)trial[4], (float)trial[5], (float)de[0], (float)de[1]);
+    f[2] = make_float4((float)de[2], (float)de[3], (float)de[4], (float)de[5]);
+    f[3] = make_float4((float)eq, (float)M.c, (float)M.phi, 0.0f);
+    if (out) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) c.tgt[(size_t)r * 6 + k] = (float)out[k];
+    }
+    if (c.list) c.list[r] = (uint32_t)i;
+}
+
 // Everything of G2P_OS! after the gathers, plus liE! and dpP!/mcP! and the
 // DM1 position update: x (in/out, FP64), tT = ΣN·vsT, dF = ΣΔu⊗∇N.  Stores
 // the particle and returns the new stress s and volume vol for the next P2G.
@@ -587,8 +646,20 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
     lin_elastic<D, R>(s, dF, de, M, srot);
     if (sp.plastic && (sp.constitutive == 1 || (sp.constitutive == 2 && D == 2))) {
         R eq = ldcs(P.epsq + i), ek = ldcs(P.epsk + i);
-        if (sp.constitutive == 1) drucker_prager<D, R>(s, eq, ek, M);
-        else mohr_coulomb_2d<R>(s, eq, ek, M);
+        if (D == 3 && sp.constitutive == 1 && sp.surr.mode == 2) {
+            if (dp_yielding<R>(s, M)) surr_features<R>(sp.surr, i, s, de, eq, M, nullptr);
+        } else if (D == 3 && sp.constitutive == 1 && sp.surr.mode == 1) {
+            R trial[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) trial[k] = s[k];
+            const R eq0 = eq;
+            drucker_prager<D, R>(s, eq, ek, M);
+            if (eq != eq0 && hash_keep(i, sp.surr.salt, sp.surr.every)) surr_features<R>(sp.surr, i, trial, de, eq0, M, s);
+        } else if (sp.constitutive == 1) {
+            drucker_prager<D, R>(s, eq, ek, M);
+        } else {
+            mohr_coulomb_2d<R>(s, eq, ek, M);
+        }
         stcs(P.epsq + i, eq);
         stcs(P.epsk + i, ek);
     } else if (MC3 && D == 3 && sp.plastic && sp.constitutive == 2) {
@@ -686,6 +757,57 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
         for (int d = 0; d < D; ++d) v[d] = ldcs(P.v[d] + i);
         if (D == 2) v[2] = R(0);
         p2g_scatter<D, R>(g, w, ldcs(P.m + i), vol, v, s, (R)sp.G);
+    }
+}
+
+// Finish the deferred returns: accept the surrogate's stress when its yield
+// residual |f(s_hat)| / max(kphi, |qphi s_hat_m|, s_ref) is within tol (f of the
+// branch the trial stress takes: the shear cone, or the tension cut-off
+// s_m = st), else fall back to the plain return.  The plastic strains follow
+// the plain return's closed-form multiplier either way.  stats[0] += rows,
+// stats[1] += fallbacks.
+template <typename R>
+__global__ void __launch_bounds__(256) k_surr_fix(PDev<3, R> P, GDev<R> g, SurrCtx c, const float *out, float tol,
+                                                  float sref, unsigned long long *stats) {
+    const uint32_t n = min(*c.cnt, c.cap);
+    uint32_t nfall = 0, nrows = 0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int64_t i = c.list[k];
+        Mat<R> M = g.mat[P.mat[i]];
+        if (P.coh) {
+            const R cc = P.coh[i];
+            M.c = cc;
+            M.kphi = cc * M.kc;
+            M.st = fmin(M.sigt, M.kphi / M.qphi);
+            M.tb = M.kphi - M.qphi * M.st;
+        }
+        R sp[6], sh[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) { sp[q] = P.sig[q][i]; sh[q] = (R)out[(size_t)k * 6 + q]; }
+        R eq = P.epsq[i], ek = P.epsk[i];
+        const bool tension = dp_branch<R>(sp, M) == 2;
+        drucker_prager<3, R>(sp, eq, ek, M);   // the plain return: fallback and plastic strains
+        const R hm = (sh[0] + sh[1] + sh[2]) * R(0.333333);
+        const R d0 = sh[0] - hm, d1 = sh[1] - hm, d2 = sh[2] - hm;
+        const R htau = sqrt(R(0.5) * (d0 * d0 + d1 * d1 + d2 * d2) + sh[3] * sh[3] + sh[4] * sh[4] + sh[5] * sh[5]);
+        const R scale = fmax(fmax(M.kphi, fabs(M.qphi * hm)), (R)sref);
+        const R resid = tension ? fabs(hm - M.st) : fabs(htau + M.qphi * hm - M.kphi);
+        const bool ok = isfinite((double)resid) && resid <= (R)tol * scale;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) P.sig[q][i] = ok ? sh[q] : sp[q];
+        P.epsq[i] = eq;
+        P.epsk[i] = ek;
+        nfall += ok ? 0u : 1u;
+        nrows += 1u;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nfall += __shfl_xor_sync(0xffffffffu, nfall, o);
+        nrows += __shfl_xor_sync(0xffffffffu, nrows, o);
+    }
+    if ((threadIdx.x & 31) == 0 && nrows) {
+        atomicAdd(&stats[0], (unsigned long long)nrows);
+        atomicAdd(&stats[1], (unsigned long long)nfall);
     }
 }
 

@@ -146,7 +146,8 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t trow, const float *bias
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(TILE) k_mlp_forward(const float *__restrict__ P, const float *__restrict__ norm,
                                                       const float *__restrict__ feat, float *__restrict__ out,
-                                                      int64_t n, int *err) {
+                                                      int64_t n, const uint32_t *n_dev, int residual, int *err) {
+    if (n_dev) n = min(n, (int64_t)*n_dev);   // rows counted on the device, capped by the buffers
     extern __shared__ __align__(128) uint8_t smem_raw[];
     uint8_t *p = smem_raw;
     Smem S;
@@ -221,7 +222,8 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const float *__restrict__ 
         tmem_ld16(trow, z);
         if (row < n) {
 #pragma unroll
-            for (int o = 0; o < 6; ++o) out[row * 6 + o] = (z[o] + S.bias[192 + o]) * S.norm[48 + o] + S.norm[32 + o];
+            for (int o = 0; o < 6; ++o)
+                out[row * 6 + o] = (z[o] + S.bias[192 + o]) * S.norm[48 + o] + S.norm[32 + o] + (residual ? f[o] : 0.0f);
         }
         fence_before_sync();
         __syncthreads();
@@ -234,25 +236,47 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const float *__restrict__ 
 
 }  // namespace
 
+namespace mpm_detail {
+constexpr size_t MLP_FWD_SMEM = 60 * 1024;   // caps residency at 3 CTAs (192 of 512 TMEM columns) per SM
+
+// Make the forward kernel launchable with its shared memory (call outside any
+// stream capture).
+__attribute__((visibility("hidden"))) cudaError_t mlp_forward_prepare() {
+    return cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_FWD_SMEM);
+}
+
+// Forward over min(*n_dev, cap) rows, the count read on the device.
+__attribute__((visibility("hidden"))) cudaError_t mlp_forward_dev(const float *P, const float *norm,
+                                                                 const float *feat, float *out, int64_t cap,
+                                                                 const uint32_t *n_dev, int residual, int *err,
+                                                                 cudaStream_t st, int nsm) {
+    const int64_t ntiles = (cap + TILE - 1) / TILE;
+    const int grid = (int)(ntiles < 3 * nsm ? ntiles : 3 * nsm);
+    if (grid < 1) return cudaSuccess;
+    k_mlp_forward<<<grid, TILE, MLP_FWD_SMEM, st>>>(P, norm, feat, out, cap, n_dev, residual, err);
+    return cudaGetLastError();
+}
+}  // namespace mpm_detail
+
 extern "C" int mpm_mlp_nparams(void) { return NPAR; }
 
 // Forward pass over n samples; all pointers are DEVICE arrays, work on `stream`.
 extern "C" int mpm_mlp_forward(const float *params, const float *norm, const float *feat, float *out, int64_t n,
-                               int *err, void *stream) {
+                               int32_t flags, int *err, void *stream) {
     if (!params || !norm || !err || n < 0 || (n > 0 && (!feat || !out))) {
         mpm_detail::set_global_error("mpm_mlp_forward: invalid arguments");
         return MPM_E_ARG;
     }
     if (n == 0) return MPM_OK;
-    const size_t smem = 60 * 1024;   // caps residency at 3 CTAs (192 of 512 TMEM columns) per SM
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = mpm_detail::MLP_FWD_SMEM;
+    cudaError_t e = mpm_detail::mlp_forward_prepare();
     if (e == cudaSuccess) {
         int dev = 0, nsm = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         const int64_t ntiles = (n + TILE - 1) / TILE;
         const int grid = (int)(ntiles < 3 * nsm ? ntiles : 3 * nsm);
-        k_mlp_forward<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, out, n, err);
+        k_mlp_forward<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, out, n, nullptr, flags & 1, err);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {
@@ -298,7 +322,8 @@ __device__ __forceinline__ void issue_gemm(uint32_t tmem_d, uint32_t a_saddr, ui
 __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ P, const float *__restrict__ norm,
                                                       const float *__restrict__ feat,
                                                       const float *__restrict__ target, int64_t n, float inv_btot,
-                                                      float *__restrict__ grad, float *__restrict__ loss, int *err) {
+                                                      int residual, float *__restrict__ grad, float *__restrict__ loss,
+                                                      int *err) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     uint8_t *p = smem_raw;
     Smem S;
@@ -383,7 +408,7 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ 
                 float d = 0.0f;
                 if (valid && o < 6) {
                     const float yh = z[o] + S.bias[192 + o];
-                    const float y = (target[row * 6 + o] - S.norm[32 + o]) / S.norm[48 + o];
+                    const float y = (target[row * 6 + o] - (residual ? f[o] : 0.0f) - S.norm[32 + o]) / S.norm[48 + o];
                     d = yh - y;
                     my_loss += 0.5f * d * d * inv_btot;
                     d *= inv_btot;
@@ -471,7 +496,8 @@ __global__ void k_adam(float *P, float *G, float *M, float *V, int npar, float l
 // arrays), ADDED to grad[mpm_mlp_nparams()]; the loss is added to *loss.
 // inv_btot scales both (1 / batch size for a mean).
 extern "C" int mpm_mlp_grad(const float *params, const float *norm, const float *feat, const float *target,
-                            int64_t n, float inv_btot, float *grad, float *loss, int *err, void *stream) {
+                            int64_t n, float inv_btot, int32_t flags, float *grad, float *loss, int *err,
+                            void *stream) {
     if (!params || !norm || !grad || !loss || !err || n < 0 || (n > 0 && (!feat || !target))) {
         mpm_detail::set_global_error("mpm_mlp_grad: invalid arguments");
         return MPM_E_ARG;
@@ -485,8 +511,8 @@ extern "C" int mpm_mlp_grad(const float *params, const float *norm, const float 
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         const int64_t ntiles = (n + TILE - 1) / TILE;
         const int grid = (int)(ntiles < nsm ? ntiles : nsm);
-        k_mlp_grad<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, target, n, inv_btot, grad, loss,
-                                                              err);
+        k_mlp_grad<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, target, n, inv_btot, flags & 1,
+                                                              grad, loss, err);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {

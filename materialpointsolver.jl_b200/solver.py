@@ -170,6 +170,29 @@ class DeviceModel:
                                            C.byref(t), ms, 8), self.h)
         return Tout.value, s.value, bool(t.value), list(ms)
 
+    # stress-return surrogate (no counterpart in the reference)
+    def set_surrogate(self, sur, tol=1e-3, sref=1e3):
+        """Replace the 3D Drucker-Prager return by the trained surrogate `sur`
+        (surrogate.Surrogate), with the yield-residual acceptance test; None
+        restores the plain return."""
+        if sur is None:
+            _lib.check(_lib.lib().mpm_set_surrogate(self.h, None, None, 0, 0.0, 0.0, 0), self.h)
+            return
+        P = np.ascontiguousarray(sur.params(), np.float32)
+        N = np.ascontiguousarray(sur.norm.cpu().numpy(), np.float32)
+        _lib.check(_lib.lib().mpm_set_surrogate(self.h, P.ctypes.data, N.ctypes.data, sur.flags, float(tol),
+                                                float(sref), 1), self.h)
+
+    def log_samples(self, feat, target, count, every):
+        """Log training samples of the plain return into device tensors
+        (feat: cap x 16, target: cap x 6 FP32, count: 1 int32); every = 0 stops."""
+        if every == 0:
+            _lib.check(_lib.lib().mpm_log_samples(self.h, None, None, None, 0, 0), self.h)
+            return
+        cap = min(feat.shape[0], target.shape[0])
+        _lib.check(_lib.lib().mpm_log_samples(self.h, feat.data_ptr(), target.data_ptr(), count.data_ptr(), cap,
+                                              int(every)), self.h)
+
     # clean_device! (devicehelpfunc_cuda.jl:71-100)
     def close(self):
         if getattr(self, "h", None):

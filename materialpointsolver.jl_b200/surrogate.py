@@ -53,11 +53,14 @@ def unpack(P):
     return [(P[ow:ow + k * n].reshape(k, n), P[ob:ob + n]) for (ow, ob), (k, n) in zip(offsets(), LAYERS)]
 
 
-def make_norm(feat, target):
-    """Per-column mean / std of features (15) and targets (6), padded to the
-    64-float layout the kernels read; constant columns get std 1."""
+def make_norm(feat, target, residual=False):
+    """Per-column mean / std of features (15) and targets (6) -- of the
+    correction target - trial stress when `residual` -- padded to the 64-float
+    layout the kernels read; constant columns get std 1."""
     feat = np.asarray(feat, np.float64)
     target = np.asarray(target, np.float64)
+    if residual:
+        target = target - feat[:, :NO]
     norm = np.zeros(64, np.float32)
     fm, fs = feat[:, :NF].mean(0), feat[:, :NF].std(0)
     tm, ts = target.mean(0), target.std(0)
@@ -81,9 +84,13 @@ def pad_features(feat):
 class Surrogate:
     """Parameters, normalisation and Adam state on one GPU."""
 
-    def __init__(self, params=None, norm=None, device=0, seed=0):
+    def __init__(self, params=None, norm=None, device=0, seed=0, residual=True):
         import torch
         self.torch = torch
+        # residual: the network predicts the plastic correction (returned minus
+        # trial stress), which is small where the trial barely yields
+        self.residual = bool(residual)
+        self.flags = 1 if self.residual else 0
         self.dev = torch.device("cuda", device)
         L = _lib.lib()
         self.npar = L.mpm_mlp_nparams()
@@ -111,7 +118,9 @@ class Surrogate:
             raise _lib.MPMError(-2, "tensor-core completion wait timed out in the surrogate kernels")
 
     def set_norm(self, feat, target):
-        self.norm.copy_(self.torch.tensor(make_norm(feat, target), device=self.dev))
+        f = feat.cpu().numpy() if hasattr(feat, "cpu") else feat
+        y = target.cpu().numpy() if hasattr(target, "cpu") else target
+        self.norm.copy_(self.torch.tensor(make_norm(f, y, self.residual), device=self.dev))
 
     def forward(self, feat16):
         """feat16: n x 16 FP32 device tensor -> n x 6 FP32 device tensor."""
@@ -120,7 +129,7 @@ class Surrogate:
         n = feat16.shape[0]
         out = t.empty((n, NO), dtype=t.float32, device=self.dev)
         _lib.check(_lib.lib().mpm_mlp_forward(self.P.data_ptr(), self.norm.data_ptr(), feat16.data_ptr(),
-                                              out.data_ptr(), n, self.err.data_ptr(), self._stream()))
+                                              out.data_ptr(), n, self.flags, self.err.data_ptr(), self._stream()))
         return out
 
     def gradient(self, feat16, target, inv_btot=None):
@@ -136,7 +145,7 @@ class Surrogate:
     def _grad(self, feat16, target, inv_btot):
         _lib.check(_lib.lib().mpm_mlp_grad(self.P.data_ptr(), self.norm.data_ptr(), feat16.contiguous().data_ptr(),
                                            target.contiguous().data_ptr(), feat16.shape[0], float(inv_btot),
-                                           self.G.data_ptr(), self.loss.data_ptr(), self.err.data_ptr(),
+                                           self.flags, self.G.data_ptr(), self.loss.data_ptr(), self.err.data_ptr(),
                                            self._stream()))
 
     def train(self, feat16, target, epochs=10, batch=16384, lr=2e-3, seed=0, lr_end=None, log=None):
@@ -168,3 +177,21 @@ class Surrogate:
 
     def params(self):
         return self.P.cpu().numpy()
+
+
+def collect_samples(dev, dt, Ti, nsteps, cap, every=1, device=0):
+    """Run `nsteps` plain steps of a DeviceModel from time Ti while logging
+    training samples of the Drucker-Prager return; returns (features n x 16,
+    targets n x 6 as device tensors, end time)."""
+    import torch
+    d = torch.device("cuda", device)
+    feat = torch.zeros((cap, NFP), dtype=torch.float32, device=d)
+    tgt = torch.zeros((cap, NO), dtype=torch.float32, device=d)
+    cnt = torch.zeros(1, dtype=torch.int32, device=d)
+    dev.log_samples(feat, tgt, cnt, every)
+    try:
+        Ti = dev.step(dt, Ti, nsteps)
+    finally:
+        dev.log_samples(None, None, None, 0)
+    n = min(int(cnt.item()) & 0xFFFFFFFF, cap)
+    return feat[:n], tgt[:n], Ti

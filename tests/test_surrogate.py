@@ -52,7 +52,7 @@ def test_reference_gradient_matches_finite_differences(pkg):
 
 
 def gpu_surrogate(pkg, P, norm):
-    return pkg.surrogate.Surrogate(params=P, norm=norm)
+    return pkg.surrogate.Surrogate(params=P, norm=norm, residual=False)
 
 
 @pytest.mark.gpu
@@ -98,3 +98,17 @@ def test_training_lowers_the_loss(pkg, gpu_lib):
     losses = sur.train(torch.tensor(feat, device="cuda"), torch.tensor(target, device="cuda"), epochs=15,
                        batch=2048, lr=3e-3)
     assert losses[-1] < 0.1 * losses[0], losses
+
+
+@pytest.mark.gpu
+def test_residual_mode_adds_the_trial_stress(pkg, gpu_lib):
+    """With the residual flag the network's output is the correction: the
+    returned stress is trial + MLP, i.e. the plain output plus features 0..5."""
+    import torch
+    feat, target, P, norm = rand_case(pkg, 500, seed=7)
+    a = pkg.surrogate.Surrogate(params=P, norm=norm, residual=False)
+    b = pkg.surrogate.Surrogate(params=P, norm=norm, residual=True)
+    x = torch.tensor(feat, device="cuda")
+    oa = a.forward(x).cpu().numpy()
+    ob = b.forward(x).cpu().numpy()
+    assert np.allclose(ob, oa + feat[:, :6], rtol=1e-6, atol=1e-5 * np.abs(oa).max())

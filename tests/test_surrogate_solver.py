@@ -1,0 +1,85 @@
+"""The surrogate inside the step (3D Drucker-Prager slope with a lognormal
+cohesion field): samples logged from plain steps are exact plain returns; with
+an acceptance tolerance of zero every deferred return falls back and the run
+equals the plain one; a network trained on the logged samples by the
+library's tensor-core kernels takes over a large share of the returns (an
+untrained one almost none) and keeps the run within the stated error of the
+plain step."""
+import numpy as np
+import pytest
+
+from helpers import fresh_particles, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def slope(pkg):
+    return pkg.workloads.slope_3d(h=0.5, domain=(20.0, 4.0, 10.0), height=3.0, crest=2.0, corr_len=1.0, nh=500,
+                                  Te=0.0, gpu_precision="mixed", seed=31, c_mean=1.0e3)
+
+
+def run(pkg, sur=None, tol=1e-3, nsteps=100):
+    c = slope(pkg)
+    d = pkg.DeviceModel(c.args, c.grid, c.mp, c.attr, c.bc)
+    if sur is not None:
+        d.set_surrogate(sur, tol=tol, sref=1e3)
+    d.step(c.dt, 0.0, nsteps)
+    out = fresh_particles(pkg, c.mp)
+    d.download(pkg._lib.F_REFERENCE, out)
+    st = d.stats()
+    d.close()
+    return c, out, st
+
+
+def runout(c, out):
+    return out.xi[:, 0].max() - c.mp.xi[:, 0].max()
+
+
+@pytest.fixture(scope="module")
+def samples(pkg, gpu_lib):
+    c = slope(pkg)
+    d = pkg.DeviceModel(c.args, c.grid, c.mp, c.attr, c.bc)
+    feat, tgt, _ = pkg.surrogate.collect_samples(d, c.dt, 0.0, 200, 2_000_000, every=1)
+    d.close()
+    return c, feat, tgt
+
+
+def test_logged_samples_are_plain_returns(pkg, orc, samples):
+    c, feat, tgt = samples
+    assert feat.shape[0] > 100_000
+    f, y = feat.cpu().numpy(), tgt.cpu().numpy()
+    K, G = c.meta["K"], c.meta["G"]
+    for i in np.random.default_rng(0).choice(len(f), 200, replace=False):
+        s, _, _ = orc.dp_point(3, f[i, :6].astype(np.float64), f[i, 12], 0.0, K, G, f[i, 13], f[i, 14], 0.0, 0.0)
+        assert np.abs(s - y[i]).max() <= 1e-6 * np.abs(s).max()
+    assert np.abs(f[:, 6:12]).max() > 0 and np.ptp(f[:, 13]) > 0   # strain increments, cohesion field
+
+
+def test_zero_tolerance_is_the_plain_step(pkg, samples):
+    c, feat, tgt = samples
+    sur = pkg.surrogate.Surrogate(seed=2)
+    sur.set_norm(feat, tgt)
+    cp, op, _ = run(pkg)
+    cs, os_, st = run(pkg, sur, tol=1e-30)
+    assert st.surr_rows > 0 and st.surr_fallbacks == st.surr_rows
+    assert rel(os_.xi - cs.mp.xi, op.xi - cp.mp.xi) < 1e-5
+    assert rel(os_.sig, op.sig) < 1e-4
+
+
+def test_trained_surrogate_gains(pkg, samples):
+    c, feat, tgt = samples
+    S = pkg.surrogate
+    sur = S.Surrogate(seed=1)
+    sur.set_norm(feat, tgt)
+    untrained = S.Surrogate(params=sur.params(), norm=sur.norm.cpu().numpy())
+    losses = sur.train(feat, tgt, epochs=80, batch=4096, lr=3e-3, lr_end=5e-5)
+    assert losses[-1] < 0.3 * losses[0]
+    cp, op, _ = run(pkg)
+    _, ou, su = run(pkg, untrained)
+    cs, os_, st = run(pkg, sur)
+    acc_u = 1.0 - su.surr_fallbacks / su.surr_rows
+    acc_t = 1.0 - st.surr_fallbacks / st.surr_rows
+    assert acc_t > 0.3 and acc_t > 5.0 * acc_u, (acc_t, acc_u)
+    assert rel(os_.xi - cs.mp.xi, op.xi - cp.mp.xi) < 1e-2
+    h = c.meta["h"]
+    assert abs(runout(cs, os_) - runout(cp, op)) <= 1e-3 * max(abs(runout(cp, op)), h)
