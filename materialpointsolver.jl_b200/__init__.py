@@ -10,6 +10,7 @@ from .types import (Args2D, Args3D, Grid2D, Grid3D, Particle2D, Particle3D, Prop
 from . import workloads
 from . import randomfield
 from . import surrogate
+from . import precision
 from . import _lib
 from .solver import (DeviceModel, host2device, device2host, clean_device, procedure,
                      materialpointsolver, time_sequence)
