@@ -57,6 +57,10 @@ extern "C" {
 #define MPM_VA_A 0
 #define MPM_VA_V 1
 
+/* update scheme (args.scheme) */
+#define MPM_SCHEME_MUSL 0
+#define MPM_SCHEME_USL 1
+
 /* 3D Mohr-Coulomb: the reference's 3D mcP! body is commented out, so its 3D
  * "mohrcoulomb" run is the elastic predictor only (LITERAL).  RESTATED applies
  * the predictor-corrector Mohr-Coulomb return mapping. */
@@ -94,6 +98,8 @@ typedef struct {
     double Te;             /* Args.Te */
     int32_t time_f32;      /* 1: accumulate Ti in Float32 (reference FP32 mode) */
     int32_t sort_every;    /* re-sort period in steps (0 = library default) */
+    int32_t scheme;        /* MPM_SCHEME_MUSL (OS_MUSL.jl) or MPM_SCHEME_USL (OS_USL.jl) */
+    int32_t reserved;      /* 0 */
 } mpm_desc;
 
 /* A host array view. */

@@ -24,6 +24,7 @@ ERRORS = {
 }
 LINEARELASTIC, DRUCKERPRAGER, MOHRCOULOMB = 0, 1, 2
 PREC_MIXED, PREC_FP64 = 0, 1
+SCHEME_MUSL, SCHEME_USL = 0, 1
 T_F64, T_F32, T_I64, T_I32 = 0, 1, 2, 3
 
 F_XI, F_VS, F_SIG, F_EPS, F_EPSQ, F_EPSK, F_EPSV = (1 << i for i in range(7))
@@ -53,7 +54,7 @@ class Desc(C.Structure):
         ("constitutive", C.c_int32), ("va", C.c_int32), ("mvl", C.c_int32), ("mc3d", C.c_int32),
         ("FLIP", C.c_double), ("PIC", C.c_double), ("zeta_s", C.c_double), ("gravity", C.c_double),
         ("Te", C.c_double),
-        ("time_f32", C.c_int32), ("sort_every", C.c_int32),
+        ("time_f32", C.c_int32), ("sort_every", C.c_int32), ("scheme", C.c_int32), ("reserved", C.c_int32),
     ]
 
 

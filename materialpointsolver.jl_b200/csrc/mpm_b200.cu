@@ -99,6 +99,9 @@ struct mpm_handle {
     void *acc = nullptr, *gat = nullptr, *gvs = nullptr;   // node records (see mpm_kernels.cuh)
     uint8_t *bcmask = nullptr;
     void *bcval = nullptr;
+    void *csigm = nullptr, *comega = nullptr;   // MVL cell sums (R), nc each
+    uint32_t *pcell = nullptr;                   // MVL start-of-step cell per particle
+    int64_t nc = 0;
     uint32_t *bflag = nullptr;   // per node block: touched by a particle window
     uint32_t *blist = nullptr;   // list of the flagged blocks
     uint32_t *bcount = nullptr;  // its length
@@ -211,6 +214,9 @@ template <typename R> GDev<R> gdev_from(mpm_handle *h) {
     g.bcval = (const T4 *)h->bcval;
     g.mat = (const Mat<R> *)h->mat;
     g.err = h->err;
+    g.csigm = (R *)h->csigm;
+    g.comega = (R *)h->comega;
+    g.pcell = h->pcell;
     g.bflag = h->bflag;
     g.blist = h->blist;
     g.bcount = h->bcount;
@@ -435,8 +441,12 @@ template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, do
     sp.constitutive = h->d.constitutive;
     sp.mc3d = h->d.mc3d == MPM_MC3D_RESTATED ? 1 : 0;
     sp.va = h->d.va;
-    sp.need_vs = (h->d.PIC != 0.0 || h->d.va == MPM_VA_V) ? 1 : 0;
+    sp.usl = h->d.scheme == MPM_SCHEME_USL ? 1 : 0;
+    // grid vs is gathered by the :v updates and by the PIC term of MUSL :a (USL :a
+    // maps the updated velocity, which is the vsT record)
+    sp.need_vs = (h->d.va == MPM_VA_V || (h->d.PIC != 0.0 && !sp.usl)) ? 1 : 0;
     sp.np = h->d.np;
+    sp.mvl = h->d.mvl ? 1 : 0;
     sp.surr = h->surr;
     sp.surr.mode = (D == 3 && h->d.constitutive == MPM_DRUCKERPRAGER) ? h->surr_mode : 0;
     sp.surr.salt = (uint32_t)(h->steps_done * 0x9E3779B9ull);
@@ -494,7 +504,7 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
     StepParams sp = make_params<D, R>(h, dt, Ti, gravity_at(h->d, Tn));
     const bool mc3 = sp.mc3d && sp.constitutive == MPM_MOHRCOULOMB;
     L.run("solve", [&] { k_solve<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
-    if (h->tiled) {
+    if (h->tiled && !sp.mvl && !sp.usl && sp.surr.mode != 2) {
         TileList tl{h->tiles, h->ntiles, h->off, h->sg};
         const TiledCfg &c = tiled_cfg<D, R>(h, sp.need_vs);
         if (np) L.run("dmap", [&] { k_dmap_tile<D, R><<<c.grid_dm, 256, c.smem_dm, h->stream>>>(P, g, sp, tl); });
@@ -504,6 +514,35 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
             if (mc3) k_g2p_tile<D, R, D == 3><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
             else k_g2p_tile<D, R><<<c.grid_g2p, 256, c.smem_g2p, h->stream>>>(P, g, sp, tl);
         });
+    } else if (sp.usl && np) {
+        // USL: no double mapping; DM1 (velocity, position) rides in the G2P pass
+        CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
+        if (sp.mvl) {
+            CK(cudaMemsetAsync(h->csigm, 0, (size_t)h->nc * sizeof(R), h->stream));
+            CK(cudaMemsetAsync(h->comega, 0, (size_t)h->nc * sizeof(R), h->stream));
+            L.run("g2p", [&] {
+                if (mc3) k_g2p<D, R, false, D == 3, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                else k_g2p<D, R, false, false, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            });
+            L.run("mvl_p2g", [&] { k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        } else {
+            L.run("g2p_p2g", [&] {
+                if (mc3) k_g2p<D, R, true, D == 3, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                else k_g2p<D, R, true, false, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            });
+        }
+    } else if (sp.mvl && np) {
+        // MVL: update + cell sums, then the cell-averaged mean stress + P2G
+        L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+        CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
+        CK(cudaMemsetAsync(h->csigm, 0, (size_t)h->nc * sizeof(R), h->stream));
+        CK(cudaMemsetAsync(h->comega, 0, (size_t)h->nc * sizeof(R), h->stream));
+        L.run("g2p", [&] {
+            if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_g2p<D, R, false><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+        });
+        L.run("mvl_p2g", [&] { k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
     } else if (sp.surr.mode == 2 && sp.plastic && np) {
         // surrogate: G2P + update with the yielding particles' returns deferred,
         // the MLP over the deferred rows, accept-or-fallback, then the scatter
@@ -969,8 +1008,8 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
               (d->dim == 2 || (d->lpz > 0 && d->lpz <= d->dz))))
             throw Err{MPM_E_ARG, "particle size must satisfy 0 < lp <= h (at most 3 uGIMP nodes per axis)"};
         if (d->constitutive < 0 || d->constitutive > 2) throw Err{MPM_E_UNSUPPORTED, "constitutive model not provided (hyperelastic is out of scope)"};
-        if (d->mvl) throw Err{MPM_E_UNSUPPORTED, "MVL volumetric-locking mitigation is not provided by this backend"};
         if (d->mc3d != MPM_MC3D_LITERAL && d->mc3d != MPM_MC3D_RESTATED) throw Err{MPM_E_ARG, "mc3d must be 0 or 1"};
+        if (d->scheme != MPM_SCHEME_MUSL && d->scheme != MPM_SCHEME_USL) throw Err{MPM_E_ARG, "scheme must be 0 (MUSL) or 1 (USL)"};
         h->d = *d;
         if (h->d.dim == 2) { h->d.nnz = 1; h->d.z1 = 0; h->d.dz = 1; h->d.lpz = 1; }
         h->fp64 = d->precision == MPM_PREC_FP64;
@@ -1002,6 +1041,13 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         size_t nblk = (size_t)h->nbx * h->nby * h->nbz;
         h->bflag = (uint32_t *)dalloc(h, nblk * 4);
         CK(cudaMemset(h->bflag, 0, nblk * 4));
+        if (d->mvl) {
+            h->nc = (d->nnx - 1) * (d->nny - 1) * (d->dim == 3 ? (d->nnz - 1) : 1);
+            const size_t rs = h->fp64 ? 8 : 4;
+            h->csigm = dalloc(h, (size_t)h->nc * rs);
+            h->comega = dalloc(h, (size_t)h->nc * rs);
+            h->pcell = (uint32_t *)dalloc(h, (size_t)std::max<int64_t>(d->np, 1) * 4);
+        }
         h->blist = (uint32_t *)dalloc(h, nblk * 4);
         h->bcount = (uint32_t *)dalloc(h, 4);
         CK(cudaMemset(h->bcount, 0, 4));
@@ -1114,6 +1160,8 @@ int mpm_set_surrogate(mpm_handle *h, const float *params, const float *norm, int
         if (!params || !norm || !(tol > 0) || !(sref > 0)) throw Err{MPM_E_ARG, "surrogate: params, norm, tol > 0, sref > 0"};
         if (h->d.dim != 3 || h->d.constitutive != MPM_DRUCKERPRAGER)
             throw Err{MPM_E_UNSUPPORTED, "the surrogate replaces the 3D Drucker-Prager return"};
+        if (h->d.mvl || h->d.scheme != MPM_SCHEME_MUSL)
+            throw Err{MPM_E_UNSUPPORTED, "the surrogate runs with the MUSL scheme and without MVL"};
         const int64_t np = h->d.np;
         const int npar = mpm_mlp_nparams();
         if (!h->surr_params) {

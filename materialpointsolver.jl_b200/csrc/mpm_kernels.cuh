@@ -62,6 +62,8 @@ template <typename R> struct GDev {
     const T4 *bcval;        // fixed values (NULL when all zero)
     const Mat<R> *mat;
     int *err;
+    R *csigm, *comega;      // MVL: per-cell sum of vol*sigma_m and of vol (NULL when off)
+    uint32_t *pcell;        // MVL: start-of-step cell of each particle
     uint32_t *bflag;        // per node block: 1 if some particle window touched it
     uint32_t *blist;        // the flagged blocks, in the order they were flagged
     uint32_t *bcount;       // number of entries in blist
@@ -173,6 +175,8 @@ struct StepParams {
     int va;          // 0 = :a, 1 = :v
     int need_vs;     // DM gathers grid vs
     int mc3d;        // 3D Mohr-Coulomb: 0 elastic predictor only (literal), 1 restated return
+    int mvl;         // volumetric-locking mitigation (cell-averaged mean stress)
+    int usl;         // USL scheme (OS_USL.jl): no double mapping, Δu = vsT·dt
     SurrCtx surr;
     int64_t np;
 };
@@ -379,7 +383,7 @@ __device__ __forceinline__ void solve_node(const GDev<R> &g, const StepParams &s
     G.b = mk4<R>(as[0], as[1], as[2], 0);
     g.gat[i] = G;
     if (sp.need_vs) g.gvs[i] = mk4<R>(vs[0], vs[1], vs[2], 0);
-    A.a = mk4<R>(m, 0, 0, 0);
+    A.a = mk4<R>(sp.usl ? R(0) : m, 0, 0, 0);   // MUSL keeps m for DM3
     A.b = mk4<R>(0, 0, 0, 0);
     g.acc[i] = A;
 }
@@ -389,8 +393,10 @@ template <int D, typename R>
 __global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
     const uint32_t n = *g.bcount;
     for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
-        const int i = block_node<D, R>(g, (int)g.blist[k], threadIdx.x);
+        const int b = (int)g.blist[k];
+        const int i = block_node<D, R>(g, b, threadIdx.x);
         if (i >= 0) solve_node<D, R>(g, sp, i);
+        if (sp.usl && threadIdx.x == 0) g.bflag[b] = 0u;   // USL has no DM3 to clear it
     }
 }
 
@@ -691,7 +697,7 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
 // dpP!/mcP!.  With FUSE, the next step's P2G scatters the updated particle
 // (resetmpstatus_OS! + P2G_OS! at the new position, gravity sp.G).
 // ---------------------------------------------------------------------------
-template <int D, typename R, bool FUSE, bool MC3 = false>
+template <int D, typename R, bool FUSE, bool MC3 = false, bool USL = false>
 __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g, StepParams sp) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= sp.np) return;
@@ -709,7 +715,11 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
     // the FP32 sum from cancelling when the motion is mostly a translation.
     // Separable sums: per (x, z) column, A = ΣNy·Δu', B = ΣdNy·Δu', T = ΣNy·vsT;
     // then ∂/∂x += dNx·Nz·A, ∂/∂y += Nx·Nz·B, ∂/∂z += Nx·dNz·A, tT += Nx·Nz·T.
-    const auto duc = g.gat[n0 + g.nny + 1 + (D == 3 ? plane : 0)].b;
+    // USL: Δu = vsT·dt (OS_USL.jl), taken from the first half of the record and
+    // scaled after the sums; the DM1 velocity update gathers as / vs alongside.
+    const int ncen = n0 + g.nny + 1 + (D == 3 ? plane : 0);
+    const auto duc = USL ? g.gat[ncen].a : g.gat[ncen].b;
+    R ta[3] = {0, 0, 0}, tv[3] = {0, 0, 0};
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         const R wz = D == 3 ? w[2].N[c] : R(1);
@@ -720,20 +730,32 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
             const R wx = w[0].N[a];
             if (wx == R(0)) continue;
             const int col = n0 + a * g.nny + c * plane;
-            R T[3] = {0, 0, 0}, A[3] = {0, 0, 0}, B[3] = {0, 0, 0};
+            R T[3] = {0, 0, 0}, A[3] = {0, 0, 0}, B[3] = {0, 0, 0}, Sa[3] = {0, 0, 0}, Sv[3] = {0, 0, 0};
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 const R wy = w[1].N[b], gy = w[1].dN[b];
                 if (wy == R(0)) continue;
                 const Node8<R> q = g.gat[col + b];
-                const R u[3] = {q.b.x - duc.x, q.b.y - duc.y, q.b.z - duc.z};
+                const auto du = USL ? q.a : q.b;
+                const R u[3] = {du.x - duc.x, du.y - duc.y, du.z - duc.z};
                 T[0] += wy * q.a.x; T[1] += wy * q.a.y; T[2] += wy * q.a.z;
 #pragma unroll
                 for (int k = 0; k < D; ++k) { A[k] += wy * u[k]; B[k] += gy * u[k]; }
+                if (USL) {
+                    Sa[0] += wy * q.b.x; Sa[1] += wy * q.b.y; Sa[2] += wy * q.b.z;
+                    if (sp.need_vs) {
+                        const auto vv = g.gvs[col + b];
+                        Sv[0] += wy * vv.x; Sv[1] += wy * vv.y; Sv[2] += wy * vv.z;
+                    }
+                }
             }
             const R wxz = wx * wz, gxz = w[0].dN[a] * wz;
 #pragma unroll
             for (int k = 0; k < D; ++k) tT[k] += wxz * T[k];
+            if (USL) {
+#pragma unroll
+                for (int k = 0; k < D; ++k) { ta[k] += wxz * Sa[k]; tv[k] += wxz * Sv[k]; }
+            }
             if (D == 2) {
                 dF[0] += gxz * A[0]; dF[1] += wxz * B[0];
                 dF[2] += gxz * A[1]; dF[3] += wxz * B[1];
@@ -748,8 +770,37 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
             }
         }
     }
+    if (USL) {
+        // Δu = vsT·dt
+        const R dt = (R)sp.dt;
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) dF[k] *= dt;
+        // doublemapping1_a_USL_OS! / doublemapping1_OS! (OS_USL.jl:185-320)
+        const R FLIP = (R)sp.FLIP, PIC = (R)sp.PIC;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const R vo = ldcs(P.v[d] + i);
+            const R vn = sp.va == 0 ? FLIP * vo + PIC * tT[d] + ta[d] * dt : FLIP * (vo + (tT[d] - tv[d])) + PIC * tT[d];
+            stcs(P.v[d] + i, vn);
+        }
+    }
     R s[6], vol;
+    int cell = 0;
+    if (!FUSE && sp.mvl) {
+        // vollock1_OS!: the cell of the step's start (the reference's p2c)
+        int ci[3];
+        particle_cell<D, R>(x, g, ci);
+        const int cx = clampi(ci[0], 0, g.ax[0].nc - 1), cy = clampi(ci[1], 0, g.ax[1].nc - 1);
+        const int cz = D == 3 ? clampi(ci[2], 0, g.ax[2].nc - 1) : 0;
+        cell = (cz * g.ax[0].nc + cx) * g.ax[1].nc + cy;
+    }
     update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol);
+    if (!FUSE && sp.mvl) {
+        const R sm = (s[0] + s[1] + s[2]) * R(0.333333);
+        atomicAdd(&g.csigm[cell], vol * sm);
+        atomicAdd(&g.comega[cell], vol);
+        g.pcell[i] = (uint32_t)cell;
+    }
     if (FUSE) {
         if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
         R v[3];
@@ -758,6 +809,33 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
         if (D == 2) v[2] = R(0);
         p2g_scatter<D, R>(g, w, ldcs(P.m + i), vol, v, s, (R)sp.G);
     }
+}
+
+// vollock2_OS! + the next step's P2G: the particle's mean stress is replaced by
+// the volume-weighted mean of its start-of-step cell (utils_OS.jl:1162-1257),
+// then it scatters at its new position.
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_mvl_p2g(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    constexpr int NV = PDev<D, R>::NV;
+    const uint32_t c = g.pcell[i];
+    const R cm = g.csigm[c] / g.comega[c];
+    R s[6];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) s[k] = P.sig[k][i];
+    const R sm = (s[0] + s[1] + s[2]) * R(0.333333);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s[k] = (s[k] - sm) + cm;
+        P.sig[k][i] = s[k];
+    }
+    double x[3];
+    load_x<D, R>(P, i, x);
+    AxisW<R> w[3];
+    if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
+    R v[3] = {P.v[0][i], P.v[1][i], D == 3 ? P.v[2][i] : R(0)};
+    p2g_scatter<D, R>(g, w, P.m[i], P.vol[i], v, s, (R)sp.G);
 }
 
 // Finish the deferred returns: accept the surrogate's stress when its yield

@@ -72,6 +72,7 @@ def make_desc(args, grid, mp, attr, device=0):
     d.FLIP, d.PIC, d.zeta_s, d.gravity, d.Te = args.FLIP, args.PIC, args.zeta_s, args.gravity, args.Te
     d.time_f32 = 1 if args.precision == "FP32" else 0
     d.sort_every = getattr(args, "sort_every", 0)
+    d.scheme = _lib.SCHEME_USL if getattr(args, "scheme", "MUSL") == "USL" else _lib.SCHEME_MUSL
     return d
 
 
@@ -246,8 +247,8 @@ def materialpointsolver(args, grid, mp, attr, bc, workflow=None, device=0, verbo
     like the reference's ``workflow`` keyword."""
     if args.device != "B200":
         raise ValueError("this package provides the :B200 device backend (args.device = 'B200')")
-    if args.coupling != "OS" or args.scheme != "MUSL":
-        raise NotImplementedError("only the one-phase MUSL scheme is provided")
+    if args.coupling != "OS" or args.scheme not in ("MUSL", "USL"):
+        raise NotImplementedError("the one-phase MUSL and USL schemes are provided")
     if args.basis != "uGIMP":
         raise NotImplementedError("only the uGIMP basis is provided")
     if args.hdf5:

@@ -309,6 +309,52 @@ void orc_solvegrid(orc_model *m, double dt) {
     }
 }
 
+// solvegrid_a_USL_OS! / solvegrid_USL_OS! (src/solvers/OS_USL.jl:147-320 /
+// :24-100): the nodal velocity is advanced in place and the displacement
+// increment comes straight from it (no double mapping).  For :a the updated
+// velocity is also written to vsT, so that doublemapping1_a_USL_OS! -- which
+// maps the updated velocity for both the position and the PIC term -- is the
+// MUSL doublemapping1_a_OS! code path of orc_dm1.
+void orc_solvegrid_usl(orc_model *m, double dt) {
+    const int64_t ni = m->ni;
+    const int D = m->dim;
+    const int64_t *idx[3] = {m->vx_idx, m->vy_idx, m->vz_idx};
+    const double *val[3] = {m->vx_val, m->vy_val, m->vz_val};
+#pragma omp parallel for if (par(m)) schedule(static)
+    for (int64_t i = 0; i < ni; ++i) {
+        double ms_denom = m->g_ms[i] < DBL_EPSILON ? 0.0 : 1.0 / m->g_ms[i];
+        double ss = 0.0;
+        for (int d = 0; d < D; ++d) ss += m->g_fs[i + ni * d] * m->g_fs[i + ni * d];
+        const double dampvs = -m->zeta_s * std::sqrt(ss);
+        if (m->va == ORC_VA_A) {
+            for (int d = 0; d < D; ++d)
+                if (idx[d][i] != 0) m->g_ps[i + ni * d] = val[d][i];
+            for (int d = 0; d < D; ++d) m->g_vs[i + ni * d] = m->g_ps[i + ni * d] * ms_denom;
+            double Fs[3];
+            for (int d = 0; d < D; ++d) Fs[d] = m->g_fs[i + ni * d] + dampvs * sgn(m->g_vs[i + ni * d]);
+            for (int d = 0; d < D; ++d) m->g_vs[i + ni * d] += Fs[d] * dt * ms_denom;
+            for (int d = 0; d < D; ++d) m->g_as[i + ni * d] = Fs[d] * ms_denom;
+            for (int d = 0; d < D; ++d)
+                if (idx[d][i] != 0) m->g_vs[i + ni * d] = val[d][i];
+            for (int d = 0; d < D; ++d)
+                if (idx[d][i] != 0) m->g_as[i + ni * d] = val[d][i];
+            for (int d = 0; d < D; ++d) {
+                m->g_dus[i + ni * d] = m->g_vs[i + ni * d] * dt;
+                m->g_vsT[i + ni * d] = m->g_vs[i + ni * d];
+            }
+        } else {
+            for (int d = 0; d < D; ++d) m->g_vs[i + ni * d] = m->g_ps[i + ni * d] * ms_denom;
+            for (int d = 0; d < D; ++d) {
+                double Fs = m->g_fs[i + ni * d] + dampvs * sgn(m->g_vs[i + ni * d]);
+                m->g_vsT[i + ni * d] = (m->g_ps[i + ni * d] + Fs * dt) * ms_denom;
+            }
+            for (int d = 0; d < D; ++d)
+                if (idx[d][i] != 0) m->g_vsT[i + ni * d] = val[d][i];
+            for (int d = 0; d < D; ++d) m->g_dus[i + ni * d] = m->g_vsT[i + ni * d] * dt;
+        }
+    }
+}
+
 // doublemapping1_a_OS! (utils_OS.jl:745-788 / :856-908) and
 // doublemapping1_OS! (utils_OS.jl:698-743 / :799-854)
 void orc_dm1(orc_model *m, double dt) {
@@ -663,10 +709,15 @@ int orc_procedure(orc_model *m, double dt, double Ti) {
     orc_resetgrid(m);
     orc_resetmp(m);
     orc_p2g(m, G);
-    orc_solvegrid(m, dt);
-    orc_dm1(m, dt);
-    orc_dm2(m);
-    orc_dm3(m, dt);
+    if (m->scheme == 1) {   // USL, src/solvers/OS_USL.jl:102-145, 325-368
+        orc_solvegrid_usl(m, dt);
+        orc_dm1(m, dt);
+    } else {
+        orc_solvegrid(m, dt);
+        orc_dm1(m, dt);
+        orc_dm2(m);
+        orc_dm3(m, dt);
+    }
     orc_g2p(m, dt);
     orc_constitutive(m, Ti);
     if (m->mvl) orc_vollock(m);

@@ -58,6 +58,7 @@ typedef struct {
     double Te, gravity, FLIP, PIC, zeta_s;
     int32_t constitutive, va, mvl, mc3d;
     int32_t nthreads;           /* 0/1: sequential literal order; >1: OpenMP */
+    int32_t scheme;             /* 0: MUSL (OS_MUSL.jl), 1: USL (OS_USL.jl) */
 } orc_model;
 
 /* One call of procedure!(…, Val(:OS), Val(:MUSL), Val(va)), src/solvers/OS_MUSL.jl:12-102 */
@@ -70,6 +71,7 @@ void orc_resetgrid(orc_model *m);
 void orc_resetmp(orc_model *m);
 void orc_p2g(orc_model *m, double G);
 void orc_solvegrid(orc_model *m, double dt);
+void orc_solvegrid_usl(orc_model *m, double dt);
 void orc_dm1(orc_model *m, double dt);
 void orc_dm2(orc_model *m);
 void orc_dm3(orc_model *m, double dt);

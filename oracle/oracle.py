@@ -52,7 +52,7 @@ class OrcModel(C.Structure):
         ("Te", C.c_double), ("gravity", C.c_double), ("FLIP", C.c_double), ("PIC", C.c_double),
         ("zeta_s", C.c_double),
         ("constitutive", C.c_int32), ("va", C.c_int32), ("mvl", C.c_int32), ("mc3d", C.c_int32),
-        ("nthreads", C.c_int32),
+        ("nthreads", C.c_int32), ("scheme", C.c_int32),
     ]
 
 
@@ -180,6 +180,7 @@ class Oracle:
         m.mvl = int(args.MVL)
         m.mc3d = 1 if getattr(args, "mc3d", "literal") == "restated" else 0
         m.nthreads = nthreads
+        m.scheme = 1 if getattr(args, "scheme", "MUSL") == "USL" else 0
         self.m = m
 
     def __getattr__(self, name):

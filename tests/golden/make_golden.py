@@ -26,6 +26,8 @@ CASES = {
     "col2d_le_pic": dict(dim=2, constitutive="linearelastic", steps=3, PIC=0.25, FLIP=0.75),
     "col3d_dp": dict(dim=3, constitutive="druckerprager", steps=3),
     "col3d_le": dict(dim=3, constitutive="linearelastic", steps=3),
+    "col2d_dp_usl": dict(dim=2, constitutive="druckerprager", steps=4, scheme="USL"),
+    "col3d_dp_usl_pic": dict(dim=3, constitutive="druckerprager", steps=3, scheme="USL", PIC=0.2, FLIP=0.8),
 }
 
 

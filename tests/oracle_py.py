@@ -172,8 +172,49 @@ class PyModel:
                     self.gfs[n, 0] += -vol * (dx * sg[ix, 0] + dy * sg[ix, 3] + dz * sg[ix, 5])
                     self.gfs[n, 1] += -vol * (dy * sg[ix, 1] + dx * sg[ix, 3] + dz * sg[ix, 4])
                     self.gfs[n, 2] += -vol * (dz * sg[ix, 2] + dx * sg[ix, 5] + dy * sg[ix, 4]) + NiM * G
-        # solvegrid_a_OS!, utils_OS.jl:547-640
         eps = np.finfo(np.float64).eps
+        if getattr(a, "scheme", "MUSL") == "USL":
+            self._usl_a(dt, eps)
+        else:
+            self._musl_a(dt, eps)
+        # G2P_OS!, utils_OS.jl:1025-1153
+        self._g2p(dt, Ti)
+
+    def _usl_a(self, dt, eps):
+        """solvegrid_a_USL_OS! + doublemapping1_a_USL_OS!, OS_USL.jl:147-320."""
+        a, D = self.args, self.D
+        for i in range(self.ni):
+            md = 0.0 if self.gms[i] < eps else 1.0 / self.gms[i]
+            for d in range(D):
+                if self.bcidx[d][i] != 0:
+                    self.gps[i, d] = self.bcval[d][i]
+            self.gvs[i] = self.gps[i] * md
+            damp = -a.zeta_s * math.sqrt(float(np.sum(self.gfs[i] ** 2)))
+            Fs = [self.gfs[i, d] + damp * sign(self.gvs[i, d]) for d in range(D)]
+            for d in range(D):
+                self.gvs[i, d] += Fs[d] * dt * md
+                self.gas[i, d] = Fs[d] * md
+            for d in range(D):
+                if self.bcidx[d][i] != 0:
+                    self.gvs[i, d] = self.bcval[d][i]
+                    self.gas[i, d] = self.bcval[d][i]
+            self.gdus[i] = self.gvs[i] * dt
+        for ix in range(self.np):
+            tp = np.zeros(D); tv = np.zeros(D)
+            for s in range(self.NIC):
+                Ni = self.Nij[ix, s]
+                if Ni == 0.0:
+                    continue
+                n = self.p2n[ix, s] - 1
+                tp += Ni * self.gvs[n]
+                tv += Ni * self.gas[n]
+            self.xi[ix] += tp * dt
+            self.vs[ix] = a.FLIP * self.vs[ix] + a.PIC * tp + tv * dt
+            self.ps[ix] = self.ms[ix] * self.vs[ix]
+
+    def _musl_a(self, dt, eps):
+        a, D = self.args, self.D
+        # solvegrid_a_OS!, utils_OS.jl:547-640
         for i in range(self.ni):
             md = 0.0 if self.gms[i] < eps else 1.0 / self.gms[i]
             for d in range(D):
@@ -218,7 +259,9 @@ class PyModel:
                 if self.bcidx[d][i] != 0:
                     self.gvs[i, d] = self.bcval[d][i]
             self.gdus[i] = self.gvs[i] * dt
-        # G2P_OS!, utils_OS.jl:1025-1153
+
+    def _g2p(self, dt, Ti):
+        a, D = self.args, self.D
         for ix in range(self.np):
             dF = np.zeros((D, D))
             for s in range(self.NIC):

@@ -115,7 +115,6 @@ def _desc(pkg, **over):
     (dict(dx=0.0), -1, b"cell size"),
     (dict(lpx=0.05), -1, b"particle size"),      # lp > h: more than 3 uGIMP nodes per axis
     (dict(constitutive=3), -8, b"constitutive"),
-    (dict(mvl=1), -8, b"MVL"),
     (dict(mc3d=5), -1, b"mc3d"),
 ])
 def test_create_rejects_bad_descriptors(pkg, L, over, code, msg):

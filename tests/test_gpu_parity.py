@@ -385,3 +385,39 @@ def test_graph_replay_matches_direct_launches(pkg, orc, gpu_lib, dim, monkeypatc
     o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc)
     o.run(case.dt, 0.0, 40)
     check_fields(outs[0], o, case.mp, TOL64)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_mvl(pkg, orc, gpu_lib, dim, prec, tol):
+    """Volumetric-locking mitigation (vollock1_OS! / vollock2_OS!,
+    utils_OS.jl:1162-1257): each particle's mean stress replaced by the
+    volume-weighted mean of its start-of-step cell, before the next P2G."""
+    mk = small2d if dim == 2 else small3d
+    case = mk(pkg, constitutive="druckerprager", gpu_precision=prec, MVL=True)
+    plain = mk(pkg, constitutive="druckerprager", gpu_precision=prec)
+    out, o = run_both(pkg, orc, case, 12)
+    check_fields(out, o, case.mp, tol, tol_stress(tol))
+    o2 = orc.Oracle(plain.args, plain.grid, plain.mp, plain.attr, plain.bc)
+    o2.run(plain.dt, 0.0, 12)
+    assert rel(o.sig, o2.sig) > 100 * tol_stress(tol)   # MVL changes the answer
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+@pytest.mark.parametrize("dim,va", [(2, "a"), (3, "a"), (2, "v"), (3, "v")])
+def test_usl(pkg, orc, gpu_lib, dim, va, prec, tol):
+    """USL (src/solvers/OS_USL.jl): no double mapping; DM1 and G2P share one
+    particle pass on the device."""
+    mk = small2d if dim == 2 else small3d
+    case = mk(pkg, constitutive="druckerprager", gpu_precision=prec, scheme="USL", va=va,
+              PIC=0.2 if va == "a" else 0.0, FLIP=0.8 if va == "a" else 1.0)
+    out, o = run_both(pkg, orc, case, 12)
+    check_fields(out, o, case.mp, tol, tol_stress(tol))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+def test_usl_mvl_graph_blocks(pkg, orc, gpu_lib, prec, tol):
+    """USL with MVL over 40 steps (replayed as captured graph blocks)."""
+    case = small3d(pkg, constitutive="druckerprager", gpu_precision=prec, scheme="USL", MVL=True)
+    out, o = run_both(pkg, orc, case, 40)
+    check_fields(out, o, case.mp, tol, tol_stress(tol))
