@@ -106,9 +106,20 @@ template <typename R> __device__ __forceinline__ void mark_block(const GDev<R> &
 // Flag the node blocks covered by the windows of the calling lanes.  The
 // active lanes of a warp (neighbouring particles after the cell sort) mark the
 // bounding box of their windows together; a box wider than 64 blocks (lanes
-// far apart) falls back to per-lane marking.
+// far apart) falls back to per-lane marking.  Marking is split in two: the
+// flag exchanges are issued before the scatter (mark_begin) and their results
+// are consumed after it (mark_end), so the atomics' round trip to L2 overlaps
+// the reductions instead of stalling the warp.
+struct MarkState {
+    int b[2];
+    unsigned old[2];
+    int n;
+};
+
 template <int D, typename R>
-__device__ __forceinline__ void mark_blocks(const GDev<R> &g, const AxisW<R> *w) {
+__device__ __forceinline__ MarkState mark_begin(const GDev<R> &g, const AxisW<R> *w) {
+    MarkState st;
+    st.n = 0;
     int lo[3], hi[3];
     block_range<D, R>(g, w, lo, hi);
     const unsigned mask = __activemask();
@@ -125,7 +136,14 @@ __device__ __forceinline__ void mark_blocks(const GDev<R> &g, const AxisW<R> *w)
         const int rank = __popc(mask & ((1u << lane) - 1u)), cnt = __popc(mask);
         for (int k = rank; k < total; k += cnt) {
             int by = blo[1] + k % ny, r = k / ny, bx = blo[0] + r % nx, bz = blo[2] + r / nx;
-            mark_block<R>(g, (bz * g.nbx + bx) * g.nby + by);
+            const int b = (bz * g.nbx + bx) * g.nby + by;
+            if (st.n < 2) {
+                st.b[st.n] = b;
+                st.old[st.n] = atomicExch(&g.bflag[b], 1u);
+                ++st.n;
+            } else {
+                mark_block<R>(g, b);
+            }
         }
     } else {
         for (int bz = lo[2]; bz <= hi[2]; ++bz)
@@ -134,6 +152,14 @@ __device__ __forceinline__ void mark_blocks(const GDev<R> &g, const AxisW<R> *w)
                     mark_block<R>(g, (bz * g.nbx + bx) * g.nby + by);
                 }
     }
+    return st;
+}
+
+// append the blocks this lane flagged first to the active-block list
+template <typename R> __device__ __forceinline__ void mark_end(const GDev<R> &g, const MarkState &st) {
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+        if (j < st.n && st.old[j] == 0u) g.blist[atomicAdd(g.bcount, 1u)] = (uint32_t)st.b[j];
 }
 
 // node of thread t in block b (returns -1 outside the grid)
@@ -246,7 +272,7 @@ __device__ __forceinline__ int window_node(const GDev<R> &g, const AxisW<R> *w, 
 template <int D, typename R>
 __device__ __forceinline__ void p2g_scatter(const GDev<R> &g, const AxisW<R> *w, R m, R vol,
                                             const R *v, const R *s, R G) {
-    mark_blocks<D, R>(g, w);
+    const MarkState mk = mark_begin<D, R>(g, w);
     const R p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : R(0)};
     const int n0 = window_n0<D, R>(g, w);
     const int plane = g.nnx * g.nny;
@@ -297,6 +323,7 @@ __device__ __forceinline__ void p2g_scatter(const GDev<R> &g, const AxisW<R> *w,
             }
         }
     }
+    mark_end<R>(g, mk);
 }
 
 template <int D, typename R>
