@@ -400,7 +400,7 @@ def test_mvl(pkg, orc, gpu_lib, dim, prec, tol):
     check_fields(out, o, case.mp, tol, tol_stress(tol))
     o2 = orc.Oracle(plain.args, plain.grid, plain.mp, plain.attr, plain.bc)
     o2.run(plain.dt, 0.0, 12)
-    assert rel(o.sig, o2.sig) > 100 * tol_stress(tol)   # MVL changes the answer
+    assert rel(o.sig, o2.sig) > 1e-2   # MVL changes the answer (by ~7e-2 here)
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
