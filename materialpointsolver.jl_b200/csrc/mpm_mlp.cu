@@ -54,6 +54,18 @@ __device__ __forceinline__ void st_bf16(uint8_t *base, uint32_t off, float v) {
     *reinterpret_cast<__nv_bfloat16 *>(base + off) = __float2bfloat16_rn(v);
 }
 
+// 8 consecutive K elements of one row = one 16-byte core-matrix row: one store
+__device__ __forceinline__ void st_bf16x8(uint8_t *base, uint32_t off, const float *v) {
+    uint4 q;
+    __nv_bfloat162 h0 = __floats2bfloat162_rn(v[0], v[1]), h1 = __floats2bfloat162_rn(v[2], v[3]),
+                   h2 = __floats2bfloat162_rn(v[4], v[5]), h3 = __floats2bfloat162_rn(v[6], v[7]);
+    q.x = *reinterpret_cast<uint32_t *>(&h0);
+    q.y = *reinterpret_cast<uint32_t *>(&h1);
+    q.z = *reinterpret_cast<uint32_t *>(&h2);
+    q.w = *reinterpret_cast<uint32_t *>(&h3);
+    *reinterpret_cast<uint4 *>(base + off) = q;
+}
+
 // W_l^T (n rows, k columns): B operand of the forward MMA
 __device__ void load_wT(uint8_t *dst, const float *P, int l) {
     const int K = lk(l), N = ln(l);
@@ -136,8 +148,10 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t trow, const float *bias
         for (int i = 0; i < 16; ++i) {
             const float zz = z[i] + bias[c + i];
             if (zkeep) zkeep[c + i] = zz;
-            st_bf16(a, kmajor_offset(t, c + i, 64), gelu(zz));
+            z[i] = gelu(zz);
         }
+        st_bf16x8(a, kmajor_offset(t, c, 64), z);
+        st_bf16x8(a, kmajor_offset(t, c + 8, 64), z + 8);
     }
 }
 
@@ -179,10 +193,12 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const float *__restrict__ 
 #pragma unroll
             for (int k = 0; k < 16; ++k) f[k] = S.norm[k];
         }
+        {
+            float xn[16];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const float xn = k < 15 ? (f[k] - S.norm[k]) / S.norm[16 + k] : 0.0f;
-            st_bf16(S.x, kmajor_offset(t, k, 16), xn);
+            for (int k = 0; k < 16; ++k) xn[k] = k < 15 ? (f[k] - S.norm[k]) / S.norm[16 + k] : 0.0f;
+            st_bf16x8(S.x, kmajor_offset(t, 0, 16), xn);
+            st_bf16x8(S.x, kmajor_offset(t, 8, 16), xn + 8);
         }
         fence_proxy_async();
         __syncthreads();
@@ -237,7 +253,9 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const float *__restrict__ 
 }  // namespace
 
 namespace mpm_detail {
-constexpr size_t MLP_FWD_SMEM = 60 * 1024;   // caps residency at 3 CTAs (192 of 512 TMEM columns) per SM
+// 42.5 KB used; 43 KB caps residency at 5 CTAs (320 of 512 TMEM columns) per SM
+constexpr size_t MLP_FWD_SMEM = 43 * 1024;
+constexpr int MLP_FWD_CTAS_PER_SM = 5;
 
 // Make the forward kernel launchable with its shared memory (call outside any
 // stream capture).
@@ -251,7 +269,7 @@ __attribute__((visibility("hidden"))) cudaError_t mlp_forward_dev(const float *P
                                                                  const uint32_t *n_dev, int residual, int *err,
                                                                  cudaStream_t st, int nsm) {
     const int64_t ntiles = (cap + TILE - 1) / TILE;
-    const int grid = (int)(ntiles < 3 * nsm ? ntiles : 3 * nsm);
+    const int grid = (int)(ntiles < MLP_FWD_CTAS_PER_SM * nsm ? ntiles : MLP_FWD_CTAS_PER_SM * nsm);
     if (grid < 1) return cudaSuccess;
     k_mlp_forward<<<grid, TILE, MLP_FWD_SMEM, st>>>(P, norm, feat, out, cap, n_dev, residual, err);
     return cudaGetLastError();
@@ -275,7 +293,8 @@ extern "C" int mpm_mlp_forward(const float *params, const float *norm, const flo
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         const int64_t ntiles = (n + TILE - 1) / TILE;
-        const int grid = (int)(ntiles < 3 * nsm ? ntiles : 3 * nsm);
+        const int grid = (int)(ntiles < mpm_detail::MLP_FWD_CTAS_PER_SM * nsm ? ntiles
+                                                                              : mpm_detail::MLP_FWD_CTAS_PER_SM * nsm);
         k_mlp_forward<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, out, n, nullptr, flags & 1, err);
         e = cudaGetLastError();
     }
@@ -302,7 +321,47 @@ namespace {
 // the sample sum is the MMA's K dimension; rows of dZ^T beyond N_l are not read
 // back (row m of D only depends on row m of A).
 // ---------------------------------------------------------------------------
-constexpr uint32_t COL_DY = 256, COL_DW = 384, TCOLS = 512;
+// TMEM columns: Z_0..Z_2 at 0/64/128, Z_3 at 192 (16), dY at 224 (64), and one
+// dW_l^T accumulator per layer that persists across the CTA's tiles (the
+// weight gradient leaves TMEM once per CTA, not once per tile).
+constexpr uint32_t COL_DY = 224, TCOLS = 512;
+__host__ __device__ constexpr uint32_t col_dw(int l) { return l == 3 ? 288u : l == 2 ? 352u : l == 1 ? 416u : 480u; }
+static_assert(col_dw(0) + 16 <= TCOLS, "TMEM budget");
+
+// Sum 16 per-lane values over the warp by recursive halving (16 shuffles):
+// returns the full sum of value index *idx; lanes with an odd id hold a copy.
+__device__ __forceinline__ float warp_sum16(const float *v, int *idx) {
+    const int lane = threadIdx.x & 31;
+    float a[8], b[4], c2[2];
+    const bool h4 = (lane >> 4) & 1, h3 = (lane >> 3) & 1, h2 = (lane >> 2) & 1, h1 = (lane >> 1) & 1;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float mine = h4 ? v[8 + i] : v[i], theirs = h4 ? v[i] : v[8 + i];
+        a[i] = mine + __shfl_xor_sync(0xffffffffu, theirs, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float mine = h3 ? a[4 + i] : a[i], theirs = h3 ? a[i] : a[4 + i];
+        b[i] = mine + __shfl_xor_sync(0xffffffffu, theirs, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const float mine = h2 ? b[2 + i] : b[i], theirs = h2 ? b[i] : b[2 + i];
+        c2[i] = mine + __shfl_xor_sync(0xffffffffu, theirs, 4);
+    }
+    const float mine = h1 ? c2[1] : c2[0], theirs = h1 ? c2[0] : c2[1];
+    float r = mine + __shfl_xor_sync(0xffffffffu, theirs, 2);
+    r += __shfl_xor_sync(0xffffffffu, r, 1);
+    *idx = (h4 ? 8 : 0) + (h3 ? 4 : 0) + (h2 ? 2 : 0) + (h1 ? 1 : 0);
+    return r;
+}
+
+// add 16 consecutive per-row values of the CTA's rows into sums[0..15] (smem)
+__device__ __forceinline__ void rows_sum16(const float *v, float *sums) {
+    int idx;
+    const float r = warp_sum16(v, &idx);
+    if ((threadIdx.x & 1) == 0 && r != 0.0f) atomicAdd(&sums[idx], r);
+}
 
 struct TSmem {
     uint8_t *w[NL];       // W_l (k rows x n), layers 1..3
@@ -313,10 +372,14 @@ struct TSmem {
     float *dbias;         // 4 x 64
 };
 
-__device__ __forceinline__ void issue_gemm(uint32_t tmem_d, uint32_t a_saddr, uint32_t b_saddr, int K, int N) {
+// D (+)= A * B^T over K; `accumulate` decides whether the first K step adds
+// to D (later steps always do)
+__device__ __forceinline__ void issue_gemm(uint32_t tmem_d, uint32_t a_saddr, uint32_t b_saddr, int K, int N,
+                                           bool accumulate = false) {
     const uint32_t idesc = idesc_bf16_f32(TILE, N);
     for (int j = 0; j < K / 16; ++j)
-        mma_bf16(tmem_d, kstep_desc(a_saddr, j, K), kstep_desc(b_saddr, j, K), idesc, j > 0 ? 1u : 0u);
+        mma_bf16(tmem_d, kstep_desc(a_saddr, j, K), kstep_desc(b_saddr, j, K), idesc,
+                 (j > 0 || accumulate) ? 1u : 0u);
 }
 
 __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ P, const float *__restrict__ norm,
@@ -361,11 +424,15 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ 
         float f[16];
 #pragma unroll
         for (int k = 0; k < 16; ++k) f[k] = valid ? feat[row * 16 + k] : S.norm[k];
+        {
+            float xn[16];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const float xn = k < 15 ? (f[k] - S.norm[k]) / S.norm[16 + k] : 0.0f;
-            st_bf16(S.x, kmajor_offset(t, k, 16), xn);
-            st_bf16(T.xT, kmajor_offset(k, t, TILE), xn);
+            for (int k = 0; k < 16; ++k) {
+                xn[k] = k < 15 ? (f[k] - S.norm[k]) / S.norm[16 + k] : 0.0f;
+                st_bf16(T.xT, kmajor_offset(k, t, TILE), xn[k]);
+            }
+            st_bf16x8(S.x, kmajor_offset(t, 0, 16), xn);
+            st_bf16x8(S.x, kmajor_offset(t, 8, 16), xn + 8);
         }
         fence_proxy_async();
         __syncthreads();
@@ -383,10 +450,11 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ 
                 tmem_ld16(trow + 64u * l + c, z);
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
-                    const float y = gelu(z[i] + S.bias[64 * l + c + i]);
-                    st_bf16(S.a, kmajor_offset(t, c + i, 64), y);
-                    st_bf16(T.yT[l], kmajor_offset(c + i, t, TILE), y);
+                    z[i] = gelu(z[i] + S.bias[64 * l + c + i]);
+                    st_bf16(T.yT[l], kmajor_offset(c + i, t, TILE), z[i]);
                 }
+                st_bf16x8(S.a, kmajor_offset(t, c, 64), z);
+                st_bf16x8(S.a, kmajor_offset(t, c + 8, 64), z + 8);
             }
             fence_before_sync();
             fence_proxy_async();
@@ -415,8 +483,9 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ 
                 }
                 st_bf16(T.dz, kmajor_offset(t, o, 16), d);
                 st_bf16(T.dzT, kmajor_offset(o, t, TILE), d);
-                if (d != 0.0f) atomicAdd(&T.dbias[192 + o], d);
+                z[o] = d;
             }
+            rows_sum16(z, T.dbias + 192);
         }
         // ---- backward through layers 3, 2, 1 (dW_l and dY_{l-1}), then dW_0
         for (int l = 3; l >= 0 && ok; --l) {
@@ -425,22 +494,13 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ 
             __syncthreads();
             if (t == 0) {
                 fence_after_sync();
-                issue_gemm(tmem + COL_DW, smem_u32(T.dzT), smem_u32(l == 0 ? T.xT : T.yT[l - 1]), TILE, lk(l));
+                issue_gemm(tmem + col_dw(l), smem_u32(T.dzT), smem_u32(l == 0 ? T.xT : T.yT[l - 1]), TILE, lk(l),
+                           tile != (int64_t)blockIdx.x);
                 if (l > 0) issue_gemm(tmem + COL_DY, smem_u32(T.dz), smem_u32(T.w[l]), ln(l), lk(l));
                 commit(bar);
             }
             ok = layer_done(bar, parity, err);
             if (!ok) break;
-            // dW_l^T: lane = output unit n, columns = inputs k
-            const int N = ln(l), K = lk(l);
-            for (int c = 0; c < K; c += 16) {
-                float g[16];
-                tmem_ld16(trow + COL_DW + c, g);
-                if (t < N) {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) atomicAdd(&grad[ow(l) + (c + i) * N + t], g[i]);
-                }
-            }
             if (l == 0) break;
             // dZ_{l-1} = dY_{l-1} .* GELU'(Z_{l-1} + b_{l-1})
             const int lp = l - 1;
@@ -454,15 +514,32 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ 
                     const float d = valid ? dy[i] * gelu_grad(z[i] + S.bias[64 * lp + c + i]) : 0.0f;
                     st_bf16(T.dz, kmajor_offset(t, c + i, 64), d);
                     st_bf16(T.dzT, kmajor_offset(c + i, t, TILE), d);
-                    if (d != 0.0f) atomicAdd(&T.dbias[64 * lp + c + i], d);
+                    dy[i] = d;
                 }
+                rows_sum16(dy, T.dbias + 64 * lp + c);
             }
         }
         fence_before_sync();
         __syncthreads();
     }
-    // bias gradients and loss
+    // weight gradients (dW_l^T accumulated over the CTA's tiles: lane = output
+    // unit n, columns = inputs k), bias gradients and loss, once per CTA
     __syncthreads();
+    fence_after_sync();
+    if (ok && (int64_t)blockIdx.x < ntiles) {
+        for (int l = 0; l < NL; ++l) {
+            const int N = ln(l), K = lk(l);
+            for (int c = 0; c < K; c += 16) {
+                float g[16];
+                tmem_ld16(trow + col_dw(l) + c, g);
+                if (t < N) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        if (g[i] != 0.0f) atomicAdd(&grad[ow(l) + (c + i) * N + t], g[i]);
+                }
+            }
+        }
+    }
     for (int i = threadIdx.x; i < 4 * 64; i += blockDim.x) {
         const int l = i / 64, nn = i % 64;
         if (nn < ln(l) && T.dbias[i] != 0.0f) atomicAdd(&grad[ob(l) + nn], T.dbias[i]);
