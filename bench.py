@@ -41,10 +41,11 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mc3d", default="literal", choices=["literal", "restated"])
-    ap.add_argument("--workload", default="column3d", choices=["column3d", "slope3d", "batch2d"],
+    ap.add_argument("--workload", default="column3d", choices=["column3d", "slope3d", "batch2d", "column2d"],
                     help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
                          "3D slope with a lognormal cohesion field; batch2d: 256 independent 2D slopes "
-                         "(15.5 M particles) advanced together, autotuned during warm-up")
+                         "(15.5 M particles) advanced together, autotuned during warm-up; column2d: the 3 200-"
+                         "particle 2D column in FP64 (launch-bound; CUDA graph replay)")
     ap.add_argument("--surrogate", action="store_true",
                     help="slope3d: train the stress-return surrogate on samples logged from plain steps "
                          "(untimed) and time steps with it")
@@ -133,6 +134,8 @@ WORKLOADS = {
                 "constitutive": "druckerprager"},
     "batch2d": {"workload": "256 independent 2D slopes in one grid, uGIMP, MUSL va=:a",
                 "constitutive": "druckerprager"},
+    "column2d": {"workload": "2D granular column collapse (3 200 particles), uGIMP, MUSL va=:a, all FP64",
+                 "constitutive": "druckerprager"},
 }
 
 
@@ -145,6 +148,8 @@ def make_case(mc3d, workload="column3d", surrogate=False):
         case = pkg.workloads.slope_3d(Te=0.0) if surrogate else pkg.workloads.slope_3d()
     elif workload == "batch2d":
         case = pkg.workloads.slope_batch_2d()
+    elif workload == "column2d":
+        case = pkg.workloads.column_collapse_2d(gpu_precision="fp64")
     else:
         case = pkg.workloads.column_collapse_3d(mc3d=mc3d)
     return pkg, case
@@ -303,11 +308,13 @@ def run_b200(args):
     result = {
         "metric": "particle-updates/s", "value": value, "unit": "particle-updates/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": t_max / K,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.workload == "column2d" else "f32",
         "data": f"synthetic (seeded lattice + jitter, seed {case.meta['seed']})",
         "config": dict(WORKLOADS[args.workload],
                        particles=npart, nodes=case.grid.ni, active_nodes=na, h=case.meta["h"],
-                       mc3d=args.mc3d, precision="FP32 bulk, FP64 positions and det(F)", sort_every=sort_used,
+                       mc3d=args.mc3d, precision=("all FP64" if args.workload == "column2d"
+                                                   else "FP32 bulk, FP64 positions and det(F)"), sort_every=sort_used,
                        particle_passes="tiled" if tiled_used else "per-particle",
                        l2=f"particle state {npart * bp_step / 1e9:.2f} GB > 126 MB L2 (no flush needed)",
                        parallelism=f"replicas x{world}",
@@ -325,7 +332,8 @@ def run_b200(args):
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(args.mc3d)
+        if args.workload in ("column3d", "column2d"):
+            result["cpu_baseline"] = cpu_baseline(args.mc3d, args.workload)
     if use_dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -337,19 +345,22 @@ def oracle_threads():
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
 
 
-def cpu_baseline(mc3d, steps=4):
+def cpu_baseline(mc3d, workload="column3d", steps=None):
     """The FP64 CPU restatement of the reference path (OpenMP, all host cores)
-    on the same 2.56 M-particle column: 1 warm-up step + `steps` timed steps."""
+    on the same workload: 1 warm-up step + a bounded number of timed steps
+    (about 10 s of CPU work)."""
     from oracle import oracle as orc
-    pkg, case = make_case(mc3d)
+    pkg, case = make_case(mc3d, workload)
     nth = oracle_threads()
+    if steps is None:
+        steps = max(2, min(4000, int(3e7 / case.mp.np)))
     o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc, nthreads=nth)
     o.run(case.dt, 0.0, 1)
     t0 = time.perf_counter()
     o.run(case.dt, case.dt, steps)
     t = time.perf_counter() - t0
     return {"value": case.mp.np * steps / t, "unit": "particle-updates/s", "cores": nth,
-            "kind": "port", "sample": f"{steps} steps of the full {case.mp.np}-particle column after 1 warm-up step"}
+            "kind": "port", "sample": f"{steps} steps of the full {case.mp.np}-particle {workload} after 1 warm-up step"}
 
 
 def run_reference(args):
