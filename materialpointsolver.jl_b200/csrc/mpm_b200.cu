@@ -74,6 +74,8 @@ struct mpm_handle {
     bool uploaded = false;
     bool coh_mode = false;   // per-particle cohesion (materials differ only in c)
     bool use_graphs = true;  // replay captured step blocks (MPM_B200_GRAPHS=0 turns it off)
+    bool prefetch = true;    // FP32 particle pass stages fields by cp.async (MPM_B200_PREFETCH=0 turns it off)
+    bool cell_major = false; // order inside a tile: rank-major (default) or cell-major (MPM_B200_ORDER=cell)
     GraphCache graph;
     int64_t graph_launches = 0;
     // stress-return surrogate: 1 = log samples into caller buffers, 2 = infer
@@ -384,8 +386,14 @@ template <int D, typename R> void do_sort(mpm_handle *h) {
     k_sort_big<<<64, 512, 0, st>>>(h->off, h->big, h->nbig, h->big_cap, h->pairs);
     CK(cudaMemsetAsync(h->ntiles, 0, 4, st));
     k_tile_list<<<cdiv(h->ntile_total, 256), 256, 0, st>>>(h->off, h->ntile_total, Tile<D>::CPT, h->tiles, h->ntiles);
-    k_tile_transpose<Tile<D>::CPT><<<h->nsm * 8, Tile<D>::CPT, 0, st>>>(h->off, h->tiles, h->ntiles, h->pairs, h->pairs2);
-    k_permute<D, R><<<cdiv(np, 256), 256, 0, st>>>(A, B, h->pairs2, np);
+    if (h->cell_major) {
+        // particles of a cell stay consecutive (tile-major, then cell, then original index)
+        k_permute<D, R><<<cdiv(np, 256), 256, 0, st>>>(A, B, h->pairs, np);
+    } else {
+        k_tile_transpose<Tile<D>::CPT><<<h->nsm * 8, Tile<D>::CPT, 0, st>>>(h->off, h->tiles, h->ntiles, h->pairs,
+                                                                             h->pairs2);
+        k_permute<D, R><<<cdiv(np, 256), 256, 0, st>>>(A, B, h->pairs2, np);
+    }
     LAUNCH_CHECK();
     std::swap(h->pbuf[0], h->pbuf[1]);
     h->since_sort = 0;
@@ -430,6 +438,9 @@ double gravity_at(const mpm_desc &d, double Ti) {
     return Ti < d.Te ? d.gravity / d.Te * Ti : d.gravity;
 }
 
+// dynamic shared memory of the particle pass (staged particle fields)
+inline size_t g2p_smem(const StepParams &sp) { return sp.prefetch ? (size_t)PF_N * PF_T * sizeof(float) : 0; }
+
 template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, double Ti, double Gscatter) {
     StepParams sp{};
     sp.dt = dt;
@@ -442,6 +453,7 @@ template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, do
     sp.mc3d = h->d.mc3d == MPM_MC3D_RESTATED ? 1 : 0;
     sp.va = h->d.va;
     sp.usl = h->d.scheme == MPM_SCHEME_USL ? 1 : 0;
+    sp.prefetch = (sizeof(R) == 4 && h->prefetch) ? 1 : 0;
     // grid vs is gathered by the :v updates and by the PIC term of MUSL :a (USL :a
     // maps the updated velocity, which is the vsT record)
     sp.need_vs = (h->d.va == MPM_VA_V || (h->d.PIC != 0.0 && !sp.usl)) ? 1 : 0;
@@ -521,14 +533,14 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
             CK(cudaMemsetAsync(h->csigm, 0, (size_t)h->nc * sizeof(R), h->stream));
             CK(cudaMemsetAsync(h->comega, 0, (size_t)h->nc * sizeof(R), h->stream));
             L.run("g2p", [&] {
-                if (mc3) k_g2p<D, R, false, D == 3, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                else k_g2p<D, R, false, false, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                if (mc3) k_g2p<D, R, false, D == 3, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+                else k_g2p<D, R, false, false, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
             });
             L.run("mvl_p2g", [&] { k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
         } else {
             L.run("g2p_p2g", [&] {
-                if (mc3) k_g2p<D, R, true, D == 3, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                else k_g2p<D, R, true, false, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                if (mc3) k_g2p<D, R, true, D == 3, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+                else k_g2p<D, R, true, false, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
             });
         }
     } else if (sp.mvl && np) {
@@ -539,8 +551,8 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         CK(cudaMemsetAsync(h->csigm, 0, (size_t)h->nc * sizeof(R), h->stream));
         CK(cudaMemsetAsync(h->comega, 0, (size_t)h->nc * sizeof(R), h->stream));
         L.run("g2p", [&] {
-            if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-            else k_g2p<D, R, false><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+            else k_g2p<D, R, false><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
         });
         L.run("mvl_p2g", [&] { k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
     } else if (sp.surr.mode == 2 && sp.plastic && np) {
@@ -550,7 +562,7 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         CK(cudaMemsetAsync(h->surr_cnt, 0, 4, h->stream));
-        L.run("g2p", [&] { k_g2p<D, R, false><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("g2p", [&] { k_g2p<D, R, false><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp); });
         L.run("mlp", [&] {
             CK(mpm_detail::mlp_forward_dev(h->surr_params, h->surr_norm, h->surr_feat, h->surr_out, np, h->surr_cnt,
                                            h->surr_residual, h->surr_err, h->stream, h->nsm));
@@ -567,8 +579,8 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         if (np) L.run("g2p_p2g", [&] {
-            if (mc3) k_g2p<D, R, true, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-            else k_g2p<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (mc3) k_g2p<D, R, true, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+            else k_g2p<D, R, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
         });
     }
     h->since_sort++;
@@ -914,8 +926,8 @@ template <int D, typename R> struct Stages {
         }
         const bool mc3 = sp.mc3d && sp.constitutive == MPM_MOHRCOULOMB;
         if ((mask & 16u) && np) L.run("g2p", [&] {
-            if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-            else k_g2p<D, R, false><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+            else k_g2p<D, R, false><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
         });
         h->acc_valid = false;
     }
@@ -1091,6 +1103,8 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         // MPM_B200_GRAPHS=0 issues every step's launches directly instead of
         // replaying captured blocks of steps.
         if (const char *e = getenv("MPM_B200_GRAPHS")) h->use_graphs = (e[0] != '0');
+        if (const char *e = getenv("MPM_B200_PREFETCH")) h->prefetch = (e[0] != '0');
+        if (const char *e = getenv("MPM_B200_ORDER")) h->cell_major = (std::string(e) == "cell");
         *out = h;
         return MPM_OK;
     } catch (const Err &e) {

@@ -29,6 +29,11 @@
 #ifndef MPM_P_MINB
 #define MPM_P_MINB 4
 #endif
+// the double-mapping pass holds less state per particle: 6 CTAs (42 registers)
+// measured faster than 4 for it, slower for the G2P pass
+#ifndef MPM_DMAP_MINB
+#define MPM_DMAP_MINB 6
+#endif
 
 namespace mpm {
 
@@ -203,6 +208,7 @@ struct StepParams {
     int mc3d;        // 3D Mohr-Coulomb: 0 elastic predictor only (literal), 1 restated return
     int mvl;         // volumetric-locking mitigation (cell-averaged mean stress)
     int usl;         // USL scheme (OS_USL.jl): no double mapping, Δu = vsT·dt
+    int prefetch;    // FP32 particle pass: fields staged in dynamic shared memory (PF_N x 256 floats)
     SurrCtx surr;
     int64_t np;
 };
@@ -434,7 +440,7 @@ __global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
 // carried out by k_g2p, which gathers the same ΣN·vsT with the same weights.
 // ---------------------------------------------------------------------------
 template <int D, typename R>
-__global__ void __launch_bounds__(256, MPM_P_MINB) k_dmap(PDev<D, R> P, GDev<R> g, StepParams sp) {
+__global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<R> g, StepParams sp) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= sp.np) return;
     using T4 = typename Vec<R>::T4;
@@ -560,6 +566,46 @@ __global__ void __launch_bounds__(128) k_dm3(GDev<R> g, StepParams sp) {
 
 // Does the Drucker-Prager return change this trial stress (the shear or
 // tension branch of dpP!, druckerprager.jl:89-155)?
+// Particle fields staged in shared memory (slot-major, 256 threads per slot)
+// by 4-byte cp.async at the start of the FP32 particle pass, so that their
+// DRAM latency overlaps the node gathers instead of following them.
+constexpr int PF_SIG = 0, PF_F = 6, PF_EPS = 15, PF_EPSQ = 21, PF_EPSK = 22, PF_VOL0 = 23, PF_M = 24,
+              PF_V = 25, PF_MAT = 28, PF_COH = 29, PF_N = 30, PF_T = 256;
+
+template <typename R> __device__ __forceinline__ R pf(const float *pre, int slot, const R *g) {
+    return pre ? (R)pre[slot * PF_T] : ldcs(g);
+}
+__device__ __forceinline__ uint32_t pfu(const float *pre, int slot, const uint32_t *g) {
+    return pre ? __float_as_uint(pre[slot * PF_T]) : ldcs(g);
+}
+__device__ __forceinline__ void cp_async4(float *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
+// issue the copies of particle i's fields into this thread's slots
+template <int D, typename R>
+__device__ __forceinline__ void prefetch_particle(float *pre, const PDev<D, R> &P, int64_t i) {
+    constexpr int NV = PDev<D, R>::NV, NF = PDev<D, R>::NF;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) cp_async4(pre + (PF_SIG + k) * PF_T, P.sig[k] + i);
+#pragma unroll
+    for (int k = 0; k < NF; ++k) cp_async4(pre + (PF_F + k) * PF_T, P.F[k] + i);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) cp_async4(pre + (PF_EPS + k) * PF_T, P.eps[k] + i);
+    cp_async4(pre + PF_EPSQ * PF_T, P.epsq + i);
+    cp_async4(pre + PF_EPSK * PF_T, P.epsk + i);
+    cp_async4(pre + PF_VOL0 * PF_T, P.vol0 + i);
+    cp_async4(pre + PF_M * PF_T, P.m + i);
+#pragma unroll
+    for (int d = 0; d < D; ++d) cp_async4(pre + (PF_V + d) * PF_T, P.v[d] + i);
+    cp_async4(pre + PF_MAT * PF_T, P.mat + i);
+    if (P.coh) cp_async4(pre + PF_COH * PF_T, P.coh + i);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void prefetch_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // 0: elastic, 1: shear branch, 2: tension branch (3D)
 template <typename R> __device__ __forceinline__ int dp_branch(const R *s, const Mat<R> &M) {
     const R sm = (s[0] + s[1] + s[2]) * R(0.333333);
@@ -604,7 +650,8 @@ __device__ __forceinline__ void surr_features(const SurrCtx &c, int64_t i, const
 // the particle and returns the new stress s and volume vol for the next P2G.
 template <int D, typename R, bool MC3 = false>
 __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp,
-                                                int64_t i, double *x, const R *tT, const R *dF, R *s, R &vol) {
+                                                int64_t i, double *x, const R *tT, const R *dF, R *s, R &vol,
+                                                const float *pre = nullptr) {
     constexpr int NV = PDev<D, R>::NV, NF = PDev<D, R>::NF;
     // position: ξ += ΔT·ΣN·vsT, accumulated in FP64
 #pragma unroll
@@ -625,18 +672,18 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
     }
     // strain
     if (D == 2) {
-        stcs(P.eps[0] + i, ldcs(P.eps[0] + i) + de[0]);
-        stcs(P.eps[1] + i, ldcs(P.eps[1] + i) + de[1]);
-        stcs(P.eps[3] + i, ldcs(P.eps[3] + i) + de[3]);
+        stcs(P.eps[0] + i, pf(pre, PF_EPS + 0, P.eps[0] + i) + de[0]);
+        stcs(P.eps[1] + i, pf(pre, PF_EPS + 1, P.eps[1] + i) + de[1]);
+        stcs(P.eps[3] + i, pf(pre, PF_EPS + 3, P.eps[3] + i) + de[3]);
     } else {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) stcs(P.eps[k] + i, ldcs(P.eps[k] + i) + de[k]);
+        for (int k = 0; k < 6; ++k) stcs(P.eps[k] + i, pf(pre, PF_EPS + k, P.eps[k] + i) + de[k]);
     }
     stcs(P.epsv + i, ev);
     // F <- (I + ΔF) F; J = det F in FP64; Ω = J Ω0
     R f[9], fn[9];
 #pragma unroll
-    for (int k = 0; k < NF; ++k) f[k] = ldcs(P.F[k] + i);
+    for (int k = 0; k < NF; ++k) f[k] = pf(pre, PF_F + k, P.F[k] + i);
     double J;
     if (D == 2) {
         fn[0] = (dF[0] + R(1)) * f[0] + dF[1] * f[2];
@@ -660,14 +707,14 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
     }
 #pragma unroll
     for (int k = 0; k < NF; ++k) stcs(P.F[k] + i, fn[k]);
-    vol = (R)(J * (double)ldcs(P.vol0 + i));
+    vol = (R)(J * (double)pf(pre, PF_VOL0, P.vol0 + i));
     stcs(P.vol + i, vol);
     // stress: liE! then dpP! / mcP! (OS_MUSL.jl:82-96)
-    Mat<R> M = g.mat[ldcs(P.mat + i)];
+    Mat<R> M = g.mat[pfu(pre, PF_MAT, P.mat + i)];
     if (P.coh) {
         // one material per particle differing only in cohesion (a random
         // field): the cohesion-dependent constants of druckerprager.jl:39-44
-        const R c = ldcs(P.coh + i);
+        const R c = pf(pre, PF_COH, P.coh + i);
         M.c = c;
         M.kphi = c * M.kc;
         M.st = fmin(M.sigt, M.kphi / M.qphi);
@@ -675,10 +722,10 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
     }
     R srot[6];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) s[k] = ldcs(P.sig[k] + i);
+    for (int k = 0; k < NV; ++k) s[k] = pf(pre, PF_SIG + k, P.sig[k] + i);
     lin_elastic<D, R>(s, dF, de, M, srot);
     if (sp.plastic && (sp.constitutive == 1 || (sp.constitutive == 2 && D == 2))) {
-        R eq = ldcs(P.epsq + i), ek = ldcs(P.epsk + i);
+        R eq = pf(pre, PF_EPSQ, P.epsq + i), ek = pf(pre, PF_EPSK, P.epsk + i);
         if (D == 3 && sp.constitutive == 1 && sp.surr.mode == 2) {
             if (dp_yielding<R>(s, M)) surr_features<R>(sp.surr, i, s, de, eq, M, nullptr);
         } else if (D == 3 && sp.constitutive == 1 && sp.surr.mode == 1) {
@@ -706,7 +753,7 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
         if (r.yielded) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) s[k] = (R)sd[k];
-            stcs(P.epsq + i, (R)((double)ldcs(P.epsq + i) + r.dq));
+            stcs(P.epsq + i, (R)((double)pf(pre, PF_EPSQ, P.epsq + i) + r.dq));
         }
     }
 #pragma unroll
@@ -728,6 +775,12 @@ template <int D, typename R, bool FUSE, bool MC3 = false, bool USL = false>
 __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g, StepParams sp) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= sp.np) return;
+    extern __shared__ float g2p_pre[];   // PF_N slots x 256 threads when sp.prefetch
+    float *pre = nullptr;
+    if (sizeof(R) == 4 && sp.prefetch) {
+        pre = g2p_pre + threadIdx.x;
+        prefetch_particle<D, R>(pre, P, i);
+    }
     double x[3];
     load_x<D, R>(P, i, x);
     AxisW<R> w[3];
@@ -805,10 +858,12 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
         // doublemapping1_a_USL_OS! / doublemapping1_OS! (OS_USL.jl:185-320)
         const R FLIP = (R)sp.FLIP, PIC = (R)sp.PIC;
 #pragma unroll
+        if (pre) prefetch_wait();
         for (int d = 0; d < D; ++d) {
-            const R vo = ldcs(P.v[d] + i);
+            const R vo = pf(pre, PF_V + d, P.v[d] + i);
             const R vn = sp.va == 0 ? FLIP * vo + PIC * tT[d] + ta[d] * dt : FLIP * (vo + (tT[d] - tv[d])) + PIC * tT[d];
             stcs(P.v[d] + i, vn);
+            if (pre) pre[(PF_V + d) * PF_T] = (float)vn;
         }
     }
     R s[6], vol;
@@ -821,7 +876,8 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
         const int cz = D == 3 ? clampi(ci[2], 0, g.ax[2].nc - 1) : 0;
         cell = (cz * g.ax[0].nc + cx) * g.ax[1].nc + cy;
     }
-    update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol);
+    if (pre) prefetch_wait();
+    update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol, pre);
     if (!FUSE && sp.mvl) {
         const R sm = (s[0] + s[1] + s[2]) * R(0.333333);
         atomicAdd(&g.csigm[cell], vol * sm);
@@ -832,9 +888,9 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
         if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
         R v[3];
 #pragma unroll
-        for (int d = 0; d < D; ++d) v[d] = ldcs(P.v[d] + i);
+        for (int d = 0; d < D; ++d) v[d] = pf(pre, PF_V + d, P.v[d] + i);
         if (D == 2) v[2] = R(0);
-        p2g_scatter<D, R>(g, w, ldcs(P.m + i), vol, v, s, (R)sp.G);
+        p2g_scatter<D, R>(g, w, pf(pre, PF_M, P.m + i), vol, v, s, (R)sp.G);
     }
 }
 

@@ -272,7 +272,6 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p_tile(PDev<D, R> P, GDev
     R *s_vT = (R *)smem_raw;          // 3 x WN
     R *s_du = s_vT + 3 * W::WN;       // 3 x WN
     const uint32_t nt = *tl.ntiles;
-    constexpr int NC = D == 3 ? 3 : 1;
     const int plane = g.nnx * g.nny;
     for (uint32_t q = blockIdx.x; q < nt; q += gridDim.x) {
         const uint32_t t = tl.tiles[q];
