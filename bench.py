@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--surrogate", action="store_true",
                     help="slope3d: train the stress-return surrogate on samples logged from plain steps "
                          "(untimed) and time steps with it")
+    ap.add_argument("--snapshot-every", type=int, default=0,
+                    help="also time K steps with an HDF5 snapshot group every N steps (submit_work!'s "
+                         "hdf5 branch) against the same chunks without snapshots")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W warm-up + K device steps (the command profilers wrap)")
     return ap.parse_args()
@@ -331,6 +334,8 @@ def run_b200(args):
                 "what": "DeviceModel upload from pinned host arrays + K steps + device2host! field set"},
         "clocks": clk.summary(),
     }
+    if args.snapshot_every > 0:
+        result["snapshots"] = snapshot_cost(pkg, case, dt, K, args.snapshot_every, local)
     if rank == 0 and not args.no_cpu_baseline:
         if args.workload in ("column3d", "column2d"):
             result["cpu_baseline"] = cpu_baseline(args.mc3d, args.workload)
@@ -339,6 +344,44 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result))
+
+
+def snapshot_cost(pkg, case, dt, K, every, local):
+    """Wall time of K steps in chunks of `every`, with and without a snapshot
+    group (all nine fields, the model's float type) before each chunk; the
+    snapshot's gather, copy and file write overlap the next chunk."""
+    import shutil
+    import tempfile
+    T = np.float32 if case.args.precision == "FP32" else np.float64
+    tmp = tempfile.mkdtemp(prefix="mpm_snap_")
+    out = {"every": every, "steps": K}
+    try:
+        for mode in ("plain", "snapshots"):
+            dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
+            f = pkg.hdf5.H5File(os.path.join(tmp, "s.h5")) if mode == "snapshots" else None
+            dev.step(dt, 0.0, 3)
+            Ti, done, groups = 0.0, 0, 0
+            t0 = time.perf_counter()
+            while done < K:
+                if f is not None:
+                    groups += 1
+                    dev.snapshot(f, groups, Ti, dtype=T)
+                n = min(every, K - done)
+                Ti = dev.step(dt, Ti, n)
+                done += n
+            if f is not None:
+                dev.snapshot_wait()
+                f.close()
+            out[f"{mode}_ms_per_step"] = (time.perf_counter() - t0) * 1e3 / K
+            dev.close()
+            if f is not None:
+                size = os.path.getsize(os.path.join(tmp, "s.h5"))
+                out.update(groups=groups, file_bytes=size, bytes_per_group=size / groups)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    extra = out["snapshots_ms_per_step"] - out["plain_ms_per_step"]
+    out["overhead_ms_per_group"] = extra * K / out["groups"]
+    return out
 
 
 def oracle_threads():

@@ -12,6 +12,7 @@
  *   mpm_destroy               clean_device! ext/CUDAExt/devicehelpfunc_cuda.jl:71-100
  *   mpm_compute_p2c           the p2c part of resetmpstatus_OS!, src/solvers/utils_OS.jl:203-205,325-328
  *   mpm_peak_bandwidth        Tpeak,        ext/CUDAExt/devicehelpfunc_cuda.jl:102-136
+ *   mpm_snapshot, mpm_h5_*    the HDF5 snapshots of submit_work!, src/solver.jl:54-111
  *
  * Host arrays are passed as views of the caller's arrays in the reference's
  * layout: Julia column-major `n x k` matrices (component k of item i at
@@ -287,6 +288,36 @@ int mpm_set_surrogate(mpm_handle *h, const float *params, const float *norm, int
  * stress to target (DEVICE arrays of cap rows); *count (device) counts rows
  * offered, rows beyond cap are dropped.  every = 0 stops logging. */
 int mpm_log_samples(mpm_handle *h, float *feat, float *target, uint32_t *count, uint32_t cap, uint32_t every);
+
+/* ---- snapshots (the HDF5 output of submit_work!, src/solver.jl:54-111) ----
+ * mpm_h5 is an HDF5 file written by the library itself (no libhdf5): groups of
+ * contiguous datasets, readable by HDF5.jl / h5py.  mpm_h5_write stores one
+ * dataset `name` ("group3/stress"; missing groups are created) of `rank`
+ * dimensions given slowest-varying first: HDF5.jl writes a Julia np x k
+ * matrix as dims {k, np}, so its column-major buffer is passed that way; rank
+ * 0 is a scalar.  The file becomes readable when mpm_h5_close returns.  Calls
+ * on one file are serialised internally.  Errors: mpm_last_error(NULL).
+ *
+ * mpm_snapshot enqueues one group of submit_work! (src/solver.jl:60-70):
+ * "group<group>/" + stress, strain_s, eqstrain, ekstrain, eqrate, coords,
+ * velocity_s, volume, mass_s (the fields of field_mask, a subset of
+ * MPM_F_SNAPSHOT) in the original particle order, and "time" = Ti, all of
+ * element type `type` (MPM_T_F64 or MPM_T_F32).  It returns at once: the
+ * fields are gathered on the handle's stream behind the steps issued so far,
+ * copied to pinned host memory on a second stream while later steps run, and
+ * written by a writer thread.  Two snapshots can be in flight; a third call
+ * waits for the older one.  mpm_snapshot_wait returns when every enqueued
+ * snapshot is in the file (written = groups written so far) and reports a
+ * writer error once; call it before mpm_h5_close. */
+typedef struct mpm_h5 mpm_h5;
+int mpm_h5_create(const char *path, mpm_h5 **out);
+int mpm_h5_write(mpm_h5 *f, const char *name, int32_t type, int32_t rank, const int64_t *dims,
+                 const void *data);
+int mpm_h5_close(mpm_h5 *f);
+#define MPM_F_SNAPSHOT (MPM_F_SIG | MPM_F_EPS | MPM_F_EPSQ | MPM_F_EPSK | MPM_F_EPSV | MPM_F_XI | \
+                        MPM_F_VS | MPM_F_OMEGA | MPM_F_MS)
+int mpm_snapshot(mpm_handle *h, mpm_h5 *f, int64_t group, double Ti, uint32_t field_mask, int32_t type);
+int mpm_snapshot_wait(mpm_handle *h, int64_t *written);
 
 /* ---- diagnostics ---- */
 /* sizeof(mpm_desc), sizeof(mpm_view), sizeof(mpm_host_views), sizeof(mpm_stats):

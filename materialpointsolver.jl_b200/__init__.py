@@ -11,8 +11,9 @@ from . import workloads
 from . import randomfield
 from . import surrogate
 from . import precision
+from . import hdf5
 from . import _lib
 from .solver import (DeviceModel, host2device, device2host, clean_device, procedure,
-                     materialpointsolver, time_sequence)
+                     materialpointsolver, time_sequence, snapshot_path)
 
 build = _lib.build

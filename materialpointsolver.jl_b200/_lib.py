@@ -30,6 +30,7 @@ T_F64, T_F32, T_I64, T_I32 = 0, 1, 2, 3
 F_XI, F_VS, F_SIG, F_EPS, F_EPSQ, F_EPSK, F_EPSV = (1 << i for i in range(7))
 F_OMEGA, F_MS, F_SIGM, F_F, F_RHO, F_P2C = (1 << i for i in range(7, 13))
 F_REFERENCE = F_SIGM | F_VS | F_XI | F_OMEGA | F_SIG | F_EPSK | F_EPSQ | F_EPSV | F_EPS | F_MS
+F_SNAPSHOT = F_SIG | F_EPS | F_EPSQ | F_EPSK | F_EPSV | F_XI | F_VS | F_OMEGA | F_MS
 
 EXPORTS = [
     "mpm_create", "mpm_upload", "mpm_destroy", "mpm_step", "mpm_step_async", "mpm_sync",
@@ -38,6 +39,7 @@ EXPORTS = [
     "mpm_set_profiling", "mpm_get_kernel_times", "mpm_abi_sizes", "mpm_cell_order_noalloc",
     "mpm_grf_eval", "mpm_set_tuning", "mpm_get_tuning", "mpm_autotune",
     "mpm_mlp_nparams", "mpm_mlp_forward", "mpm_mlp_grad", "mpm_mlp_adam", "mpm_set_surrogate", "mpm_log_samples",
+    "mpm_h5_create", "mpm_h5_write", "mpm_h5_close", "mpm_snapshot", "mpm_snapshot_wait",
 ]
 NOALLOC_MAX_PARTICLES = 1 << 19
 NOALLOC_MAX_KEYS = 1 << 19
@@ -86,12 +88,12 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
               "-Xcompiler", "-fPIC", "-shared"]
 
 
-TRANSLATION_UNITS = ["mpm_b200.cu", "mpm_noalloc.cu", "mpm_grf.cu", "mpm_mlp.cu"]
+TRANSLATION_UNITS = ["mpm_b200.cu", "mpm_noalloc.cu", "mpm_grf.cu", "mpm_mlp.cu", "mpm_h5.cpp"]
 
 
 def sources():
     return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
-            if f.endswith((".cu", ".cuh"))] + [os.path.join(INCLUDE, "mpm_b200.h")]
+            if f.endswith((".cu", ".cuh", ".cpp"))] + [os.path.join(INCLUDE, "mpm_b200.h")]
 
 
 def build(force=False, verbose=False):
@@ -154,6 +156,11 @@ def lib():
     L.mpm_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int64, vp]
     L.mpm_grf_eval.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                C.c_double, C.c_void_p]
+    L.mpm_h5_create.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.mpm_h5_write.argtypes = [vp, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_int64), vp]
+    L.mpm_h5_close.argtypes = [vp]
+    L.mpm_snapshot.argtypes = [vp, vp, C.c_int64, C.c_double, C.c_uint32, C.c_int32]
+    L.mpm_snapshot_wait.argtypes = [vp, C.POINTER(C.c_int64)]
     sizes = [C.c_int64() for _ in range(4)]
     L.mpm_abi_sizes(*[C.byref(x) for x in sizes])
     mine = [C.sizeof(Desc), C.sizeof(View), C.sizeof(HostViews), C.sizeof(Stats)]

@@ -12,9 +12,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace mpm;
@@ -63,6 +67,37 @@ struct GraphCache {
     bool tiled = false;
     int surr_mode = 0;
     int64_t launches = 0, steps = 0, sorts = 0;
+};
+
+// Snapshots in flight (mpm_snapshot): two slots, each a device buffer the
+// un-permuting gather writes and a pinned host buffer the copy stream fills;
+// a writer thread puts a slot into the file once its copy finished.
+struct SnapJob {
+    int slot;
+    mpm_h5 *file;
+    int64_t group;
+    double Ti;
+    uint32_t mask;
+    int32_t type;
+};
+struct SnapState {
+    cudaStream_t copy = nullptr;
+    cudaEvent_t gathered[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+    void *dev[2] = {nullptr, nullptr}, *host[2] = {nullptr, nullptr};
+    size_t cap = 0;
+    bool busy[2] = {false, false};
+    int next = 0;
+    int device = 0;
+    int64_t np = 0;
+    int dim = 3;
+    std::thread th;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<SnapJob> q;
+    bool stop = false;
+    int err = MPM_OK;
+    std::string msg;
+    int64_t written = 0;
 };
 
 struct mpm_handle {
@@ -129,6 +164,7 @@ struct mpm_handle {
     std::vector<cudaEvent_t> kev;
     int kernels_per_step = 4;
     int64_t launches = 0;
+    SnapState *snap = nullptr;
 };
 
 namespace {
@@ -859,6 +895,73 @@ template <int D, typename R> struct Download {
     }
 };
 
+// ---- snapshots: the particle fields of one HDF5 group of submit_work! ------------
+// (src/solver.jl:60-70: stress, strain_s, eqstrain, ekstrain, eqrate, coords,
+// velocity_s, volume, mass_s), gathered into the original particle order.
+struct SnapField {
+    uint32_t bit;
+    const char *name;
+};
+constexpr SnapField kSnapFields[] = {
+    {MPM_F_SIG, "stress"},    {MPM_F_EPS, "strain_s"},   {MPM_F_EPSQ, "eqstrain"},
+    {MPM_F_EPSK, "ekstrain"}, {MPM_F_EPSV, "eqrate"},    {MPM_F_XI, "coords"},
+    {MPM_F_VS, "velocity_s"}, {MPM_F_OMEGA, "volume"},   {MPM_F_MS, "mass_s"}};
+
+int snap_columns(uint32_t bit, int dim) {
+    const int nv = dim == 2 ? 4 : 6;
+    switch (bit) {
+    case MPM_F_SIG: case MPM_F_EPS: return nv;
+    case MPM_F_XI: case MPM_F_VS: return dim;
+    default: return 1;
+    }
+}
+
+struct SnapCols {
+    const void *src[24];
+    int32_t f64[24];   // 1: the column is FP64 (positions), else the bulk type
+};
+
+template <typename R, typename O>
+__global__ void k_snap_gather(SnapCols c, const uint32_t *orig, int64_t np, O *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const int col = blockIdx.y;
+    const double v = c.f64[col] ? ((const double *)c.src[col])[i] : (double)((const R *)c.src[col])[i];
+    out[(int64_t)col * np + orig[i]] = (O)v;
+}
+
+template <int D, typename R> struct SnapGather {
+    // Launches the gather of `mask`'s fields into `out` (element type `type`) on the compute stream.
+    static void go(mpm_handle *h, uint32_t mask, int32_t type, void *out) {
+        const int64_t np = h->d.np;
+        PDev<D, R> P = pdev_from<D, R>(h, 0);
+        constexpr int NV = PDev<D, R>::NV;
+        SnapCols c{};
+        int n = 0;
+        auto add = [&](const void *p, int f64) { c.src[n] = p; c.f64[n] = f64; ++n; };
+        for (const SnapField &f : kSnapFields) {
+            if (!(mask & f.bit)) continue;
+            switch (f.bit) {
+            case MPM_F_SIG: for (int k = 0; k < NV; ++k) add(P.sig[k], 0); break;
+            case MPM_F_EPS: for (int k = 0; k < NV; ++k) add(P.eps[k], 0); break;
+            case MPM_F_EPSQ: add(P.epsq, 0); break;
+            case MPM_F_EPSK: add(P.epsk, 0); break;
+            case MPM_F_EPSV: add(P.epsv, 0); break;
+            case MPM_F_XI: for (int d = 0; d < D; ++d) add(P.x[d], 1); break;
+            case MPM_F_VS: for (int d = 0; d < D; ++d) add(P.v[d], 0); break;
+            case MPM_F_OMEGA: add(P.vol, 0); break;
+            case MPM_F_MS: add(P.m, 0); break;
+            }
+        }
+        if (!n || !np) return;
+        const dim3 grid((unsigned)cdiv(np, 256), (unsigned)n);
+        if (type == MPM_T_F64) k_snap_gather<R, double><<<grid, 256, 0, h->stream>>>(c, P.orig, np, (double *)out);
+        else k_snap_gather<R, float><<<grid, 256, 0, h->stream>>>(c, P.orig, np, (float *)out);
+        LAUNCH_CHECK();
+        ++h->launches;
+    }
+};
+
 template <int D, typename R> struct P2CAll {
     static void go(mpm_handle *h, int64_t *out) {
         const int64_t np = h->d.np;
@@ -965,6 +1068,75 @@ template <int D, typename R> struct GridOut {
         }
     }
 };
+
+// Writer thread of a handle's snapshots: waits for each slot's device-to-host
+// copy, writes the slot's fields as group<i>/<name> and group<i>/time, frees
+// the slot.  Ends when asked to stop and the queue is empty.
+void snap_writer(SnapState *S) {
+    cudaSetDevice(S->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    while (true) {
+        S->cv.wait(lk, [&] { return S->stop || !S->q.empty(); });
+        if (S->q.empty()) break;
+        const SnapJob j = S->q.front();
+        lk.unlock();
+        int rc = MPM_OK;
+        std::string msg;
+        const cudaError_t e = cudaEventSynchronize(S->copied[j.slot]);
+        if (e != cudaSuccess) {
+            rc = MPM_E_CUDA;
+            msg = std::string("snapshot copy: ") + cudaGetErrorString(e);
+        }
+        const size_t es = j.type == MPM_T_F64 ? 8 : 4;
+        const char *base = (const char *)S->host[j.slot];
+        const std::string g = "group" + std::to_string(j.group) + "/";
+        for (const SnapField &f : kSnapFields) {
+            if (rc != MPM_OK) break;
+            if (!(j.mask & f.bit)) continue;
+            const int k = snap_columns(f.bit, S->dim);
+            const int64_t dims[2] = {k, S->np};   // a Julia np x k matrix is the dataspace (k, np)
+            rc = mpm_h5_write(j.file, (g + f.name).c_str(), j.type, k > 1 ? 2 : 1, k > 1 ? dims : dims + 1, base);
+            if (rc != MPM_OK) msg = mpm_last_error(nullptr);
+            base += (size_t)k * S->np * es;
+        }
+        if (rc == MPM_OK) {
+            const double t64 = j.Ti;
+            const float t32 = (float)j.Ti;
+            rc = mpm_h5_write(j.file, (g + "time").c_str(), j.type, 0, nullptr,
+                              j.type == MPM_T_F64 ? (const void *)&t64 : (const void *)&t32);
+            if (rc != MPM_OK) msg = mpm_last_error(nullptr);
+        }
+        lk.lock();
+        S->q.pop_front();
+        S->busy[j.slot] = false;
+        if (rc == MPM_OK) ++S->written;
+        else if (S->err == MPM_OK) {
+            S->err = rc;
+            S->msg = msg;
+        }
+        S->cv.notify_all();
+    }
+}
+
+void snap_destroy(mpm_handle *h) {
+    SnapState *S = h->snap;
+    if (!S) return;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+    }
+    S->cv.notify_all();
+    if (S->th.joinable()) S->th.join();
+    for (int k = 0; k < 2; ++k) {
+        if (S->dev[k]) cudaFree(S->dev[k]);
+        if (S->host[k]) cudaFreeHost(S->host[k]);
+        if (S->gathered[k]) cudaEventDestroy(S->gathered[k]);
+        if (S->copied[k]) cudaEventDestroy(S->copied[k]);
+    }
+    if (S->copy) cudaStreamDestroy(S->copy);
+    delete S;
+    h->snap = nullptr;
+}
 
 int fail(mpm_handle *h, const Err &e) {
     if (h) h->last_error = e.msg;
@@ -1294,6 +1466,96 @@ int mpm_download(mpm_handle *h, const mpm_host_views *v, uint32_t mask) {
     } catch (const Err &e) { return fail(h, e); }
 }
 
+int mpm_snapshot(mpm_handle *h, mpm_h5 *f, int64_t group, double Ti, uint32_t mask, int32_t type) {
+    if (!h) return MPM_E_ARG;
+    try {
+        if (!f) throw Err{MPM_E_ARG, "mpm_snapshot: null file"};
+        if (!h->uploaded) throw Err{MPM_E_STATE, "mpm_snapshot before mpm_upload"};
+        if (type != MPM_T_F64 && type != MPM_T_F32) throw Err{MPM_E_ARG, "snapshot type must be MPM_T_F64 or MPM_T_F32"};
+        if (!mask || (mask & ~(uint32_t)MPM_F_SNAPSHOT)) throw Err{MPM_E_ARG, "snapshot fields outside MPM_F_SNAPSHOT"};
+        if (group < 0) throw Err{MPM_E_ARG, "negative snapshot group"};
+        CK(cudaSetDevice(h->dev));
+        const int64_t np = h->d.np;
+        int64_t ncol = 0;
+        for (const SnapField &fd : kSnapFields)
+            if (mask & fd.bit) ncol += snap_columns(fd.bit, h->d.dim);
+        const size_t bytes = std::max<size_t>(16, (size_t)(ncol * np) * (type == MPM_T_F64 ? 8 : 4));
+        SnapState *S = h->snap;
+        if (!S) {
+            S = new SnapState;
+            S->device = h->dev;
+            S->np = np;
+            S->dim = h->d.dim;
+            h->snap = S;
+            CK(cudaStreamCreateWithFlags(&S->copy, cudaStreamNonBlocking));
+            for (int k = 0; k < 2; ++k) {
+                CK(cudaEventCreateWithFlags(&S->gathered[k], cudaEventDisableTiming));
+                CK(cudaEventCreateWithFlags(&S->copied[k], cudaEventDisableTiming));
+            }
+            S->th = std::thread(snap_writer, S);
+        }
+        std::unique_lock<std::mutex> lk(S->mu);
+        if (S->err != MPM_OK) {
+            Err e{S->err, S->msg};
+            S->err = MPM_OK;
+            throw e;
+        }
+        if (S->cap < bytes) {
+            S->cv.wait(lk, [&] { return !S->busy[0] && !S->busy[1]; });
+            for (int k = 0; k < 2; ++k) {
+                if (S->dev[k]) { cudaFree(S->dev[k]); h->bytes -= S->cap; S->dev[k] = nullptr; }
+                if (S->host[k]) { cudaFreeHost(S->host[k]); S->host[k] = nullptr; }
+            }
+            S->cap = 0;
+            for (int k = 0; k < 2; ++k) {
+                CK(cudaMalloc(&S->dev[k], bytes));
+                h->bytes += bytes;
+                CK(cudaMallocHost(&S->host[k], bytes));
+            }
+            S->cap = bytes;
+        }
+        const int slot = S->next;
+        S->cv.wait(lk, [&] { return !S->busy[slot]; });
+        S->busy[slot] = true;
+        S->next ^= 1;
+        lk.unlock();
+        try {
+            // gather on the compute stream (after every step issued so far), copy on the copy stream
+            dispatch<SnapGather>(h, mask, type, S->dev[slot]);
+            CK(cudaEventRecord(S->gathered[slot], h->stream));
+            CK(cudaStreamWaitEvent(S->copy, S->gathered[slot], 0));
+            CK(cudaMemcpyAsync(S->host[slot], S->dev[slot], bytes, cudaMemcpyDeviceToHost, S->copy));
+            CK(cudaEventRecord(S->copied[slot], S->copy));
+        } catch (...) {
+            std::lock_guard<std::mutex> g(S->mu);
+            S->busy[slot] = false;
+            throw;
+        }
+        lk.lock();
+        S->q.push_back(SnapJob{slot, f, group, Ti, mask, type});
+        S->cv.notify_all();
+        return MPM_OK;
+    } catch (const Err &e) { return fail(h, e); }
+}
+
+int mpm_snapshot_wait(mpm_handle *h, int64_t *written) {
+    if (!h) return MPM_E_ARG;
+    SnapState *S = h->snap;
+    if (!S) {
+        if (written) *written = 0;
+        return MPM_OK;
+    }
+    std::unique_lock<std::mutex> lk(S->mu);
+    S->cv.wait(lk, [&] { return S->q.empty(); });
+    if (written) *written = S->written;
+    if (S->err != MPM_OK) {
+        const Err e{S->err, S->msg};
+        S->err = MPM_OK;
+        return fail(h, e);
+    }
+    return MPM_OK;
+}
+
 int mpm_compute_p2c(mpm_handle *h, int64_t *out) {
     if (!h || !out) return MPM_E_ARG;
     try {
@@ -1349,6 +1611,7 @@ int mpm_destroy(mpm_handle *h) {
     if (!h) return MPM_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    snap_destroy(h);
     for (void *p : h->allocs) cudaFree(p);
     if (h->graph.exec) cudaGraphExecDestroy(h->graph.exec);
     for (auto e : h->kev) cudaEventDestroy(e);

@@ -857,8 +857,8 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
         for (int k = 0; k < D * D; ++k) dF[k] *= dt;
         // doublemapping1_a_USL_OS! / doublemapping1_OS! (OS_USL.jl:185-320)
         const R FLIP = (R)sp.FLIP, PIC = (R)sp.PIC;
-#pragma unroll
         if (pre) prefetch_wait();
+#pragma unroll
         for (int d = 0; d < D; ++d) {
             const R vo = pf(pre, PF_V + d, P.v[d] + i);
             const R vn = sp.va == 0 ? FLIP * vo + PIC * tT[d] + ta[d] * dt : FLIP * (vo + (tT[d] - tv[d])) + PIC * tT[d];

@@ -11,6 +11,7 @@ runs of consecutive steps so the host is not in the loop of every step.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import time
 
 import numpy as np
@@ -194,6 +195,21 @@ class DeviceModel:
         _lib.check(_lib.lib().mpm_log_samples(self.h, feat.data_ptr(), target.data_ptr(), count.data_ptr(), cap,
                                               int(every)), self.h)
 
+    # HDF5 snapshots (submit_work!, src/solver.jl:60-76)
+    def snapshot(self, h5file, group, Ti, fields=_lib.F_SNAPSHOT, dtype=np.float64):
+        """Enqueue group ``group<group>`` of the particle fields and ``time`` =
+        Ti into ``h5file`` (hdf5.H5File); returns at once, the copy and the
+        file write overlap the following steps."""
+        t = _lib.T_F64 if np.dtype(dtype) == np.float64 else _lib.T_F32
+        _lib.check(_lib.lib().mpm_snapshot(self.h, h5file.h, int(group), float(Ti), fields, t), self.h)
+
+    def snapshot_wait(self):
+        """Wait until every enqueued snapshot is in its file; returns how many
+        groups were written."""
+        n = C.c_int64()
+        _lib.check(_lib.lib().mpm_snapshot_wait(self.h, C.byref(n)), self.h)
+        return n.value
+
     # clean_device! (devicehelpfunc_cuda.jl:71-100)
     def close(self):
         if getattr(self, "h", None):
@@ -239,6 +255,55 @@ def procedure(args, dev, dT, Ti):
     dev.step(dT, Ti, 1)
 
 
+def snapshot_path(args):
+    """<project_path>/<project_name>/<project_name>.h5 (src/solver.jl:57)."""
+    return os.path.join(args.project_path, args.project_name, f"{args.project_name}.h5")
+
+
+def _run_with_snapshots(args, grid, mp, attr, bc, dev, nsteps, workflow):
+    """submit_work!'s HDF5 branch (src/solver.jl:54-111): a group before the
+    step whenever ``hdf5_switch`` is 0 or ``hdf5_step``, i.e. before steps 0,
+    hdf5_step, 2*hdf5_step, ...; then FILE_NUM (groups written + 1), the grid
+    coordinates, the initial particle coordinates, nid and the velocity BCs.
+    The runs between snapshots go to the device as one call; each snapshot's
+    copy and file write overlap the next run."""
+    from .hdf5 import H5File
+    T = np.float32 if args.precision == "FP32" else np.float64
+    path = snapshot_path(args)
+    if os.path.isfile(path):
+        os.remove(path)
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    f = H5File(path)
+    try:
+        hdf5_id, done, Ti = 1, 0, T(0.0)
+        while done < nsteps:
+            dev.snapshot(f, hdf5_id, float(Ti), dtype=T)
+            hdf5_id += 1
+            n = min(args.hdf5_step, nsteps - done)
+            if workflow is None:
+                Ti = T(dev.step(args.dT, float(Ti), n))
+            else:
+                for _ in range(n):
+                    workflow(args, dev, args.dT, float(Ti))
+                    Ti = T(Ti + T(args.dT))
+            done += n
+        dev.snapshot_wait()
+        I = attr.nid.dtype
+        f.write("FILE_NUM", np.asarray(hdf5_id, I))
+        f.write("grid_coords", grid.xi)
+        f.write("mp_coords0", mp.xi0)
+        f.write("nid", attr.nid)
+        axes = ("x", "y", "z")[:grid.dim]
+        for a in axes:
+            f.write(f"vbc_{a}s_idx", getattr(bc, f"v{a}_s_idx"))
+            f.write(f"vbc_{a}s_val", getattr(bc, f"v{a}_s_val"))
+    finally:
+        try:
+            dev.snapshot_wait()
+        finally:
+            f.close()
+
+
 def materialpointsolver(args, grid, mp, attr, bc, workflow=None, device=0, verbose=False):
     """Entry point mirroring materialpointsolver! (src/MaterialPointSolver.jl:61-76).
 
@@ -251,14 +316,14 @@ def materialpointsolver(args, grid, mp, attr, bc, workflow=None, device=0, verbo
         raise NotImplementedError("the one-phase MUSL and USL schemes are provided")
     if args.basis != "uGIMP":
         raise NotImplementedError("only the uGIMP basis is provided")
-    if args.hdf5:
-        raise NotImplementedError("HDF5 snapshots are not provided by this backend")
     dev = host2device(args, grid, mp, attr, bc, device)
     try:
         mp.p2c[:] = dev.p2c().astype(mp.p2c.dtype)   # initmpstatus! (src/solver.jl:45)
         nsteps = time_sequence(args)
         args.start_time = time.time()
-        if workflow is None:
+        if args.hdf5:
+            _run_with_snapshots(args, grid, mp, attr, bc, dev, nsteps, workflow)
+        elif workflow is None:
             Ti = dev.step(args.dT, 0.0, nsteps) if nsteps else 0.0
         else:
             T = np.float32 if args.precision == "FP32" else np.float64
