@@ -61,6 +61,10 @@ extern "C" {
 /* update scheme (args.scheme) */
 #define MPM_SCHEME_MUSL 0
 #define MPM_SCHEME_USL 1
+/* coupling: one-phase (OS_*.jl) or two-phase solid + water (TS_MUSL.jl, MUSL only;
+ * restated: the reference's own two-phase path does not run as shipped) */
+#define MPM_COUPLING_OS 0
+#define MPM_COUPLING_TS 1
 
 /* 3D Mohr-Coulomb: the reference's 3D mcP! body is commented out, so its 3D
  * "mohrcoulomb" run is the elastic predictor only (LITERAL).  RESTATED applies
@@ -100,7 +104,8 @@ typedef struct {
     int32_t time_f32;      /* 1: accumulate Ti in Float32 (reference FP32 mode) */
     int32_t sort_every;    /* re-sort period in steps (0 = library default) */
     int32_t scheme;        /* MPM_SCHEME_MUSL (OS_MUSL.jl) or MPM_SCHEME_USL (OS_USL.jl) */
-    int32_t reserved;      /* 0 */
+    int32_t coupling;      /* MPM_COUPLING_OS or MPM_COUPLING_TS (Args.coupling) */
+    double zeta_w;         /* Args.ζw (two-phase water damping) */
 } mpm_desc;
 
 /* A host array view. */
@@ -134,6 +139,16 @@ typedef struct {
     mpm_view Ks, Gs, c, phi, psi, sigt, Hp, cr; /* nmat each */
     /* VBoundary2D/3D, per node in the reference's node order */
     mpm_view vx_idx, vx_val, vy_idx, vy_val, vz_idx, vz_val;
+    /* two-phase (coupling = TS): Particle2D/3D water fields, Property Kw and k,
+     * VBoundary water velocity BC (vx_w_idx … vz_w_val; absent = none) */
+    mpm_view n;       /* n      np         porosity */
+    mpm_view rhow;    /* ρw     np         (upload; download: ρw0 / J) */
+    mpm_view sigw;    /* σw     np         pore pressure */
+    mpm_view vw;      /* vw     np x dim   */
+    mpm_view epsw;    /* ϵijw   np x 4|6   */
+    mpm_view mw;      /* mw     np         (download only) */
+    mpm_view Kw, kperm; /* nmat each */
+    mpm_view vxw_idx, vxw_val, vyw_idx, vyw_val, vzw_idx, vzw_val;
 } mpm_host_views;
 
 /* download field mask */
@@ -150,9 +165,17 @@ typedef struct {
 #define MPM_F_F (1u << 10)
 #define MPM_F_RHO (1u << 11)
 #define MPM_F_P2C (1u << 12)
+#define MPM_F_MW (1u << 13)     /* two-phase fields */
+#define MPM_F_VW (1u << 14)
+#define MPM_F_SIGW (1u << 15)
+#define MPM_F_EPSW (1u << 16)
+#define MPM_F_N (1u << 17)
+#define MPM_F_RHOW (1u << 18)
 /* the set device2host! copies (devicehelpfunc_cuda.jl:46-55) */
 #define MPM_F_REFERENCE (MPM_F_SIGM | MPM_F_VS | MPM_F_XI | MPM_F_OMEGA | MPM_F_SIG | \
                          MPM_F_EPSK | MPM_F_EPSQ | MPM_F_EPSV | MPM_F_EPS | MPM_F_MS)
+/* ... and the two-phase additions (devicehelpfunc_cuda.jl:56-62) */
+#define MPM_F_REFERENCE_TS (MPM_F_REFERENCE | MPM_F_MW | MPM_F_VW | MPM_F_SIGW | MPM_F_EPSW | MPM_F_N)
 
 typedef struct {
     int64_t steps_done;        /* steps run on this handle */
@@ -301,7 +324,8 @@ int mpm_log_samples(mpm_handle *h, float *feat, float *target, uint32_t *count, 
  * mpm_snapshot enqueues one group of submit_work! (src/solver.jl:60-70):
  * "group<group>/" + stress, strain_s, eqstrain, ekstrain, eqrate, coords,
  * velocity_s, volume, mass_s (the fields of field_mask, a subset of
- * MPM_F_SNAPSHOT) in the original particle order, and "time" = Ti, all of
+ * MPM_F_SNAPSHOT; two-phase models also pressure_w, strain_w, velocity_w,
+ * porosity, MPM_F_SNAPSHOT_TS) in the original particle order, and "time" = Ti, all of
  * element type `type` (MPM_T_F64 or MPM_T_F32).  It returns at once: the
  * fields are gathered on the handle's stream behind the steps issued so far,
  * copied to pinned host memory on a second stream while later steps run, and
@@ -316,6 +340,8 @@ int mpm_h5_write(mpm_h5 *f, const char *name, int32_t type, int32_t rank, const 
 int mpm_h5_close(mpm_h5 *f);
 #define MPM_F_SNAPSHOT (MPM_F_SIG | MPM_F_EPS | MPM_F_EPSQ | MPM_F_EPSK | MPM_F_EPSV | MPM_F_XI | \
                         MPM_F_VS | MPM_F_OMEGA | MPM_F_MS)
+/* two-phase groups add pressure_w, strain_w, velocity_w, porosity (src/solver.jl:73-76) */
+#define MPM_F_SNAPSHOT_TS (MPM_F_SNAPSHOT | MPM_F_SIGW | MPM_F_EPSW | MPM_F_VW | MPM_F_N)
 int mpm_snapshot(mpm_handle *h, mpm_h5 *f, int64_t group, double Ti, uint32_t field_mask, int32_t type);
 int mpm_snapshot_wait(mpm_handle *h, int64_t *written);
 

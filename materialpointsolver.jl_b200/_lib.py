@@ -25,12 +25,16 @@ ERRORS = {
 LINEARELASTIC, DRUCKERPRAGER, MOHRCOULOMB = 0, 1, 2
 PREC_MIXED, PREC_FP64 = 0, 1
 SCHEME_MUSL, SCHEME_USL = 0, 1
+COUPLING_OS, COUPLING_TS = 0, 1
 T_F64, T_F32, T_I64, T_I32 = 0, 1, 2, 3
 
 F_XI, F_VS, F_SIG, F_EPS, F_EPSQ, F_EPSK, F_EPSV = (1 << i for i in range(7))
 F_OMEGA, F_MS, F_SIGM, F_F, F_RHO, F_P2C = (1 << i for i in range(7, 13))
+F_MW, F_VW, F_SIGW, F_EPSW, F_N, F_RHOW = (1 << i for i in range(13, 19))
 F_REFERENCE = F_SIGM | F_VS | F_XI | F_OMEGA | F_SIG | F_EPSK | F_EPSQ | F_EPSV | F_EPS | F_MS
+F_REFERENCE_TS = F_REFERENCE | F_MW | F_VW | F_SIGW | F_EPSW | F_N
 F_SNAPSHOT = F_SIG | F_EPS | F_EPSQ | F_EPSK | F_EPSV | F_XI | F_VS | F_OMEGA | F_MS
+F_SNAPSHOT_TS = F_SNAPSHOT | F_SIGW | F_EPSW | F_VW | F_N
 
 EXPORTS = [
     "mpm_create", "mpm_upload", "mpm_destroy", "mpm_step", "mpm_step_async", "mpm_sync",
@@ -56,7 +60,8 @@ class Desc(C.Structure):
         ("constitutive", C.c_int32), ("va", C.c_int32), ("mvl", C.c_int32), ("mc3d", C.c_int32),
         ("FLIP", C.c_double), ("PIC", C.c_double), ("zeta_s", C.c_double), ("gravity", C.c_double),
         ("Te", C.c_double),
-        ("time_f32", C.c_int32), ("sort_every", C.c_int32), ("scheme", C.c_int32), ("reserved", C.c_int32),
+        ("time_f32", C.c_int32), ("sort_every", C.c_int32), ("scheme", C.c_int32), ("coupling", C.c_int32),
+        ("zeta_w", C.c_double),
     ]
 
 
@@ -71,7 +76,9 @@ _VIEW_NAMES = ["xi", "vs", "sig", "eps", "epsq", "epsk", "epsv", "Omega", "Omega
 class HostViews(C.Structure):
     _fields_ = ([(n, View) for n in _VIEW_NAMES] +
                 [(n, View) for n in ("Ks", "Gs", "c", "phi", "psi", "sigt", "Hp", "cr")] +
-                [(n, View) for n in ("vx_idx", "vx_val", "vy_idx", "vy_val", "vz_idx", "vz_val")])
+                [(n, View) for n in ("vx_idx", "vx_val", "vy_idx", "vy_val", "vz_idx", "vz_val")] +
+                [(n, View) for n in ("n", "rhow", "sigw", "vw", "epsw", "mw", "Kw", "kperm")] +
+                [(n, View) for n in ("vxw_idx", "vxw_val", "vyw_idx", "vyw_val", "vzw_idx", "vzw_val")])
 
 
 class Stats(C.Structure):

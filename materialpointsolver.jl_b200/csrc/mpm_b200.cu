@@ -5,6 +5,7 @@
 // cell sort.  Kernels live in mpm_kernels.cuh / mpm_sort.cuh.
 #include "../../include/mpm_b200.h"
 #include "mpm_tiled.cuh"
+#include "mpm_ts.cuh"
 
 #include <cuda_runtime.h>
 
@@ -134,6 +135,8 @@ struct mpm_handle {
     void *pbuf[2] = {nullptr, nullptr};
     // grid
     void *acc = nullptr, *gat = nullptr, *gvs = nullptr;   // node records (see mpm_kernels.cuh)
+    bool ts = false;                                         // two-phase coupling (mpm_ts.cuh)
+    void *accw = nullptr, *accd = nullptr, *gatw = nullptr, *bcvalw = nullptr;
     uint8_t *bcmask = nullptr;
     void *bcval = nullptr;
     void *csigm = nullptr, *comega = nullptr;   // MVL cell sums (R), nc each
@@ -201,10 +204,17 @@ template <int D, typename R> PDev<D, R> pdev_from(mpm_handle *h, int which) {
     P.orig = (uint32_t *)take(4);
     R *coh = (R *)take(sizeof(R));
     P.coh = h->coh_mode ? coh : nullptr;
+    if (h->ts) {
+        P.n = (R *)take(sizeof(R));
+        P.sigw = (R *)take(sizeof(R));
+        P.mw = (R *)take(sizeof(R));
+        for (int d = 0; d < 3; ++d) P.vw[d] = d < D ? (R *)take(sizeof(R)) : nullptr;
+        for (int c = 0; c < 6; ++c) P.epsw[c] = c < PDev<D, R>::NV ? (R *)take(sizeof(R)) : nullptr;
+    }
     return P;
 }
 
-size_t pbuf_bytes(int D, bool fp64, int64_t np) {
+size_t pbuf_bytes(int D, bool fp64, int64_t np, bool ts) {
     size_t R = fp64 ? 8 : 4;
     size_t per = 0;
     auto add = [&](size_t elem, int count) { per += count * (((np * elem + 255) / 256) * 256); };
@@ -216,6 +226,11 @@ size_t pbuf_bytes(int D, bool fp64, int64_t np) {
     add(R, NV);
     add(R, 7);
     add(4, 2);
+    if (ts) {
+        add(R, 3);      // n, σw, mw
+        add(R, D);      // vw
+        add(R, NV);     // ϵijw
+    }
     return per;
 }
 
@@ -261,6 +276,10 @@ template <typename R> GDev<R> gdev_from(mpm_handle *h) {
     g.nbx = h->nbx;
     g.nby = h->nby;
     g.nbz = h->nbz;
+    g.accw = (Node8<R> *)h->accw;
+    g.accd = (T4 *)h->accd;
+    g.gatw = (Node8<R> *)h->gatw;
+    g.bcvalw = (const T4 *)h->bcvalw;
     return g;
 }
 
@@ -304,11 +323,14 @@ __global__ void k_iota(uint32_t *a, int64_t n) {
 }
 template <int D, typename R>
 __global__ void k_derived(PDev<D, R> P, int64_t np, int what, double *out) {
-    // what: 0 Ω = det(F) Ω0 (FP64 det), 1 σm, 2 ρs = ρs0 / J, with ρs0 = m / Ω0
+    // what: 0 Ω = det(F) Ω0 (FP64 det), 1 σm, 2 ρs = ρs0 / J, with ρs0 = m / Ω0,
+    // 3 ρw = mw / Ω (two-phase)
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
     double v = 0;
-    if (what == 1) {
+    if (what == 3) {
+        v = (double)P.mw[i] / (double)P.vol[i];
+    } else if (what == 1) {
         v = (double)((P.sig[0][i] + P.sig[1][i] + P.sig[2][i]) * (R)0.333333);
     } else {
         double J;
@@ -396,6 +418,11 @@ template <typename R> void build_materials(mpm_handle *h, const mpm_host_views *
         m.sphi = (R)std::sin(phi); m.cphi = (R)std::cos(phi); m.tphi = (R)std::tan(phi);
         m.spsi = (R)std::sin(psi); m.tpsi = (R)std::tan(psi);
         m.kc = (R)((6.0 * std::cos(phi)) / (1.732051 * (3.0 + std::sin(phi))));
+        if (h->ts) {
+            m.Kw = (R)get(v->Kw, v->Kw.ld > i ? i : 0);
+            m.kperm = (R)get(v->kperm, v->kperm.ld > i ? i : 0);
+            if (!(m.kperm != R(0))) throw Err{MPM_E_ARG, "two-phase model needs a non-zero permeability k"};
+        }
     }
     CK(cudaMemcpy(h->mat, M.data(), nm * sizeof(Mat<R>), cudaMemcpyHostToDevice));
 }
@@ -495,8 +522,10 @@ template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, do
     sp.need_vs = (h->d.va == MPM_VA_V || (h->d.PIC != 0.0 && !sp.usl)) ? 1 : 0;
     sp.np = h->d.np;
     sp.mvl = h->d.mvl ? 1 : 0;
+    sp.ts = h->ts ? 1 : 0;
+    sp.zeta_w = h->d.zeta_w;
     sp.surr = h->surr;
-    sp.surr.mode = (D == 3 && h->d.constitutive == MPM_DRUCKERPRAGER) ? h->surr_mode : 0;
+    sp.surr.mode = (D == 3 && h->d.constitutive == MPM_DRUCKERPRAGER && !h->ts) ? h->surr_mode : 0;
     sp.surr.salt = (uint32_t)(h->steps_done * 0x9E3779B9ull);
     return sp;
 }
@@ -510,7 +539,13 @@ template <int D, typename R> void standalone_p2g(mpm_handle *h, double Ti, Launc
     PDev<D, R> P = pdev_from<D, R>(h, 0);
     GDev<R> g = gdev_from<R>(h);
     StepParams sp = make_params<D, R>(h, 0.0, Ti, gravity_at(h->d, Ti));
-    if (np) L.run("p2g", [&] { k_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+    if (h->ts) {
+        CK(cudaMemsetAsync(h->accw, 0, h->ni * sizeof(Node8<R>), h->stream));
+        CK(cudaMemsetAsync(h->accd, 0, h->ni * sizeof(T4), h->stream));
+        if (np) L.run("p2g", [&] { k_p2g_ts<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+    } else if (np) {
+        L.run("p2g", [&] { k_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+    }
     h->acc_valid = true;
     h->acc_Ti = Ti;
 }
@@ -551,6 +586,20 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
     GDev<R> g = gdev_from<R>(h);
     StepParams sp = make_params<D, R>(h, dt, Ti, gravity_at(h->d, Tn));
     const bool mc3 = sp.mc3d && sp.constitutive == MPM_MOHRCOULOMB;
+    if (sp.ts) {
+        // two-phase MUSL (TS_MUSL.jl): solve, DM1+DM2, DM3, G2P_TS! + next P2G_TS!
+        L.run("solve", [&] { k_solve_ts<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+        if (np) L.run("dmap", [&] { k_dmap_ts<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("dm3", [&] { k_dm3_ts<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+        CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
+        if (np) L.run("g2p_p2g", [&] {
+            if (mc3) k_g2p_ts<D, R, true, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_g2p_ts<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+        });
+        h->since_sort++;
+        h->steps_done++;
+        return;
+    }
     L.run("solve", [&] { k_solve<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
     if (h->tiled && !sp.mvl && !sp.usl && sp.surr.mode != 2) {
         TileList tl{h->tiles, h->ntiles, h->off, h->sg};
@@ -778,6 +827,29 @@ template <int D, typename R> struct Upload {
                 for (int64_t i = 0; i < np; ++i) m[i] = (R)(view_get(v->Omega, i, 0) * view_get(v->rho, i, 0));
                 CK(cudaMemcpy(P.m, m.data(), np * sizeof(R), cudaMemcpyHostToDevice));
             }
+            if (h->ts) {
+                // two-phase fields (particle.jl:103-128); mw = Ω·ρw is invariant like ms
+                req(v->n, "n");
+                req(v->rhow, "rhow");
+                upload_col<R>(h, v->n, 0, P.n, np);
+                opt(v->sigw, P.sigw);
+                for (int d = 0; d < D; ++d) {
+                    if (v->vw.ptr) upload_col<R>(h, v->vw, d, P.vw[d], np);
+                    else CK(cudaMemsetAsync(P.vw[d], 0, np * sizeof(R), h->stream));
+                }
+                for (int c = 0; c < NV; ++c) {
+                    if (v->epsw.ptr) upload_col<R>(h, v->epsw, c, P.epsw[c], np);
+                    else CK(cudaMemsetAsync(P.epsw[c], 0, np * sizeof(R), h->stream));
+                }
+                std::vector<R> mw(np);
+                for (int64_t i = 0; i < np; ++i) {
+                    const double n = view_get(v->n, i, 0);
+                    if (!(n > 0.0 && n < 1.0)) throw Err{MPM_E_ARG, "two-phase porosity n must lie in (0, 1)"};
+                    mw[i] = (R)(view_get(v->Omega, i, 0) * view_get(v->rhow, i, 0));
+                }
+                CK(cudaMemcpy(P.mw, mw.data(), np * sizeof(R), cudaMemcpyHostToDevice));
+                if (!v->Kw.ptr || !v->kperm.ptr) throw Err{MPM_E_ARG, "two-phase model needs the Kw and k arrays"};
+            }
             {
                 std::vector<uint32_t> mid(np);
                 for (int64_t i = 0; i < np; ++i) {
@@ -806,6 +878,12 @@ template <int D, typename R> struct Upload {
         bool anyval = false;
         const mpm_view *idx[3] = {&v->vx_idx, &v->vy_idx, &v->vz_idx};
         const mpm_view *vv[3] = {&v->vx_val, &v->vy_val, &v->vz_val};
+        // water velocity BC (VBoundary *_w_*): arrays shorter than ni (the
+        // reference's [0] default) mean none
+        const mpm_view *widx[3] = {&v->vxw_idx, &v->vyw_idx, &v->vzw_idx};
+        const mpm_view *wv[3] = {&v->vxw_val, &v->vyw_val, &v->vzw_val};
+        std::vector<T4> valw(h->ts ? ni : 0);
+        bool anyw = false;
         for (int64_t r = 0; r < ni; ++r) {
             int64_t inode = r;
             if (D == 2) {  // reference 2D: y descending inside a column
@@ -821,8 +899,25 @@ template <int D, typename R> struct Upload {
                     if (vals[d] != R(0)) anyval = true;
                 }
             }
+            if (h->ts) {
+                R wvals[3] = {0, 0, 0};
+                for (int d = 0; d < D; ++d) {
+                    if (widx[d]->ptr && widx[d]->ld >= ni && view_geti(*widx[d], r) != 0) {
+                        mk |= (uint8_t)(8 << d);
+                        wvals[d] = (wv[d]->ptr && wv[d]->ld >= ni) ? (R)view_get(*wv[d], r, 0) : R(0);
+                        if (wvals[d] != R(0)) anyw = true;
+                    }
+                }
+                valw[inode].x = wvals[0]; valw[inode].y = wvals[1]; valw[inode].z = wvals[2]; valw[inode].w = 0;
+            }
             mask[inode] = mk;
             val[inode].x = vals[0]; val[inode].y = vals[1]; val[inode].z = vals[2]; val[inode].w = 0;
+        }
+        if (anyw) {
+            if (!h->bcvalw) h->bcvalw = dalloc(h, ni * sizeof(T4));
+            CK(cudaMemcpy(h->bcvalw, valw.data(), ni * sizeof(T4), cudaMemcpyHostToDevice));
+        } else {
+            h->bcvalw = nullptr;
         }
         CK(cudaMemcpy(h->bcmask, mask.data(), ni, cudaMemcpyHostToDevice));
         if (anyval) {
@@ -857,6 +952,13 @@ template <int D, typename R> struct Download {
         if (mask & MPM_F_EPSK) { chk(v->epsk, "epsk"); download_col<R>(h, P.epsk, P.orig, v->epsk, 0, np); }
         if (mask & MPM_F_EPSV) { chk(v->epsv, "epsv"); download_col<R>(h, P.epsv, P.orig, v->epsv, 0, np); }
         if (mask & MPM_F_MS) { chk(v->ms, "ms"); download_col<R>(h, P.m, P.orig, v->ms, 0, np); }
+        const uint32_t tsmask = MPM_F_MW | MPM_F_VW | MPM_F_SIGW | MPM_F_EPSW | MPM_F_N | MPM_F_RHOW;
+        if ((mask & tsmask) && !h->ts) throw Err{MPM_E_ARG, "two-phase fields requested from a one-phase model"};
+        if (mask & MPM_F_MW) { chk(v->mw, "mw"); download_col<R>(h, P.mw, P.orig, v->mw, 0, np); }
+        if (mask & MPM_F_N) { chk(v->n, "n"); download_col<R>(h, P.n, P.orig, v->n, 0, np); }
+        if (mask & MPM_F_SIGW) { chk(v->sigw, "sigw"); download_col<R>(h, P.sigw, P.orig, v->sigw, 0, np); }
+        if (mask & MPM_F_VW) { chk(v->vw, "vw"); for (int d = 0; d < D; ++d) download_col<R>(h, P.vw[d], P.orig, v->vw, d, np); }
+        if (mask & MPM_F_EPSW) { chk(v->epsw, "epsw"); for (int c = 0; c < NV; ++c) download_col<R>(h, P.epsw[c], P.orig, v->epsw, c, np); }
         auto derived = [&](int what, const mpm_view &vw, const char *name) {
             chk(vw, name);
             double *tmp = (double *)dalloc(h, np * 8);
@@ -874,6 +976,7 @@ template <int D, typename R> struct Download {
         if (mask & MPM_F_OMEGA) derived(0, v->Omega, "Omega");
         if (mask & MPM_F_SIGM) derived(1, v->sigm, "sigm");
         if (mask & MPM_F_RHO) derived(2, v->rho, "rho");
+        if (mask & MPM_F_RHOW) derived(3, v->rhow, "rhow");
         if (mask & MPM_F_P2C) {
             chk(v->p2c, "p2c");
             if (v->p2c.type != MPM_T_I64 && v->p2c.type != MPM_T_I32) throw Err{MPM_E_ARG, "p2c view must be integer"};
@@ -905,20 +1008,22 @@ struct SnapField {
 constexpr SnapField kSnapFields[] = {
     {MPM_F_SIG, "stress"},    {MPM_F_EPS, "strain_s"},   {MPM_F_EPSQ, "eqstrain"},
     {MPM_F_EPSK, "ekstrain"}, {MPM_F_EPSV, "eqrate"},    {MPM_F_XI, "coords"},
-    {MPM_F_VS, "velocity_s"}, {MPM_F_OMEGA, "volume"},   {MPM_F_MS, "mass_s"}};
+    {MPM_F_VS, "velocity_s"}, {MPM_F_OMEGA, "volume"},   {MPM_F_MS, "mass_s"},
+    // two-phase groups (src/solver.jl:73-76)
+    {MPM_F_SIGW, "pressure_w"}, {MPM_F_EPSW, "strain_w"}, {MPM_F_VW, "velocity_w"}, {MPM_F_N, "porosity"}};
 
 int snap_columns(uint32_t bit, int dim) {
     const int nv = dim == 2 ? 4 : 6;
     switch (bit) {
-    case MPM_F_SIG: case MPM_F_EPS: return nv;
-    case MPM_F_XI: case MPM_F_VS: return dim;
+    case MPM_F_SIG: case MPM_F_EPS: case MPM_F_EPSW: return nv;
+    case MPM_F_XI: case MPM_F_VS: case MPM_F_VW: return dim;
     default: return 1;
     }
 }
 
 struct SnapCols {
-    const void *src[24];
-    int32_t f64[24];   // 1: the column is FP64 (positions), else the bulk type
+    const void *src[40];
+    int32_t f64[40];   // 1: the column is FP64 (positions), else the bulk type
 };
 
 template <typename R, typename O>
@@ -951,6 +1056,10 @@ template <int D, typename R> struct SnapGather {
             case MPM_F_VS: for (int d = 0; d < D; ++d) add(P.v[d], 0); break;
             case MPM_F_OMEGA: add(P.vol, 0); break;
             case MPM_F_MS: add(P.m, 0); break;
+            case MPM_F_SIGW: add(P.sigw, 0); break;
+            case MPM_F_EPSW: for (int k = 0; k < NV; ++k) add(P.epsw[k], 0); break;
+            case MPM_F_VW: for (int d = 0; d < D; ++d) add(P.vw[d], 0); break;
+            case MPM_F_N: add(P.n, 0); break;
             }
         }
         if (!n || !np) return;
@@ -1194,7 +1303,13 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         if (d->constitutive < 0 || d->constitutive > 2) throw Err{MPM_E_UNSUPPORTED, "constitutive model not provided (hyperelastic is out of scope)"};
         if (d->mc3d != MPM_MC3D_LITERAL && d->mc3d != MPM_MC3D_RESTATED) throw Err{MPM_E_ARG, "mc3d must be 0 or 1"};
         if (d->scheme != MPM_SCHEME_MUSL && d->scheme != MPM_SCHEME_USL) throw Err{MPM_E_ARG, "scheme must be 0 (MUSL) or 1 (USL)"};
+        if (d->coupling != MPM_COUPLING_OS && d->coupling != MPM_COUPLING_TS) throw Err{MPM_E_ARG, "coupling must be 0 (OS) or 1 (TS)"};
+        if (d->coupling == MPM_COUPLING_TS && d->scheme != MPM_SCHEME_MUSL)
+            throw Err{MPM_E_UNSUPPORTED, "the two-phase coupling has the MUSL scheme only (TS_MUSL.jl)"};
+        if (d->coupling == MPM_COUPLING_TS && d->mvl)
+            throw Err{MPM_E_UNSUPPORTED, "MVL with the two-phase coupling is not provided"};
         h->d = *d;
+        h->ts = d->coupling == MPM_COUPLING_TS;
         if (h->d.dim == 2) { h->d.nnz = 1; h->d.z1 = 0; h->d.dz = 1; h->d.lpz = 1; }
         h->fp64 = d->precision == MPM_PREC_FP64;
         h->sort_every = d->sort_every > 0 ? d->sort_every : 8;
@@ -1206,7 +1321,7 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         CK(cudaEventCreate(&h->ev1));
         const size_t R = h->fp64 ? 8 : 4;
         const size_t T4 = 4 * R;
-        size_t pb = pbuf_bytes(d->dim, h->fp64, d->np);
+        size_t pb = pbuf_bytes(d->dim, h->fp64, d->np, h->ts);
         h->pbuf[0] = dalloc(h, pb);
         h->pbuf[1] = dalloc(h, pb);
         h->acc = dalloc(h, ni * 2 * T4);
@@ -1214,6 +1329,14 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         h->gvs = (d->PIC != 0.0 || d->va == MPM_VA_V) ? dalloc(h, ni * T4) : nullptr;
         CK(cudaMemset(h->acc, 0, ni * 2 * T4));
         CK(cudaMemset(h->gat, 0, ni * 2 * T4));
+        if (h->ts) {
+            h->accw = dalloc(h, ni * 2 * T4);
+            h->accd = dalloc(h, ni * T4);
+            h->gatw = dalloc(h, ni * 2 * T4);
+            CK(cudaMemset(h->accw, 0, ni * 2 * T4));
+            CK(cudaMemset(h->accd, 0, ni * T4));
+            CK(cudaMemset(h->gatw, 0, ni * 2 * T4));
+        }
         if (h->gvs) CK(cudaMemset(h->gvs, 0, ni * T4));
         h->bcmask = (uint8_t *)dalloc(h, ni);
         CK(cudaMemset(h->bcmask, 0, ni));
@@ -1472,7 +1595,8 @@ int mpm_snapshot(mpm_handle *h, mpm_h5 *f, int64_t group, double Ti, uint32_t ma
         if (!f) throw Err{MPM_E_ARG, "mpm_snapshot: null file"};
         if (!h->uploaded) throw Err{MPM_E_STATE, "mpm_snapshot before mpm_upload"};
         if (type != MPM_T_F64 && type != MPM_T_F32) throw Err{MPM_E_ARG, "snapshot type must be MPM_T_F64 or MPM_T_F32"};
-        if (!mask || (mask & ~(uint32_t)MPM_F_SNAPSHOT)) throw Err{MPM_E_ARG, "snapshot fields outside MPM_F_SNAPSHOT"};
+        const uint32_t allowed = h->ts ? (uint32_t)MPM_F_SNAPSHOT_TS : (uint32_t)MPM_F_SNAPSHOT;
+        if (!mask || (mask & ~allowed)) throw Err{MPM_E_ARG, "snapshot fields outside MPM_F_SNAPSHOT(_TS) of this model"};
         if (group < 0) throw Err{MPM_E_ARG, "negative snapshot group"};
         CK(cudaSetDevice(h->dev));
         const int64_t np = h->d.np;
@@ -1590,6 +1714,7 @@ int mpm_run_stages(mpm_handle *h, double dt, double Ti, uint32_t mask) {
     if (!h) return MPM_E_ARG;
     try {
         if (!h->uploaded) throw Err{MPM_E_STATE, "mpm_run_stages before mpm_upload"};
+        if (h->ts) throw Err{MPM_E_UNSUPPORTED, "per-stage runs are provided for the one-phase step"};
         CK(cudaSetDevice(h->dev));
         dispatch<Stages>(h, dt, Ti, mask);
         CK(cudaStreamSynchronize(h->stream));

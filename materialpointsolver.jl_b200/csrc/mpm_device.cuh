@@ -188,7 +188,8 @@ template <typename R> struct Mat {
     R kphi, qphi, qpsi, st, ab, tb, dq;   // Drucker-Prager (druckerprager.jl:39-44, 59)
     R sphi, cphi, tphi, spsi, tpsi;       // Mohr-Coulomb
     R kc;                                 // kphi per unit cohesion
-    R pad;
+    R Kw, kperm;                          // two-phase: water bulk modulus, permeability k
+    R pad[3];
 };
 
 // liE!, src/materials/linearelastic.jl:22-69 (2D) / :78-140 (3D).  s: Voigt

@@ -50,6 +50,11 @@ template <int D, typename R> struct PDev {
     R *m, *vol0, *vol;
     uint32_t *mat, *orig;
     R *coh;   // per-particle cohesion (random-field materials), else NULL
+    // two-phase fields (coupling = :TS), else NULL: porosity n, pore pressure σw,
+    // water mass mw = Ω·ρw (invariant like m), water velocity, water strain ϵijw
+    R *n, *sigw, *mw;
+    R *vw[3];
+    R *epsw[6];
 };
 
 template <typename R> struct alignas(2 * sizeof(typename Vec<R>::T4)) Node8 {
@@ -73,6 +78,11 @@ template <typename R> struct GDev {
     uint32_t *blist;        // the flagged blocks, in the order they were flagged
     uint32_t *bcount;       // number of entries in blist
     int nbx, nby, nbz;      // node blocks per axis (blocks of BX x BY x BZ nodes)
+    // two-phase records (coupling = :TS), else NULL: acc holds {ms, ps | fs, mi}
+    Node8<R> *accw;         // a = (mw, pw), b = (fw, 0)
+    T4 *accd;               // drag force (fd, 0)
+    Node8<R> *gatw;         // a = (vwT, 0), b = (vw, 0) after the solve, (Δuw, 0) after DM3
+    const T4 *bcvalw;       // fixed water velocities (NULL when all zero); bcmask bits 3-5
 };
 
 // streaming (evict-first) access to the particle arrays, which are touched
@@ -209,6 +219,8 @@ struct StepParams {
     int mvl;         // volumetric-locking mitigation (cell-averaged mean stress)
     int usl;         // USL scheme (OS_USL.jl): no double mapping, Δu = vsT·dt
     int prefetch;    // FP32 particle pass: fields staged in dynamic shared memory (PF_N x 256 floats)
+    int ts;          // two-phase coupling (TS_MUSL.jl)
+    double zeta_w;   // ζw, water damping (two-phase)
     SurrCtx surr;
     int64_t np;
 };
@@ -651,7 +663,7 @@ __device__ __forceinline__ void surr_features(const SurrCtx &c, int64_t i, const
 template <int D, typename R, bool MC3 = false>
 __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp,
                                                 int64_t i, double *x, const R *tT, const R *dF, R *s, R &vol,
-                                                const float *pre = nullptr) {
+                                                const float *pre = nullptr, double *Jout = nullptr) {
     constexpr int NV = PDev<D, R>::NV, NF = PDev<D, R>::NF;
     // position: ξ += ΔT·ΣN·vsT, accumulated in FP64
 #pragma unroll
@@ -709,6 +721,7 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
     for (int k = 0; k < NF; ++k) stcs(P.F[k] + i, fn[k]);
     vol = (R)(J * (double)pf(pre, PF_VOL0, P.vol0 + i));
     stcs(P.vol + i, vol);
+    if (Jout) *Jout = J;
     // stress: liE! then dpP! / mcP! (OS_MUSL.jl:82-96)
     Mat<R> M = g.mat[pfu(pre, PF_MAT, P.mat + i)];
     if (P.coh) {

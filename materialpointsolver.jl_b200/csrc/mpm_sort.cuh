@@ -267,6 +267,13 @@ __global__ void k_permute(PDev<D, R> src, PDev<D, R> dst, const uint2 *pairs, in
     dst.m[k] = src.m[o]; dst.vol0[k] = src.vol0[o]; dst.vol[k] = src.vol[o];
     dst.mat[k] = src.mat[o];
     if (src.coh) dst.coh[k] = src.coh[o];
+    if (src.n) {
+        dst.n[k] = src.n[o]; dst.sigw[k] = src.sigw[o]; dst.mw[k] = src.mw[o];
+#pragma unroll
+        for (int d = 0; d < D; ++d) dst.vw[d][k] = src.vw[d][o];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) dst.epsw[c][k] = src.epsw[c][o];
+    }
     dst.orig[k] = pr.x;
 }
 

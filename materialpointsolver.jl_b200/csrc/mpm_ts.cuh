@@ -1,0 +1,394 @@
+// mpm_ts.cuh -- two-phase (coupling = :TS) MUSL step: procedure!(…, Val(:TS),
+// Val(:MUSL)), src/solvers/TS_MUSL.jl:13-54, kernels of src/solvers/utils_TS.jl.
+//
+// The reference's two-phase path does not run as shipped; this restatement
+// keeps its arithmetic and repairs three defects:
+//   * submit_work! calls workflow(…, Val(coupling), Val(scheme), Val(va))
+//     (src/solver.jl:84-85) while the :TS procedure! takes two Val arguments
+//     (TS_MUSL.jl:13-23): the step runs whatever va is;
+//   * G2P_TS! reads mp.ρs_init / mp.ρw_init (utils_TS.jl:849-850, 953-954),
+//     fields Particle2D/3D do not have (particle.jl:60-62: ρs0 / ρw0), and the
+//     3D kernel writes mp.Δfs (utils_TS.jl:893-895): the fields meant are used;
+//   * resetmpstatus_TS! evaluates the uGIMP basis on the first NIC of the
+//     16 / 64 candidate nodes (utils_TS.jl:216-227, 266-283), leaving support
+//     nodes out: the weights are the one-phase support-filtered stencil.
+// Kept as written: grid.mi accumulates N·mw·n while the mixture's gravity uses
+// the particle's mi = Ω((1-n)ρs + nρw); zero (not eps) guards the nodal
+// inverses; the 3D G2P_TS! adds the solid strain increment to ϵijw.
+//
+// Same step structure as the one-phase MUSL kernels: particle masses ms = Ω·ρs
+// and mw = Ω·ρw are invariant (Ω = JΩ0, ρ = ρ0/J) and kept per particle; the
+// G2P pass carries DM1's position update and, fused, the next step's
+// resetmpstatus_TS! + P2G_TS! at the new position.  Node records (FP32, 32 B):
+//   acc  {ms, psx, psy, psz | fsx, fsy, fsz, mi}    gat  {vsT, 0 | vs -> Δus, 0}
+//   accw {mw, pwx, pwy, pwz | fwx, fwy, fwz, 0}     gatw {vwT, 0 | vw -> Δuw, 0}
+//   accd {fdx, fdy, fdz, 0}
+#pragma once
+#include "mpm_kernels.cuh"
+
+namespace mpm {
+
+// P2G_TS!, utils_TS.jl:295-393: solid mass (1-n)·ms, Σ N·mw·n, water mass,
+// both momenta, the mixture force -Ω ∇N·(σ + σw I) + N·mi·G, the water force
+// -Ω ∇N σw + N·mw·G (gravity on the last axis) and the drag N·(n mw G/k)(vw - vs).
+template <int D, typename R>
+__device__ __forceinline__ void p2g_scatter_ts(const GDev<R> &g, const AxisW<R> *w, R ms, R mw, R n, R vol,
+                                               const R *vs, const R *vw, const R *s, R sw, R G, R kperm) {
+    const MarkState mk = mark_begin<D, R>(g, w);
+    const R one_n = R(1) - n;
+    const R mi = one_n * ms + n * mw;   // Ω((1-n)ρs + nρw)
+    const R tdg = (n * mw * G) / kperm;
+    R ps[3], pw[3], dr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        ps[d] = d < D ? ms * vs[d] * one_n : R(0);
+        pw[d] = d < D ? mw * vw[d] * n : R(0);
+        dr[d] = d < D ? tdg * (vw[d] - vs[d]) : R(0);
+    }
+    // rows of σ + σw I (Voigt xx yy zz xy yz zx; 2D xx yy zz xy)
+    R sx[3], sy[3], sz[3];
+    if (D == 2) {
+        sx[0] = s[0] + sw; sx[1] = s[3]; sx[2] = R(0);
+        sy[0] = s[3]; sy[1] = s[1] + sw; sy[2] = R(0);
+        sz[0] = sz[1] = sz[2] = R(0);
+    } else {
+        sx[0] = s[0] + sw; sx[1] = s[3]; sx[2] = s[5];
+        sy[0] = s[3]; sy[1] = s[1] + sw; sy[2] = s[4];
+        sz[0] = s[5]; sz[1] = s[4]; sz[2] = s[2] + sw;
+    }
+    const int n0 = window_n0<D, R>(g, w);
+    const int plane = g.nnx * g.nny;
+    constexpr int NC = D == 3 ? 3 : 1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const R wz = D == 3 ? w[2].N[c] : R(1), gz = D == 3 ? w[2].dN[c] : R(0);
+        if (wz == R(0)) continue;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const R wx = w[0].N[a], gx = w[0].dN[a];
+            if (wx == R(0)) continue;
+            const int col = n0 + a * g.nny + c * plane;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const R wy = w[1].N[b], gy = w[1].dN[b];
+                if (wy == R(0)) continue;
+                const R N = wx * wy * wz;
+                const R dN[3] = {gx * wy * wz, wx * gy * wz, wx * wy * gz};
+                R fs[3], fw[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    fs[d] = R(0);
+                    fw[d] = R(0);
+                }
+                fs[0] = -vol * (dN[0] * sx[0] + dN[1] * sx[1] + dN[2] * sx[2]);
+                fs[1] = -vol * (dN[0] * sy[0] + dN[1] * sy[1] + dN[2] * sy[2]);
+                if (D == 3) fs[2] = -vol * (dN[0] * sz[0] + dN[1] * sz[1] + dN[2] * sz[2]);
+#pragma unroll
+                for (int d = 0; d < D; ++d) fw[d] = -vol * (dN[d] * sw);
+                fs[D - 1] += N * mi * G;
+                fw[D - 1] += N * mw * G;
+                const int q = col + b;
+                red_add4(&g.acc[q].a, N * ms * one_n, N * ps[0], N * ps[1], N * ps[2]);
+                red_add4(&g.acc[q].b, fs[0], fs[1], fs[2], N * mw * n);
+                red_add4(&g.accw[q].a, N * mw, N * pw[0], N * pw[1], N * pw[2]);
+                red_add4(&g.accw[q].b, fw[0], fw[1], fw[2], R(0));
+                red_add4(&g.accd[q], N * dr[0], N * dr[1], N * dr[2], R(0));
+            }
+        }
+    }
+    mark_end<R>(g, mk);
+}
+
+template <int D, typename R>
+__device__ __forceinline__ void load_vel(R *const *src, int64_t i, R *v) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d] = d < D ? src[d][i] : R(0);
+}
+
+// Standalone two-phase P2G (first step after an upload).
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_p2g_ts(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    double x[3];
+    load_x<D, R>(P, i, x);
+    AxisW<R> w[3];
+    if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
+    R vs[3], vw[3], s[6];
+    load_vel<D, R>(P.v, i, vs);
+    load_vel<D, R>(P.vw, i, vw);
+#pragma unroll
+    for (int k = 0; k < PDev<D, R>::NV; ++k) s[k] = P.sig[k][i];
+    const Mat<R> &M = g.mat[P.mat[i]];
+    p2g_scatter_ts<D, R>(g, w, P.m[i], P.mw[i], P.n[i], P.vol[i], vs, vw, s, P.sigw[i], (R)sp.G, M.kperm);
+}
+
+// solvegrid_TS!, utils_TS.jl:404-532.  Keeps the masses for DM3 and clears the
+// momenta, forces, Σ N·mw·n and the drag.
+template <int D, typename R>
+__device__ __forceinline__ void solve_node_ts(const GDev<R> &g, const StepParams &sp, int i) {
+    using T4 = typename Vec<R>::T4;
+    const Node8<R> S = g.acc[i], W = g.accw[i];
+    const T4 fd4 = g.accd[i];
+    const R ms = S.a.x, mw = W.a.x, mi = S.b.w;
+    const R msd = ms == R(0) ? R(0) : R(1) / ms, mwd = mw == R(0) ? R(0) : R(1) / mw;
+    const R ps[3] = {S.a.y, S.a.z, S.a.w}, pw[3] = {W.a.y, W.a.z, W.a.w};
+    const R fs[3] = {S.b.x, S.b.y, S.b.z}, fw[3] = {W.b.x, W.b.y, W.b.z}, fd[3] = {fd4.x, fd4.y, fd4.z};
+    R vs[3] = {0, 0, 0}, vw[3] = {0, 0, 0}, vsT[3] = {0, 0, 0}, vwT[3] = {0, 0, 0};
+    R qw = R(0), qs = R(0);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        vs[d] = ps[d] * msd;
+        vw[d] = pw[d] * mwd;
+        qw += fw[d] * fw[d];
+        qs += (fs[d] - fw[d]) * (fs[d] - fw[d]);
+    }
+    const R tw = -(R)sp.zeta_w * sqrt(qw), tsd = -(R)sp.zeta * sqrt(qs);
+    const R dt = (R)sp.dt;
+    const uint8_t bm = g.bcmask[i];
+    R bv[3] = {0, 0, 0}, bw[3] = {0, 0, 0};
+    if (g.bcval) { const T4 b = g.bcval[i]; bv[0] = b.x; bv[1] = b.y; bv[2] = b.z; }
+    if (g.bcvalw) { const T4 b = g.bcvalw[i]; bw[0] = b.x; bw[1] = b.y; bw[2] = b.z; }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const R dw = tw * sgn(vw[d]), ds = tsd * sgn(vs[d]);
+        const R aw = mwd * (fw[d] + dw + fd[d]);
+        const R as = msd * (-mi * aw + fs[d] + dw + ds);
+        vsT[d] = vs[d] + as * dt;
+        vwT[d] = vw[d] + aw * dt;
+        if (bm & (1 << d)) vsT[d] = bv[d];
+        if (bm & (8 << d)) vwT[d] = bw[d];
+    }
+    Node8<R> o;
+    o.a = mk4<R>(vsT[0], vsT[1], vsT[2], 0);
+    o.b = mk4<R>(vs[0], vs[1], vs[2], 0);
+    g.gat[i] = o;
+    o.a = mk4<R>(vwT[0], vwT[1], vwT[2], 0);
+    o.b = mk4<R>(vw[0], vw[1], vw[2], 0);
+    g.gatw[i] = o;
+    Node8<R> z;
+    z.b = mk4<R>(0, 0, 0, 0);
+    z.a = mk4<R>(ms, 0, 0, 0);
+    g.acc[i] = z;
+    z.a = mk4<R>(mw, 0, 0, 0);
+    g.accw[i] = z;
+    g.accd[i] = z.b;
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(128) k_solve_ts(GDev<R> g, StepParams sp) {
+    const uint32_t nb = *g.bcount;
+    for (uint32_t k = blockIdx.x; k < nb; k += gridDim.x) {
+        const int i = block_node<D, R>(g, (int)g.blist[k], threadIdx.x);
+        if (i >= 0) solve_node_ts<D, R>(g, sp, i);
+    }
+}
+
+// doublemapping1_TS! (utils_TS.jl:543-648, velocities of both phases) fused
+// with doublemapping2_TS! (utils_TS.jl:657-704, re-scatter of both momenta).
+// The position update of DM1 is done by k_g2p_ts from the same ΣN·vsT.
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    double x[3];
+    load_x<D, R>(P, i, x);
+    AxisW<R> w[3];
+    particle_weights<D, R>(x, g, w);   // out-of-grid particles get zero weights
+    const int n0 = window_n0<D, R>(g, w);
+    const int plane = g.nnx * g.nny;
+    constexpr int NC = D == 3 ? 3 : 1;
+    R s1[3] = {0, 0, 0}, s2[3] = {0, 0, 0}, w1[3] = {0, 0, 0}, w2[3] = {0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const R wz = D == 3 ? w[2].N[c] : R(1);
+        if (wz == R(0)) continue;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const R wxz = w[0].N[a] * wz;
+            if (wxz == R(0)) continue;
+            const int col = n0 + a * g.nny + c * plane;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const R wy = w[1].N[b];
+                if (wy == R(0)) continue;
+                const R N = wxz * wy;
+                const Node8<R> S = g.gat[col + b], W = g.gatw[col + b];
+                const R vT[3] = {S.a.x, S.a.y, S.a.z}, v0[3] = {S.b.x, S.b.y, S.b.z};
+                const R wT[3] = {W.a.x, W.a.y, W.a.z}, w0[3] = {W.b.x, W.b.y, W.b.z};
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    s1[d] += N * (vT[d] - v0[d]);
+                    s2[d] += N * vT[d];
+                    w1[d] += N * (wT[d] - w0[d]);
+                    w2[d] += N * wT[d];
+                }
+            }
+        }
+    }
+    const R FLIP = (R)sp.FLIP, PIC = (R)sp.PIC;
+    const R n = P.n[i], ms = P.m[i], mw = P.mw[i];
+    R ps[3] = {0, 0, 0}, pw[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const R vs = FLIP * (P.v[d][i] + s1[d]) + PIC * s2[d];
+        const R vw = FLIP * (P.vw[d][i] + w1[d]) + PIC * w2[d];
+        P.v[d][i] = vs;
+        P.vw[d][i] = vw;
+        ps[d] = ms * vs * (R(1) - n);
+        pw[d] = mw * vw * n;
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const R wz = D == 3 ? w[2].N[c] : R(1);
+        if (wz == R(0)) continue;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const R wxz = w[0].N[a] * wz;
+            if (wxz == R(0)) continue;
+            const int col = n0 + a * g.nny + c * plane;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const R wy = w[1].N[b];
+                if (wy == R(0)) continue;
+                const R N = wxz * wy;
+                red_add4(&g.acc[col + b].a, R(0), N * ps[0], N * ps[1], N * ps[2]);
+                red_add4(&g.accw[col + b].a, R(0), N * pw[0], N * pw[1], N * pw[2]);
+            }
+        }
+    }
+}
+
+// doublemapping3_TS!, utils_TS.jl:713-780: nodal velocities of both phases from
+// the re-mapped momenta, BC, Δus = vs·ΔT, Δuw = vw·ΔT.  Clears the masses and
+// momenta for the next P2G and the block flags.
+template <int D, typename R>
+__device__ __forceinline__ void dm3_node_ts(const GDev<R> &g, const StepParams &sp, int i) {
+    using T4 = typename Vec<R>::T4;
+    const T4 S = g.acc[i].a, W = g.accw[i].a;
+    const R msd = S.x == R(0) ? R(0) : R(1) / S.x, mwd = W.x == R(0) ? R(0) : R(1) / W.x;
+    const R ps[3] = {S.y, S.z, S.w}, pw[3] = {W.y, W.z, W.w};
+    const uint8_t bm = g.bcmask[i];
+    R bv[3] = {0, 0, 0}, bw[3] = {0, 0, 0};
+    if (g.bcval) { const T4 b = g.bcval[i]; bv[0] = b.x; bv[1] = b.y; bv[2] = b.z; }
+    if (g.bcvalw) { const T4 b = g.bcvalw[i]; bw[0] = b.x; bw[1] = b.y; bw[2] = b.z; }
+    const R dt = (R)sp.dt;
+    R us[3] = {0, 0, 0}, uw[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        R vs = ps[d] * msd, vw = pw[d] * mwd;
+        if (bm & (1 << d)) vs = bv[d];
+        if (bm & (8 << d)) vw = bw[d];
+        us[d] = vs * dt;
+        uw[d] = vw * dt;
+    }
+    g.gat[i].b = mk4<R>(us[0], us[1], us[2], 0);
+    g.gatw[i].b = mk4<R>(uw[0], uw[1], uw[2], 0);
+    g.acc[i].a = mk4<R>(0, 0, 0, 0);
+    g.accw[i].a = mk4<R>(0, 0, 0, 0);
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(128) k_dm3_ts(GDev<R> g, StepParams sp) {
+    const uint32_t nb = *g.bcount;
+    for (uint32_t k = blockIdx.x; k < nb; k += gridDim.x) {
+        const int b = (int)g.blist[k];
+        const int i = block_node<D, R>(g, b, threadIdx.x);
+        if (i >= 0) dm3_node_ts<D, R>(g, sp, i);
+        if (threadIdx.x == 0) g.bflag[b] = 0u;
+    }
+}
+
+// G2P_TS! (utils_TS.jl:790-961): the solid part is G2P_OS!'s arithmetic
+// (update_particle: position, strain, F, J, Ω, liE! + dpP!/mcP!), then the
+// water strain, the pore pressure σw += Kw/n ((1-n) tr ΔFs + n tr ΔFw) and
+// the porosity n = 1 - (1-n)/ΔJ with ΔJ = J Ω0 / Ω_old.  With FUSE the next
+// step's P2G_TS! scatters the particle at its new position.
+template <int D, typename R, bool FUSE, bool MC3 = false>
+__global__ void __launch_bounds__(256) k_g2p_ts(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    double x[3];
+    load_x<D, R>(P, i, x);
+    AxisW<R> w[3];
+    particle_weights<D, R>(x, g, w);
+    const int n0 = window_n0<D, R>(g, w);
+    const int plane = g.nnx * g.nny;
+    constexpr int NC = D == 3 ? 3 : 1;
+    // ΣΔu⊗∇N = Σ(Δu - Δu_c)⊗∇N (Σ∇N = 0): the window centre's increments are
+    // subtracted so that FP32 sums of a near-translation do not cancel
+    const int ncen = n0 + g.nny + 1 + (D == 3 ? plane : 0);
+    const auto cs = g.gat[ncen].b, cw = g.gatw[ncen].b;
+    R tT[3] = {0, 0, 0}, dF[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, dW[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const R wz = D == 3 ? w[2].N[c] : R(1), gz = D == 3 ? w[2].dN[c] : R(0);
+        if (wz == R(0)) continue;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const R wx = w[0].N[a], gx = w[0].dN[a];
+            if (wx == R(0)) continue;
+            const int col = n0 + a * g.nny + c * plane;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const R wy = w[1].N[b], gy = w[1].dN[b];
+                if (wy == R(0)) continue;
+                const R N = wx * wy * wz;
+                const R dN[3] = {gx * wy * wz, wx * gy * wz, wx * wy * gz};
+                const Node8<R> S = g.gat[col + b];
+                const auto Wb = g.gatw[col + b].b;
+                const R us[3] = {S.b.x - cs.x, S.b.y - cs.y, S.b.z - cs.z};
+                const R uw[3] = {Wb.x - cw.x, Wb.y - cw.y, Wb.z - cw.z};
+                tT[0] += N * S.a.x; tT[1] += N * S.a.y; tT[2] += N * S.a.z;
+#pragma unroll
+                for (int r = 0; r < D; ++r)
+#pragma unroll
+                    for (int q = 0; q < D; ++q) {
+                        dF[r * D + q] += us[r] * dN[q];
+                        dW[r * D + q] += uw[r] * dN[q];
+                    }
+            }
+        }
+    }
+    constexpr int NV = PDev<D, R>::NV;
+    const R vol_old = P.vol[i];
+    R s[6], vol;
+    double J = 1.0;
+    update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol, nullptr, &J);
+    // water part of G2P_TS!
+    const Mat<R> &M = g.mat[P.mat[i]];
+    const R n = P.n[i];
+    R trs, trw;
+    if (D == 2) {
+        P.epsw[0][i] += dW[0];
+        P.epsw[1][i] += dW[3];
+        P.epsw[3][i] += dW[1] + dW[2];
+        trs = dF[0] + dF[3];
+        trw = dW[0] + dW[3];
+    } else {
+        // the solid increments, as utils_TS.jl:929-934 writes them
+        P.epsw[0][i] += dF[0];
+        P.epsw[1][i] += dF[4];
+        P.epsw[2][i] += dF[8];
+        P.epsw[3][i] += dF[1] + dF[3];
+        P.epsw[4][i] += dF[5] + dF[7];
+        P.epsw[5][i] += dF[2] + dF[6];
+        trs = dF[0] + dF[4] + dF[8];
+        trw = dW[0] + dW[4] + dW[8];
+    }
+    const R dJ = (R)(J * (double)P.vol0[i] / (double)vol_old);
+    const R sw = P.sigw[i] + (M.Kw / n) * ((R(1) - n) * trs + n * trw);
+    const R nn = R(1) - (R(1) - n) / dJ;
+    P.sigw[i] = sw;
+    P.n[i] = nn;
+    if (FUSE) {
+        if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
+        R vs[3], vw[3];
+        load_vel<D, R>(P.v, i, vs);
+        load_vel<D, R>(P.vw, i, vw);
+        p2g_scatter_ts<D, R>(g, w, P.m[i], P.mw[i], nn, vol, vs, vw, s, sw, (R)sp.G, M.kperm);
+    }
+    (void)NV;
+}
+
+}  // namespace mpm

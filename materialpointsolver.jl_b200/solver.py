@@ -48,6 +48,16 @@ def host_views(grid, mp, attr, bc):
     hv.vy_idx, hv.vy_val = _view(bc.vy_s_idx), _view(bc.vy_s_val)
     if grid.dim == 3:
         hv.vz_idx, hv.vz_val = _view(bc.vz_s_idx), _view(bc.vz_s_val)
+    if getattr(mp, "phase", 1) == 2:
+        # two-phase fields (particle.jl:103-128), Kw and k, water BC
+        hv.n, hv.rhow, hv.sigw, hv.vw = _view(mp.n), _view(mp.rho_w), _view(mp.sigw), _view(mp.vw)
+        hv.epsw, hv.mw = _view(mp.epsw), _view(mp.mw)
+        hv.Kw, hv.kperm = _view(attr.Kw), _view(attr.k)
+        for c in "xyz"[:grid.dim]:
+            idx = getattr(bc, f"v{c}_w_idx", None)
+            if idx is not None:
+                setattr(hv, f"v{c}w_idx", _view(idx))
+                setattr(hv, f"v{c}w_val", _view(getattr(bc, f"v{c}_w_val")))
     return hv
 
 
@@ -74,6 +84,8 @@ def make_desc(args, grid, mp, attr, device=0):
     d.time_f32 = 1 if args.precision == "FP32" else 0
     d.sort_every = getattr(args, "sort_every", 0)
     d.scheme = _lib.SCHEME_USL if getattr(args, "scheme", "MUSL") == "USL" else _lib.SCHEME_MUSL
+    d.coupling = _lib.COUPLING_TS if getattr(args, "coupling", "OS") == "TS" else _lib.COUPLING_OS
+    d.zeta_w = getattr(args, "zeta_w", 0.0)
     return d
 
 
@@ -228,7 +240,7 @@ def host2device(args, grid, mp, attr, bc, device=0):
 
 
 def device2host(args, mp, dev, verbose=False):
-    dev.download(_lib.F_REFERENCE, mp)
+    dev.download(_lib.F_REFERENCE_TS if args.coupling == "TS" else _lib.F_REFERENCE, mp)
     if verbose:
         print("downloading from :B200 -> host")
 
@@ -276,8 +288,9 @@ def _run_with_snapshots(args, grid, mp, attr, bc, dev, nsteps, workflow):
     f = H5File(path)
     try:
         hdf5_id, done, Ti = 1, 0, T(0.0)
+        fields = _lib.F_SNAPSHOT_TS if args.coupling == "TS" else _lib.F_SNAPSHOT
         while done < nsteps:
-            dev.snapshot(f, hdf5_id, float(Ti), dtype=T)
+            dev.snapshot(f, hdf5_id, float(Ti), fields=fields, dtype=T)
             hdf5_id += 1
             n = min(args.hdf5_step, nsteps - done)
             if workflow is None:
@@ -297,6 +310,10 @@ def _run_with_snapshots(args, grid, mp, attr, bc, dev, nsteps, workflow):
         for a in axes:
             f.write(f"vbc_{a}s_idx", getattr(bc, f"v{a}_s_idx"))
             f.write(f"vbc_{a}s_val", getattr(bc, f"v{a}_s_val"))
+        if args.coupling == "TS":
+            for a in axes:
+                f.write(f"vbc_{a}w_idx", getattr(bc, f"v{a}_w_idx"))
+                f.write(f"vbc_{a}w_val", getattr(bc, f"v{a}_w_val"))
     finally:
         try:
             dev.snapshot_wait()
@@ -312,8 +329,9 @@ def materialpointsolver(args, grid, mp, attr, bc, workflow=None, device=0, verbo
     like the reference's ``workflow`` keyword."""
     if args.device != "B200":
         raise ValueError("this package provides the :B200 device backend (args.device = 'B200')")
-    if args.coupling != "OS" or args.scheme not in ("MUSL", "USL"):
-        raise NotImplementedError("the one-phase MUSL and USL schemes are provided")
+    if not ((args.coupling == "OS" and args.scheme in ("MUSL", "USL")) or
+            (args.coupling == "TS" and args.scheme == "MUSL")):
+        raise NotImplementedError("the one-phase MUSL and USL and the two-phase MUSL schemes are provided")
     if args.basis != "uGIMP":
         raise NotImplementedError("only the uGIMP basis is provided")
     dev = host2device(args, grid, mp, attr, bc, device)

@@ -341,6 +341,32 @@ class Particle:
         self.ps = _f(np.zeros((npart, D)), T2)
         self.vs = _f(np.zeros((npart, D)), T2)
 
+    def _init_water(self, n, rho_w):
+        """Two-phase fields (particle.jl:103-128): per particle when phase = 2,
+        single-entry placeholders otherwise."""
+        D, T1, T2, npart = self.dim, self.T1, self.T2, self.np
+        nv = 4 if D == 2 else 6
+        n = np.zeros(1) if n is None else np.asarray(n, np.float64).ravel()
+        rho_w = np.zeros(1) if rho_w is None else np.asarray(rho_w, np.float64).ravel()
+        k, dof = (npart, D) if self.phase == 2 else (1, 1)
+        if self.phase == 2:
+            if n.shape == (1,):
+                n = np.full(npart, n[0])
+            if rho_w.shape == (1,):
+                rho_w = np.full(npart, rho_w[0])
+            if n.shape != (npart,) or rho_w.shape != (npart,):
+                raise ValueError("n and ρw must have one entry per particle")
+        self.n = np.asarray(n, T2).copy()
+        self.rho_w = np.asarray(rho_w, T2).copy()
+        self.rho_w0 = self.rho_w.copy()
+        self.mw = np.zeros(k, T2)
+        self.mi = np.zeros(k, T2)
+        self.sigw = np.zeros(k, T2)
+        self.epsw = _f(np.zeros((k, nv)), T2)
+        self.depsw = _f(np.zeros((k, nv)), T2)
+        self.vw = _f(np.zeros((k, dof)), T2)
+        self.pw = _f(np.zeros((k, dof)), T2)
+
     def alloc_weights(self):
         """The reference's per-particle stencil tables (p2n, Nij, ∂N*); only the
         oracle fills them, the device recomputes weights instead of storing them."""
@@ -361,6 +387,7 @@ class Particle2D(Particle):
             raise ValueError("dx and dy should be positive")
         self.dx, self.dy = float(dx), float(dy)
         self._init(2, precision, NIC if NIC in (4, 9) else 9, (dx, dy), xi, rho, phase)
+        self._init_water(n, rho_w)
 
 
 class Particle3D(Particle):
@@ -372,6 +399,7 @@ class Particle3D(Particle):
             raise ValueError("dx, dy, and dz should be positive")
         self.dx, self.dy, self.dz = float(dx), float(dy), float(dz)
         self._init(3, precision, NIC if NIC in (8, 27) else 27, (dx, dy, dz), xi, rho, phase)
+        self._init_water(n, rho_w)
 
 
 def UserParticle2D(*, ϵ="FP64", **kw):
@@ -436,26 +464,40 @@ class VBoundary:
 class VBoundary2D(VBoundary):
     dim = 2
 
-    def __init__(self, *, precision="FP64", vx_s_idx, vx_s_val, vy_s_idx, vy_s_val, **_):
+    def __init__(self, *, precision="FP64", vx_s_idx, vx_s_val, vy_s_idx, vy_s_val, vx_w_idx=(0,),
+                 vx_w_val=(0,), vy_w_idx=(0,), vy_w_val=(0,), **_):
         T1, T2 = _types(precision)
-        if not (len(vx_s_idx) == len(vx_s_val) and len(vy_s_idx) == len(vy_s_val)):
-            raise ValueError("The length of vx_s_idx, vx_s_val, vy_s_idx, vy_s_val should be the same.")
+        if not (len(vx_s_idx) == len(vx_s_val) and len(vy_s_idx) == len(vy_s_val) and
+                len(vx_w_idx) == len(vx_w_val) and len(vy_w_idx) == len(vy_w_val)):
+            raise ValueError("The length of vx_s_idx, vx_s_val, vy_s_idx, vy_s_val, vx_w_idx, vx_w_val, "
+                             "vy_w_idx, vy_w_val should be the same.")
         self.vx_s_idx = np.asarray(vx_s_idx).astype(T1)
         self.vx_s_val = np.asarray(vx_s_val, T2)
         self.vy_s_idx = np.asarray(vy_s_idx).astype(T1)
         self.vy_s_val = np.asarray(vy_s_val, T2)
+        # water velocity BC (boundary.jl:54-68; [0] = none)
+        self.vx_w_idx = np.asarray(vx_w_idx).astype(T1)
+        self.vx_w_val = np.asarray(vx_w_val, T2)
+        self.vy_w_idx = np.asarray(vy_w_idx).astype(T1)
+        self.vy_w_val = np.asarray(vy_w_val, T2)
 
 
 class VBoundary3D(VBoundary):
     dim = 3
 
     def __init__(self, *, precision="FP64", vx_s_idx, vx_s_val, vy_s_idx, vy_s_val, vz_s_idx,
-                 vz_s_val, **_):
+                 vz_s_val, vx_w_idx=(0,), vx_w_val=(0,), vy_w_idx=(0,), vy_w_val=(0,), vz_w_idx=(0,),
+                 vz_w_val=(0,), **_):
         T1, T2 = _types(precision)
         if not (len(vx_s_idx) == len(vx_s_val) and len(vy_s_idx) == len(vy_s_val)
-                and len(vz_s_idx) == len(vz_s_val)):
+                and len(vz_s_idx) == len(vz_s_val) and len(vx_w_idx) == len(vx_w_val)
+                and len(vy_w_idx) == len(vy_w_val) and len(vz_w_idx) == len(vz_w_val)):
             raise ValueError("The length of vx_s_idx, vx_s_val, vy_s_idx, vy_s_val, vz_s_idx, "
-                             "vz_s_val should be the same.")
+                             "vz_s_val (and the water BC arrays) should be the same.")
+        water = {"x": (vx_w_idx, vx_w_val), "y": (vy_w_idx, vy_w_val), "z": (vz_w_idx, vz_w_val)}
+        for c, (idx, val) in water.items():
+            setattr(self, f"v{c}_w_idx", np.asarray(idx).astype(T1))
+            setattr(self, f"v{c}_w_val", np.asarray(val, T2))
         self.vx_s_idx = np.asarray(vx_s_idx).astype(T1)
         self.vx_s_val = np.asarray(vx_s_val, T2)
         self.vy_s_idx = np.asarray(vy_s_idx).astype(T1)

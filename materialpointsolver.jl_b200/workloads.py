@@ -360,3 +360,66 @@ def slope_runouts(case, xi):
     for s in case.meta["slopes"]:
         out.append(float(xi[s["start"]:s["end"], 0].max() - s["x0"] - s["toe0"]))
     return np.array(out)
+
+
+def saturated_column(*, dim=2, h=0.01, ppc=2, seed=1006, jitter=0.1, size=(0.1, 0.06, 0.2), box=None, pad=2,
+                     precision="FP64", constitutive="linearelastic", E=1.0e6, nu=0.3, rho_s=2650.0,
+                     rho_w=1000.0, n=0.3, Kw=2.2e7, k=1.0e-3, phi_deg=30.0, c=0.0, gravity=-9.81,
+                     Te=0.0, zeta_s=0.0, zeta_w=0.0, Ttol=0.05, cfl=0.2, gpu_precision="mixed",
+                     project_path="/tmp", **extra):
+    """Two-phase (coupling = :TS) saturated soil column of `size` (x, [y,] up)
+    in a box of `box` (default: the column's own footprint, i.e. a column
+    confined laterally; a wider box lets it collapse toward +x): porosity `n`,
+    solid and water densities, water bulk
+    modulus `Kw` and permeability `k` (the drag n·mw·g/k of P2G_TS!).  Walls
+    and floor are impermeable and free-slip for both phases (normal solid and
+    water velocities fixed to 0).  Δt = CFL·h / c with the undrained P-wave
+    speed c = sqrt((K + 4G/3 + Kw/n) / ((1 - n) ρs))."""
+    K, G = elastic_constants(E, nu)
+    dt = cfl * h / math.sqrt((K + 4.0 * G / 3.0 + Kw / n) / ((1.0 - n) * rho_s))
+    lp = h / ppc
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ext = size[:2] if dim == 2 else size
+    axes = [jl_range(lp / 2, lp, L - lp / 2) for L in (ext[0], ext[1]) + ((ext[2],) if dim == 3 else ())]
+    bx = tuple(box) if box is not None else tuple(ext)
+    pts = meshbuilder(*axes)
+    pts = pts + rng.uniform(-jitter * h, jitter * h, size=pts.shape)
+    npart = pts.shape[0]
+    akw = dict(Ttol=Ttol, Te=Te, ΔT=dt, FLIP=1, PIC=0, constitutive=constitutive, basis="uGIMP",
+               device="B200", coupling="TS", scheme="MUSL", va="a", gravity=gravity, ζs=zeta_s, ζw=zeta_w,
+               project_name=f"saturated{dim}d", project_path=project_path, ϵ=precision,
+               gpu_precision=gpu_precision, make_project_dir=False)
+    akw.update(extra)
+    mat = dict(ν=[nu], Es=[E], Gs=[G], Ks=[K], σt=[0.0], ϕ=[math.radians(phi_deg)], ϕr=[0.0], ψ=[0.0],
+               c=[c], cr=[0.0], Hp=[0.0], Kw=[Kw], k=[k])
+    attr = UserProperty(ϵ=precision, nid=np.ones(npart, np.int64), **mat)
+    eps = 1e-9 * h
+    if dim == 2:
+        args = UserArgs2D(**akw)
+        grid = UserGrid2D(ϵ=precision, x1=-pad * h, x2=bx[0] + pad * h, y1=-pad * h, y2=bx[1] + 3 * h,
+                          dx=h, dy=h, NIC=9, phase=2)
+        mp = UserParticle2D(ϵ=precision, NIC=9, dx=lp, dy=lp, ξ=pts, ρs=np.full(npart, rho_s), phase=2,
+                            n=np.full(npart, n), ρw=np.full(npart, rho_w))
+        gx, gy = grid.xi[:, 0], grid.xi[:, 1]
+        fx = ((gx <= eps) | (gx >= bx[0] - eps)).astype(np.int64)
+        fy = (gy <= eps).astype(np.int64)
+        z = np.zeros(grid.ni)
+        bc = UserVBoundary2D(ϵ=precision, vx_s_idx=fx, vx_s_val=z, vy_s_idx=fy, vy_s_val=z,
+                             vx_w_idx=fx, vx_w_val=z, vy_w_idx=fy, vy_w_val=z)
+    else:
+        args = UserArgs3D(**akw)
+        grid = UserGrid3D(ϵ=precision, x1=-pad * h, x2=bx[0] + pad * h, y1=-pad * h, y2=bx[1] + pad * h,
+                          z1=-pad * h, z2=bx[2] + 3 * h, dx=h, dy=h, dz=h, NIC=27, phase=2)
+        mp = UserParticle3D(ϵ=precision, NIC=27, dx=lp, dy=lp, dz=lp, ξ=pts, ρs=np.full(npart, rho_s),
+                            phase=2, n=np.full(npart, n), ρw=np.full(npart, rho_w))
+        gx, gy, gz = grid.xi[:, 0], grid.xi[:, 1], grid.xi[:, 2]
+        fx = ((gx <= eps) | (gx >= bx[0] - eps)).astype(np.int64)
+        fy = ((gy <= eps) | (gy >= bx[1] - eps)).astype(np.int64)
+        fz = (gz <= eps).astype(np.int64)
+        z = np.zeros(grid.ni)
+        bc = UserVBoundary3D(ϵ=precision, vx_s_idx=fx, vx_s_val=z, vy_s_idx=fy, vy_s_val=z, vz_s_idx=fz,
+                             vz_s_val=z, vx_w_idx=fx, vx_w_val=z, vy_w_idx=fy, vy_w_val=z, vz_w_idx=fz,
+                             vz_w_val=z)
+    nsteps = int(math.ceil(Ttol / dt))
+    return Case(f"saturated_column_{dim}d", args, grid, mp, attr, bc, dt, nsteps,
+                dict(np=npart, h=h, K=K, G=G, seed=seed, height=ext[-1], rho_w=rho_w, n=n))

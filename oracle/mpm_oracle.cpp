@@ -15,6 +15,7 @@
 // File:line citations are relative to the MaterialPointSolver.jl repository.
 #include "mpm_oracle.h"
 #include <cmath>
+#include <vector>
 #include <cstring>
 #include <cfloat>
 #include <algorithm>
@@ -148,6 +149,15 @@ void orc_resetgrid(orc_model *m) {
         if (i < m->nc) { m->g_sigm[i] = 0.0; m->g_omega[i] = 0.0; }
         m->g_ms[i] = 0.0;
         for (int d = 0; d < D; ++d) { m->g_ps[i + ni * d] = 0.0; m->g_fs[i + ni * d] = 0.0; }
+        if (m->coupling == 1) {   // resetgridstatus_TS!, utils_TS.jl:44-106
+            m->g_mi[i] = 0.0;
+            m->g_mw[i] = 0.0;
+            for (int d = 0; d < D; ++d) {
+                m->g_pw[i + ni * d] = 0.0;
+                m->g_fw[i + ni * d] = 0.0;
+                m->g_fd[i + ni * d] = 0.0;
+            }
+        }
     }
 }
 
@@ -506,6 +516,267 @@ void orc_g2p(orc_model *m, double dt) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Two-phase MUSL (procedure!(…, Val(:TS), Val(:MUSL)), src/solvers/TS_MUSL.jl:13-54,
+// kernels in src/solvers/utils_TS.jl).  The reference's own path does not run
+// as shipped; the restatement keeps its arithmetic and repairs three defects:
+//   * submit_work! calls workflow(…, Val(coupling), Val(scheme), Val(va))
+//     (src/solver.jl:84-85) but the :TS procedure! takes two Val arguments
+//     (TS_MUSL.jl:13-23): here the step is reached whatever va is;
+//   * G2P_TS! reads mp.ρs_init / mp.ρw_init (utils_TS.jl:849-850, 953-954), which
+//     Particle2D/3D do not have (src/types/particle.jl:60-62 define ρs0 / ρw0),
+//     and the 3D kernel writes mp.Δfs (utils_TS.jl:893-895) for ΔFs: the
+//     fields meant are used;
+//   * resetmpstatus_TS! evaluates the uGIMP basis on the first NIC entries of
+//     the 16 / 64 candidate nodes (utils_TS.jl:216-227, 266-283), which leaves
+//     support nodes out whenever the particle sits in the right part of its
+//     cell: the weights here are the one-phase CPU stencil (support-filtered,
+//     resetmpstatus_OS_CPU!, utils_OS.jl:235-277, 363-415).
+// Kept as written: grid.mi accumulates N·mw·n (utils_TS.jl:317, 366) while the
+// gravity on the mixture uses the particle's mi; iszero (not eps) guards the
+// nodal inverses; the 3D G2P_TS! adds the SOLID strain increment to ϵijw
+// (utils_TS.jl:929-934; the 2D kernel adds the water increment).
+// ---------------------------------------------------------------------------
+
+// resetmpstatus_TS! masses and momenta (utils_TS.jl:205-211, 252-261)
+void orc_resetmp_ts(orc_model *m) {
+    orc_resetmp(m);   // p2c, weights, ms = Ω·ρs
+    const int64_t np = m->np;
+    const int D = m->dim;
+#pragma omp parallel for if (par(m)) schedule(static)
+    for (int64_t ix = 0; ix < np; ++ix) {
+        const double n = m->n[ix], vol = m->Omega[ix];
+        m->ms[ix] = vol * m->rho[ix];
+        m->mw[ix] = vol * m->rhow[ix];
+        m->mi[ix] = vol * ((1.0 - n) * m->rho[ix] + n * m->rhow[ix]);
+        for (int d = 0; d < D; ++d) {
+            m->ps[ix + np * d] = m->ms[ix] * m->vs[ix + np * d] * (1.0 - n);
+            m->pw[ix + np * d] = m->mw[ix] * m->vw[ix + np * d] * n;
+        }
+    }
+}
+
+// P2G_TS!, utils_TS.jl:295-334 (2D) and :344-393 (3D)
+void orc_p2g_ts(orc_model *m, double G) {
+    const int64_t np = m->np, ni = m->ni, NIC = m->nic;
+    const int D = m->dim, nv = nv_of(D);
+    const bool at = par(m);
+#pragma omp parallel for if (at) schedule(static)
+    for (int64_t ix = 0; ix < np; ++ix) {
+        const double *sg = m->sig;
+        double s[6];
+        for (int k = 0; k < nv; ++k) s[k] = sg[ix + np * k];
+        const double n = m->n[ix], sw = m->sigw[ix], vol = m->Omega[ix];
+        const double tdg = (n * m->mw[ix] * G) / m->kperm[m->nid[ix] - 1];
+        for (int64_t q = 0; q < NIC; ++q) {
+            const double Ni = m->Nij[ix + np * q];
+            if (Ni == 0.0) continue;
+            const double dN[3] = {m->dNx[ix + np * q], m->dNy[ix + np * q], D == 3 ? m->dNz[ix + np * q] : 0.0};
+            const int64_t nd = m->p2n[ix + np * q] - 1;
+            atomic_add(&m->g_ms[nd], Ni * m->ms[ix] * (1.0 - n), at);
+            atomic_add(&m->g_mi[nd], Ni * m->mw[ix] * n, at);
+            atomic_add(&m->g_mw[nd], Ni * m->mw[ix], at);
+            for (int d = 0; d < D; ++d) {
+                atomic_add(&m->g_ps[nd + ni * d], Ni * m->ps[ix + np * d], at);
+                atomic_add(&m->g_pw[nd + ni * d], Ni * m->pw[ix + np * d], at);
+            }
+            // water force: −Ω ∂N σw (+ N mw G on the last axis)
+            for (int d = 0; d < D; ++d) {
+                double f = -vol * (dN[d] * sw);
+                if (d == D - 1) f += Ni * m->mw[ix] * G;
+                atomic_add(&m->g_fw[nd + ni * d], f, at);
+            }
+            // mixture force: −Ω (∂N (σ + σw I)) (+ N mi G on the last axis)
+            double fs[3];
+            if (D == 2) {
+                fs[0] = -vol * (dN[0] * (s[0] + sw) + dN[1] * s[3]);
+                fs[1] = -vol * (dN[1] * (s[1] + sw) + dN[0] * s[3]) + Ni * m->mi[ix] * G;
+            } else {
+                fs[0] = -vol * (dN[0] * (s[0] + sw) + dN[1] * s[3] + dN[2] * s[5]);
+                fs[1] = -vol * (dN[1] * (s[1] + sw) + dN[0] * s[3] + dN[2] * s[4]);
+                fs[2] = -vol * (dN[2] * (s[2] + sw) + dN[0] * s[5] + dN[1] * s[4]) + Ni * m->mi[ix] * G;
+            }
+            for (int d = 0; d < D; ++d) {
+                atomic_add(&m->g_fs[nd + ni * d], fs[d], at);
+                atomic_add(&m->g_fd[nd + ni * d], Ni * tdg * (m->vw[ix + np * d] - m->vs[ix + np * d]), at);
+            }
+        }
+    }
+}
+
+// solvegrid_TS!, utils_TS.jl:404-455 (2D) and :465-532 (3D)
+void orc_solvegrid_ts(orc_model *m, double dt) {
+    const int64_t ni = m->ni;
+    const int D = m->dim;
+    const int64_t *si[3] = {m->vx_idx, m->vy_idx, m->vz_idx}, *wi[3] = {m->vxw_idx, m->vyw_idx, m->vzw_idx};
+    const double *sv[3] = {m->vx_val, m->vy_val, m->vz_val}, *wv[3] = {m->vxw_val, m->vyw_val, m->vzw_val};
+#pragma omp parallel for if (par(m)) schedule(static)
+    for (int64_t i = 0; i < ni; ++i) {
+        const double msd = m->g_ms[i] == 0.0 ? 0.0 : 1.0 / m->g_ms[i];
+        const double mwd = m->g_mw[i] == 0.0 ? 0.0 : 1.0 / m->g_mw[i];
+        double vs[3], vw[3], fs[3], fw[3];
+        for (int d = 0; d < D; ++d) {
+            vs[d] = m->g_ps[i + ni * d] * msd;
+            vw[d] = m->g_pw[i + ni * d] * mwd;
+            fs[d] = m->g_fs[i + ni * d];
+            fw[d] = m->g_fw[i + ni * d];
+            m->g_vs[i + ni * d] = vs[d];
+            m->g_vw[i + ni * d] = vw[d];
+        }
+        double qw = 0.0, qs = 0.0;
+        for (int d = 0; d < D; ++d) {
+            qw += fw[d] * fw[d];
+            qs += (fs[d] - fw[d]) * (fs[d] - fw[d]);
+        }
+        const double tw = -m->zeta_w * std::sqrt(qw), ts_ = -m->zeta_s * std::sqrt(qs);
+        for (int d = 0; d < D; ++d) {
+            const double dw = tw * sgn(vw[d]), ds = ts_ * sgn(vs[d]);
+            const double aw = mwd * (fw[d] + dw + m->g_fd[i + ni * d]);
+            const double as = msd * (-m->g_mi[i] * aw + fs[d] + dw + ds);
+            m->g_aw[i + ni * d] = aw;
+            m->g_as[i + ni * d] = as;
+            m->g_vsT[i + ni * d] = vs[d] + as * dt;
+            m->g_vwT[i + ni * d] = vw[d] + aw * dt;
+        }
+        for (int d = 0; d < D; ++d) {
+            if (si[d][i] != 0) m->g_vsT[i + ni * d] = sv[d][i];
+            if (wi[d][i] != 0) m->g_vwT[i + ni * d] = wv[d][i];
+        }
+        for (int d = 0; d < D; ++d) {
+            m->g_ps[i + ni * d] = 0.0;
+            m->g_pw[i + ni * d] = 0.0;
+        }
+    }
+}
+
+// doublemapping1_TS!, utils_TS.jl:543-585 (2D) and :596-648 (3D)
+void orc_dm1_ts(orc_model *m, double dt) {
+    const int64_t np = m->np, ni = m->ni, NIC = m->nic;
+    const int D = m->dim;
+#pragma omp parallel for if (par(m)) schedule(static)
+    for (int64_t ix = 0; ix < np; ++ix) {
+        double pos[3] = {0, 0, 0}, s1[3] = {0, 0, 0}, s2[3] = {0, 0, 0}, w1[3] = {0, 0, 0}, w2[3] = {0, 0, 0};
+        for (int64_t q = 0; q < NIC; ++q) {
+            const double Ni = m->Nij[ix + np * q];
+            if (Ni == 0.0) continue;
+            const int64_t nd = m->p2n[ix + np * q] - 1;
+            for (int d = 0; d < D; ++d) {
+                const double vT = m->g_vsT[nd + ni * d], wT = m->g_vwT[nd + ni * d];
+                pos[d] += Ni * vT;
+                s1[d] += Ni * (vT - m->g_vs[nd + ni * d]);
+                s2[d] += Ni * vT;
+                w1[d] += Ni * (wT - m->g_vw[nd + ni * d]);
+                w2[d] += Ni * wT;
+            }
+        }
+        const double n = m->n[ix];
+        for (int d = 0; d < D; ++d) {
+            m->xi[ix + np * d] += dt * pos[d];
+            m->vs[ix + np * d] = m->FLIP * (m->vs[ix + np * d] + s1[d]) + m->PIC * s2[d];
+            m->vw[ix + np * d] = m->FLIP * (m->vw[ix + np * d] + w1[d]) + m->PIC * w2[d];
+            m->ps[ix + np * d] = m->ms[ix] * m->vs[ix + np * d] * (1.0 - n);
+            m->pw[ix + np * d] = m->mw[ix] * m->vw[ix + np * d] * n;
+        }
+    }
+}
+
+// doublemapping2_TS!, utils_TS.jl:657-704
+void orc_dm2_ts(orc_model *m) {
+    const int64_t np = m->np, ni = m->ni, NIC = m->nic;
+    const int D = m->dim;
+    const bool at = par(m);
+#pragma omp parallel for if (at) schedule(static)
+    for (int64_t ix = 0; ix < np; ++ix) {
+        for (int64_t q = 0; q < NIC; ++q) {
+            const double Ni = m->Nij[ix + np * q];
+            if (Ni == 0.0) continue;
+            const int64_t nd = m->p2n[ix + np * q] - 1;
+            for (int d = 0; d < D; ++d) {
+                atomic_add(&m->g_ps[nd + ni * d], m->ps[ix + np * d] * Ni, at);
+                atomic_add(&m->g_pw[nd + ni * d], m->pw[ix + np * d] * Ni, at);
+            }
+        }
+    }
+}
+
+// doublemapping3_TS!, utils_TS.jl:713-780
+void orc_dm3_ts(orc_model *m, double dt) {
+    const int64_t ni = m->ni;
+    const int D = m->dim;
+    const int64_t *si[3] = {m->vx_idx, m->vy_idx, m->vz_idx}, *wi[3] = {m->vxw_idx, m->vyw_idx, m->vzw_idx};
+    const double *sv[3] = {m->vx_val, m->vy_val, m->vz_val}, *wv[3] = {m->vxw_val, m->vyw_val, m->vzw_val};
+#pragma omp parallel for if (par(m)) schedule(static)
+    for (int64_t i = 0; i < ni; ++i) {
+        const double msd = m->g_ms[i] == 0.0 ? 0.0 : 1.0 / m->g_ms[i];
+        const double mwd = m->g_mw[i] == 0.0 ? 0.0 : 1.0 / m->g_mw[i];
+        for (int d = 0; d < D; ++d) {
+            double vs = m->g_ps[i + ni * d] * msd, vw = m->g_pw[i + ni * d] * mwd;
+            if (si[d][i] != 0) vs = sv[d][i];
+            if (wi[d][i] != 0) vw = wv[d][i];
+            m->g_vs[i + ni * d] = vs;
+            m->g_vw[i + ni * d] = vw;
+            m->g_dus[i + ni * d] = vs * dt;
+            m->g_duw[i + ni * d] = vw * dt;
+        }
+    }
+}
+
+// G2P_TS!, utils_TS.jl:790-857 (2D) and :867-961 (3D): the solid part is
+// G2P_OS!'s arithmetic (same expressions), then the water strain, the pore
+// pressure and the porosity.
+void orc_g2p_ts(orc_model *m, double dt) {
+    const int64_t np = m->np, ni = m->ni, NIC = m->nic;
+    const int D = m->dim, nv = nv_of(D);
+    std::vector<double> vol_old(m->Omega, m->Omega + np);
+    orc_g2p(m, dt);   // ΔFs, ϵv, Δϵijs, ϵijs, F, J, Ω, ρs = ρs0 / J
+#pragma omp parallel for if (par(m)) schedule(static)
+    for (int64_t ix = 0; ix < np; ++ix) {
+        double dw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int64_t q = 0; q < NIC; ++q) {
+            if (m->Nij[ix + np * q] == 0.0) continue;
+            const int64_t nd = m->p2n[ix + np * q] - 1;
+            const double dN[3] = {m->dNx[ix + np * q], m->dNy[ix + np * q], D == 3 ? m->dNz[ix + np * q] : 0.0};
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) dw[a * D + b] += m->g_duw[nd + ni * a] * dN[b];
+        }
+        const double *dF = m->dF;
+        double *ew = m->epsw, *dew = m->depsw;
+        double trs, trw;
+        if (D == 2) {
+            dew[ix] = dw[0]; dew[ix + np] = dw[3]; dew[ix + 3 * np] = dw[1] + dw[2];
+            ew[ix] += dw[0]; ew[ix + np] += dw[3]; ew[ix + 3 * np] += dw[1] + dw[2];
+            trs = dF[ix] + dF[ix + 3 * np];
+            trw = dw[0] + dw[3];
+        } else {
+            dew[ix] = dw[0]; dew[ix + np] = dw[4]; dew[ix + 2 * np] = dw[8];
+            dew[ix + 3 * np] = dw[1] + dw[3]; dew[ix + 4 * np] = dw[5] + dw[7]; dew[ix + 5 * np] = dw[2] + dw[6];
+            const double d0 = dF[ix], d1 = dF[ix + np], d2 = dF[ix + 2 * np], d3 = dF[ix + 3 * np],
+                         d4 = dF[ix + 4 * np], d5 = dF[ix + 5 * np], d6 = dF[ix + 6 * np],
+                         d7 = dF[ix + 7 * np], d8 = dF[ix + 8 * np];
+            ew[ix] += d0; ew[ix + np] += d4; ew[ix + 2 * np] += d8;   // solid increments, as written
+            ew[ix + 3 * np] += d1 + d3; ew[ix + 4 * np] += d5 + d7; ew[ix + 5 * np] += d2 + d6;
+            trs = d0 + d4 + d8;
+            trw = dw[0] + dw[4] + dw[8];
+        }
+        (void)nv;
+        double J;
+        const double *F = m->F;
+        if (D == 2) {
+            J = F[ix] * F[ix + 3 * np] - F[ix + np] * F[ix + 2 * np];
+        } else {
+            double g[9];
+            for (int k = 0; k < 9; ++k) g[k] = F[ix + np * k];
+            J = g[0] * g[4] * g[8] + g[1] * g[5] * g[6] + g[2] * g[3] * g[7] - g[6] * g[4] * g[2] -
+                g[7] * g[5] * g[0] - g[8] * g[3] * g[1];
+        }
+        const double dJ = J * m->Omega0[ix] / vol_old[ix];
+        m->rhow[ix] = m->rhow0[ix] / J;
+        const double n = m->n[ix];
+        m->sigw[ix] += (m->Kw[m->nid[ix] - 1] / n) * ((1.0 - n) * trs + n * trw);
+        m->n[ix] = 1.0 - (1.0 - n) / dJ;
+    }
+}
+
 }  // extern "C"
 
 namespace {
@@ -707,6 +978,17 @@ int orc_procedure(orc_model *m, double dt, double Ti) {
 #endif
     double G = Ti < m->Te ? m->gravity / m->Te * Ti : m->gravity;
     orc_resetgrid(m);
+    if (m->coupling == 1) {   // procedure!(…, Val(:TS), Val(:MUSL)), TS_MUSL.jl:24-53
+        orc_resetmp_ts(m);
+        orc_p2g_ts(m, G);
+        orc_solvegrid_ts(m, dt);
+        orc_dm1_ts(m, dt);
+        orc_dm2_ts(m);
+        orc_dm3_ts(m, dt);
+        orc_g2p_ts(m, dt);
+        orc_constitutive(m, Ti);
+        return 0;
+    }
     orc_resetmp(m);
     orc_p2g(m, G);
     if (m->scheme == 1) {   // USL, src/solvers/OS_USL.jl:102-145, 325-368

@@ -59,6 +59,18 @@ typedef struct {
     int32_t constitutive, va, mvl, mc3d;
     int32_t nthreads;           /* 0/1: sequential literal order; >1: OpenMP */
     int32_t scheme;             /* 0: MUSL (OS_MUSL.jl), 1: USL (OS_USL.jl) */
+    /* ---- two-phase coupling (:TS, src/solvers/TS_MUSL.jl, utils_TS.jl) ---- */
+    int32_t coupling;           /* 0: :OS, 1: :TS */
+    int32_t pad_ts;
+    double zeta_w;              /* ζw */
+    double *g_mi, *g_mw;        /* ni */
+    double *g_pw, *g_fw, *g_fd, *g_vw, *g_vwT, *g_aw, *g_duw; /* ni x dim */
+    double *mw, *mi, *n, *rhow, *rhow0, *sigw; /* np */
+    double *vw, *pw;            /* np x dim */
+    double *epsw, *depsw;       /* np x nv */
+    const double *Kw, *kperm;   /* per material: water bulk modulus, permeability k */
+    const int64_t *vxw_idx, *vyw_idx, *vzw_idx; /* ni: water velocity BC */
+    const double *vxw_val, *vyw_val, *vzw_val;
 } orc_model;
 
 /* One call of procedure!(…, Val(:OS), Val(:MUSL), Val(va)), src/solvers/OS_MUSL.jl:12-102 */
@@ -77,6 +89,14 @@ void orc_dm2(orc_model *m);
 void orc_dm3(orc_model *m, double dt);
 void orc_g2p(orc_model *m, double dt);
 void orc_constitutive(orc_model *m, double Ti);
+/* Two-phase stages (utils_TS.jl); orc_procedure runs them when coupling = 1. */
+void orc_resetmp_ts(orc_model *m);
+void orc_p2g_ts(orc_model *m, double G);
+void orc_solvegrid_ts(orc_model *m, double dt);
+void orc_dm1_ts(orc_model *m, double dt);
+void orc_dm2_ts(orc_model *m);
+void orc_dm3_ts(orc_model *m, double dt);
+void orc_g2p_ts(orc_model *m, double dt);
 
 /* Julia float fld/cld and the p2c formula (utils_OS.jl:247-249, 380-383). */
 double orc_fld(double a, double b);

@@ -53,6 +53,15 @@ class OrcModel(C.Structure):
         ("zeta_s", C.c_double),
         ("constitutive", C.c_int32), ("va", C.c_int32), ("mvl", C.c_int32), ("mc3d", C.c_int32),
         ("nthreads", C.c_int32), ("scheme", C.c_int32),
+        ("coupling", C.c_int32), ("pad_ts", C.c_int32), ("zeta_w", C.c_double),
+        ("g_mi", _dp), ("g_mw", _dp),
+        ("g_pw", _dp), ("g_fw", _dp), ("g_fd", _dp), ("g_vw", _dp), ("g_vwT", _dp), ("g_aw", _dp),
+        ("g_duw", _dp),
+        ("mw", _dp), ("mi", _dp), ("n", _dp), ("rhow", _dp), ("rhow0", _dp), ("sigw", _dp),
+        ("vw", _dp), ("pw", _dp), ("epsw", _dp), ("depsw", _dp),
+        ("Kw", _dp), ("kperm", _dp),
+        ("vxw_idx", _ip), ("vyw_idx", _ip), ("vzw_idx", _ip),
+        ("vxw_val", _dp), ("vyw_val", _dp), ("vzw_val", _dp),
     ]
 
 
@@ -100,6 +109,13 @@ def lib():
         L.orc_dm3.argtypes = [C.POINTER(OrcModel), C.c_double]
         L.orc_g2p.argtypes = [C.POINTER(OrcModel), C.c_double]
         L.orc_constitutive.argtypes = [C.POINTER(OrcModel), C.c_double]
+        L.orc_resetmp_ts.argtypes = [C.POINTER(OrcModel)]
+        L.orc_p2g_ts.argtypes = [C.POINTER(OrcModel), C.c_double]
+        L.orc_solvegrid_ts.argtypes = [C.POINTER(OrcModel), C.c_double]
+        L.orc_dm1_ts.argtypes = [C.POINTER(OrcModel), C.c_double]
+        L.orc_dm2_ts.argtypes = [C.POINTER(OrcModel)]
+        L.orc_dm3_ts.argtypes = [C.POINTER(OrcModel), C.c_double]
+        L.orc_g2p_ts.argtypes = [C.POINTER(OrcModel), C.c_double]
         _lib = L
     return _lib
 
@@ -156,6 +172,25 @@ class Oracle:
         keep["vx_val"] = _d(bc.vx_s_val)
         keep["vy_val"] = _d(bc.vy_s_val)
         keep["vz_val"] = _d(bc.vz_s_val) if D == 3 else zeros_d
+        ts = getattr(args, "coupling", "OS") == "TS"
+        if ts:
+            # two-phase state (particle.jl:103-128, grid.jl TS arrays, boundary.jl water BC)
+            keep["g_mi"], keep["g_mw"] = np.zeros(ni), np.zeros(ni)
+            for k in ("g_pw", "g_fw", "g_fd", "g_vw", "g_vwT", "g_aw", "g_duw"):
+                keep[k] = np.zeros((ni, D), order="F")
+            keep["mw"], keep["mi"] = np.zeros(npart), np.zeros(npart)
+            keep["n"], keep["rhow"], keep["rhow0"] = _d(mp.n), _d(mp.rho_w), _d(mp.rho_w0)
+            keep["sigw"] = _d(mp.sigw)
+            keep["vw"] = _d(mp.vw)
+            keep["pw"] = np.zeros((npart, D), order="F")
+            keep["epsw"], keep["depsw"] = _d(mp.epsw), _d(mp.depsw)
+            keep["Kw"] = _d(np.broadcast_to(attr.Kw, (len(attr.Es),)))
+            keep["kperm"] = _d(np.broadcast_to(attr.k, (len(attr.Es),)))
+            for c in "xyz":
+                idx = getattr(bc, f"v{c}_w_idx", None) if (c != "z" or D == 3) else None
+                full = idx is not None and len(idx) == ni
+                keep[f"v{c}w_idx"] = _i(idx) if full else zeros_i
+                keep[f"v{c}w_val"] = _d(getattr(bc, f"v{c}_w_val")) if full else zeros_d
         self.a = keep
         m = OrcModel()
         m.dim, m.nic = D, NIC
@@ -181,6 +216,8 @@ class Oracle:
         m.mc3d = 1 if getattr(args, "mc3d", "literal") == "restated" else 0
         m.nthreads = nthreads
         m.scheme = 1 if getattr(args, "scheme", "MUSL") == "USL" else 0
+        m.coupling = 1 if ts else 0
+        m.zeta_w = getattr(args, "zeta_w", 0.0)
         self.m = m
 
     def __getattr__(self, name):

@@ -11,8 +11,9 @@ def rel(a, b):
 
 def fresh_particles(pkg, mp):
     """An output particle struct shaped like `mp` for downloads."""
+    w = dict(phase=2, n=mp.n, rho_w=mp.rho_w) if getattr(mp, "phase", 1) == 2 else {}
     if mp.dim == 2:
-        out = pkg.Particle2D(precision=mp.precision, dx=mp.dx, dy=mp.dy, xi=mp.xi, rho=mp.rho)
+        out = pkg.Particle2D(precision=mp.precision, dx=mp.dx, dy=mp.dy, xi=mp.xi, rho=mp.rho, **w)
     else:
-        out = pkg.Particle3D(precision=mp.precision, dx=mp.dx, dy=mp.dy, dz=mp.dz, xi=mp.xi, rho=mp.rho)
+        out = pkg.Particle3D(precision=mp.precision, dx=mp.dx, dy=mp.dy, dz=mp.dz, xi=mp.xi, rho=mp.rho, **w)
     return out

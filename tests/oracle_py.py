@@ -406,3 +406,172 @@ class PyModel:
             self.step(dt, Ti)
             Ti += dt
         return Ti
+
+
+class PyModelTS(PyModel):
+    """Two-phase MUSL step (procedure!(…, Val(:TS), Val(:MUSL)), TS_MUSL.jl:24-53,
+    utils_TS.jl), transliterated with the same repairs as the C++ oracle:
+    ρs0 / ρw0 for the missing ρs_init / ρw_init (utils_TS.jl:849-850, 953-954),
+    ΔFs for Δfs (:893-895), and the one-phase support-filtered uGIMP stencil
+    instead of the first NIC candidates (:216-227, 266-283)."""
+
+    def __init__(self, args, grid, mp, attr, bc):
+        super().__init__(args, grid, mp, attr, bc)
+        D, ni, npart = self.D, self.ni, self.np
+        f = lambda a: np.array(a, np.float64)
+        self.n, self.rhow, self.rhow0, self.sigw = f(mp.n), f(mp.rho_w), f(mp.rho_w0), f(mp.sigw)
+        self.vw, self.epsw = f(mp.vw), f(mp.epsw)
+        self.pw = np.zeros((npart, D))
+        self.mw = np.zeros(npart)
+        self.mi = np.zeros(npart)
+        self.depsw = np.zeros_like(self.epsw)
+        nm = len(attr.Es)
+        self.Kw = np.broadcast_to(np.array(attr.Kw, np.float64), (nm,))
+        self.kp = np.broadcast_to(np.array(attr.k, np.float64), (nm,))
+        self.wbcidx, self.wbcval = [], []
+        for c in "xyz"[:D]:
+            idx = np.array(getattr(bc, f"v{c}_w_idx"), np.int64)
+            ok = len(idx) == ni
+            self.wbcidx.append(idx if ok else np.zeros(ni, np.int64))
+            self.wbcval.append(np.array(getattr(bc, f"v{c}_w_val"), np.float64) if ok else np.zeros(ni))
+        self.gmi, self.gmw = np.zeros(ni), np.zeros(ni)
+        self.gpw, self.gfw, self.gfd, self.gvw, self.gvwT, self.gaw, self.gduw = (
+            np.zeros((ni, D)) for _ in range(7))
+
+    def step(self, dt, Ti):
+        a, D = self.args, self.D
+        G = a.gravity / a.Te * Ti if Ti < a.Te else a.gravity
+        for arr in (self.gms, self.gps, self.gfs, self.gmi, self.gmw, self.gpw, self.gfw, self.gfd):
+            arr[:] = 0.0
+        # resetmpstatus_TS! (weights: the one-phase stencil)
+        self.resetmp()
+        for ix in range(self.np):
+            n, vol = self.n[ix], self.Omega[ix]
+            self.ms[ix] = vol * self.rho[ix]
+            self.mw[ix] = vol * self.rhow[ix]
+            self.mi[ix] = vol * ((1.0 - n) * self.rho[ix] + n * self.rhow[ix])
+            self.ps[ix] = self.ms[ix] * self.vs[ix] * (1.0 - n)
+            self.pw[ix] = self.mw[ix] * self.vw[ix] * n
+        # P2G_TS!, utils_TS.jl:295-393
+        for ix in range(self.np):
+            n, vol, sw, s = self.n[ix], self.Omega[ix], self.sigw[ix], self.sig[ix]
+            tdg = (n * self.mw[ix] * G) / self.kp[self.nid[ix] - 1]
+            for q in range(self.NIC):
+                Ni = self.Nij[ix, q]
+                if Ni == 0.0:
+                    continue
+                nd = self.p2n[ix, q] - 1
+                dN = [self.dN[k, ix, q] for k in range(D)]
+                self.gms[nd] += Ni * self.ms[ix] * (1.0 - n)
+                self.gmi[nd] += Ni * self.mw[ix] * n
+                self.gmw[nd] += Ni * self.mw[ix]
+                self.gps[nd] += Ni * self.ps[ix]
+                self.gpw[nd] += Ni * self.pw[ix]
+                for d in range(D):
+                    self.gfw[nd, d] += -vol * (dN[d] * sw) + (Ni * self.mw[ix] * G if d == D - 1 else 0.0)
+                if D == 2:
+                    self.gfs[nd, 0] += -vol * (dN[0] * (s[0] + sw) + dN[1] * s[3])
+                    self.gfs[nd, 1] += -vol * (dN[1] * (s[1] + sw) + dN[0] * s[3]) + Ni * self.mi[ix] * G
+                else:
+                    self.gfs[nd, 0] += -vol * (dN[0] * (s[0] + sw) + dN[1] * s[3] + dN[2] * s[5])
+                    self.gfs[nd, 1] += -vol * (dN[1] * (s[1] + sw) + dN[0] * s[3] + dN[2] * s[4])
+                    self.gfs[nd, 2] += (-vol * (dN[2] * (s[2] + sw) + dN[0] * s[5] + dN[1] * s[4]) +
+                                        Ni * self.mi[ix] * G)
+                self.gfd[nd] += Ni * tdg * (self.vw[ix] - self.vs[ix])
+        # solvegrid_TS!, utils_TS.jl:404-532
+        for i in range(self.ni):
+            msd = 0.0 if self.gms[i] == 0.0 else 1.0 / self.gms[i]
+            mwd = 0.0 if self.gmw[i] == 0.0 else 1.0 / self.gmw[i]
+            self.gvs[i] = self.gps[i] * msd
+            self.gvw[i] = self.gpw[i] * mwd
+            tw = -a.zeta_w * math.sqrt(float(np.sum(self.gfw[i] ** 2)))
+            tsd = -a.zeta_s * math.sqrt(float(np.sum((self.gfs[i] - self.gfw[i]) ** 2)))
+            for d in range(D):
+                dw, ds = tw * sign(self.gvw[i, d]), tsd * sign(self.gvs[i, d])
+                self.gaw[i, d] = mwd * (self.gfw[i, d] + dw + self.gfd[i, d])
+                self.gas[i, d] = msd * (-self.gmi[i] * self.gaw[i, d] + self.gfs[i, d] + dw + ds)
+                self.gvsT[i, d] = self.gvs[i, d] + self.gas[i, d] * dt
+                self.gvwT[i, d] = self.gvw[i, d] + self.gaw[i, d] * dt
+            for d in range(D):
+                if self.bcidx[d][i] != 0:
+                    self.gvsT[i, d] = self.bcval[d][i]
+                if self.wbcidx[d][i] != 0:
+                    self.gvwT[i, d] = self.wbcval[d][i]
+            self.gps[i] = 0.0
+            self.gpw[i] = 0.0
+        # doublemapping1_TS!, utils_TS.jl:543-648
+        for ix in range(self.np):
+            pos, s1, s2, w1, w2 = (np.zeros(D) for _ in range(5))
+            for q in range(self.NIC):
+                Ni = self.Nij[ix, q]
+                if Ni == 0.0:
+                    continue
+                nd = self.p2n[ix, q] - 1
+                pos += Ni * self.gvsT[nd]
+                s1 += Ni * (self.gvsT[nd] - self.gvs[nd])
+                s2 += Ni * self.gvsT[nd]
+                w1 += Ni * (self.gvwT[nd] - self.gvw[nd])
+                w2 += Ni * self.gvwT[nd]
+            n = self.n[ix]
+            self.xi[ix] += dt * pos
+            self.vs[ix] = a.FLIP * (self.vs[ix] + s1) + a.PIC * s2
+            self.vw[ix] = a.FLIP * (self.vw[ix] + w1) + a.PIC * w2
+            self.ps[ix] = self.ms[ix] * self.vs[ix] * (1.0 - n)
+            self.pw[ix] = self.mw[ix] * self.vw[ix] * n
+        # doublemapping2_TS!
+        for ix in range(self.np):
+            for q in range(self.NIC):
+                Ni = self.Nij[ix, q]
+                if Ni != 0.0:
+                    nd = self.p2n[ix, q] - 1
+                    self.gps[nd] += self.ps[ix] * Ni
+                    self.gpw[nd] += self.pw[ix] * Ni
+        # doublemapping3_TS!
+        for i in range(self.ni):
+            msd = 0.0 if self.gms[i] == 0.0 else 1.0 / self.gms[i]
+            mwd = 0.0 if self.gmw[i] == 0.0 else 1.0 / self.gmw[i]
+            self.gvs[i] = self.gps[i] * msd
+            self.gvw[i] = self.gpw[i] * mwd
+            for d in range(D):
+                if self.bcidx[d][i] != 0:
+                    self.gvs[i, d] = self.bcval[d][i]
+                if self.wbcidx[d][i] != 0:
+                    self.gvw[i, d] = self.wbcval[d][i]
+            self.gdus[i] = self.gvs[i] * dt
+            self.gduw[i] = self.gvw[i] * dt
+        # G2P_TS!: the solid part and the constitutive update are G2P_OS! + liE!/dpP!;
+        # the water part needs the pre-step volume
+        vol_old = self.Omega.copy()
+        self._g2p(dt, Ti)
+        for ix in range(self.np):
+            dw = np.zeros((D, D))
+            for q in range(self.NIC):
+                if self.Nij[ix, q] == 0.0:
+                    continue
+                nd = self.p2n[ix, q] - 1
+                for r in range(D):
+                    for c in range(D):
+                        dw[r, c] += self.gduw[nd, r] * self.dN[c, ix, q]
+            dF = self.dF[ix].reshape(D, D)
+            if D == 2:
+                dew = [dw[0, 0], dw[1, 1], 0.0, dw[0, 1] + dw[1, 0]]
+                self.depsw[ix, [0, 1, 3]] = [dew[0], dew[1], dew[3]]
+                self.epsw[ix, [0, 1, 3]] += [dew[0], dew[1], dew[3]]
+            else:
+                self.depsw[ix] = [dw[0, 0], dw[1, 1], dw[2, 2], dw[0, 1] + dw[1, 0], dw[1, 2] + dw[2, 1],
+                                  dw[0, 2] + dw[2, 0]]
+                # the solid increments, as utils_TS.jl:929-934 writes them
+                self.epsw[ix] += [dF[0, 0], dF[1, 1], dF[2, 2], dF[0, 1] + dF[1, 0], dF[1, 2] + dF[2, 1],
+                                  dF[0, 2] + dF[2, 0]]
+            Fv = self.F[ix]
+            if D == 2:
+                J = Fv[0] * Fv[3] - Fv[1] * Fv[2]
+            else:
+                J = (Fv[0] * Fv[4] * Fv[8] + Fv[1] * Fv[5] * Fv[6] + Fv[2] * Fv[3] * Fv[7] -
+                     Fv[6] * Fv[4] * Fv[2] - Fv[7] * Fv[5] * Fv[0] - Fv[8] * Fv[3] * Fv[1])
+            dJ = J * self.Omega0[ix] / vol_old[ix]
+            self.rhow[ix] = self.rhow0[ix] / J
+            n = self.n[ix]
+            trs, trw = float(np.trace(dF)), float(np.trace(dw))
+            self.sigw[ix] += (self.Kw[self.nid[ix] - 1] / n) * ((1.0 - n) * trs + n * trw)
+            self.n[ix] = 1.0 - (1.0 - n) / dJ

@@ -133,7 +133,7 @@ class _FakeDevice:
     def __init__(self, mp):
         self.mp, self.calls, self.steps = mp, [], 0
 
-    def snapshot(self, f, group, Ti, dtype=np.float64):
+    def snapshot(self, f, group, Ti, fields=None, dtype=np.float64):
         self.calls.append((group, self.steps, Ti))
         f.write(f"group{group}/coords", self.mp.xi)
         f.write(f"group{group}/time", np.asarray(Ti, dtype))

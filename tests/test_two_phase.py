@@ -1,0 +1,173 @@
+"""Two-phase MUSL (coupling = :TS, src/solvers/TS_MUSL.jl, utils_TS.jl).
+
+The reference's own two-phase path does not run as shipped (procedure!
+signature, missing ρs_init / ρw_init / Δfs fields, first-NIC stencil); the C++
+oracle and the Python transliteration restate it with the same three repairs.
+
+CPU: the oracle against the independent transliteration (2D and 3D, Drucker-
+Prager, gravity ramp, damping of both phases, FLIP/PIC); mass conservation of
+P2G_TS! (grid sums of the solid mass, Σ N·mw·n and the water mass); the
+descriptor and the host views of a two-phase model; entry-point validation.
+
+GPU: the sm_100a two-phase kernels through the C ABI against the oracle --
+FP64 device to 1e-9, mixed to 1e-4 (displacement, velocities, F, volume,
+porosity) and 1e-3 (stress, pore pressure, strains) -- including the pore
+pressure, the water velocity and the porosity; the same across many re-sorts
+and graph-replayed blocks; the two-phase snapshot groups."""
+import numpy as np
+import pytest
+
+from helpers import fresh_particles, rel
+from oracle_py import PyModelTS
+
+TOL64 = 1e-9
+TOL32 = 1e-4
+TOL32_STRESS = 1e-3
+
+
+def case2d(pkg, **kw):
+    base = dict(dim=2, h=0.01, size=(0.06, 0.08), box=(0.12, 0.1), constitutive="druckerprager", phi_deg=30.0,
+                Te=0.0, zeta_s=0.02, zeta_w=0.01, k=1e-2)
+    base.update(kw)
+    return pkg.workloads.saturated_column(**base)
+
+
+def case3d(pkg, **kw):
+    base = dict(dim=3, h=0.02, size=(0.08, 0.06, 0.1), box=(0.16, 0.06, 0.12), constitutive="druckerprager",
+                phi_deg=30.0, Te=0.0, zeta_s=0.02, zeta_w=0.01, k=1e-2)
+    base.update(kw)
+    return pkg.workloads.saturated_column(**base)
+
+
+FIELDS = ("xi", "vs", "vw", "sig", "sigw", "n", "epsw", "F", "Omega", "eps", "epsq")
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_matches_transliteration(pkg, orc, dim):
+    mk = case2d if dim == 2 else case3d
+    c = mk(pkg, Te=0.001, FLIP=0.9, PIC=0.1)
+    rng = np.random.default_rng(5)
+    c.mp.vs[:] = rng.uniform(-0.05, 0.05, c.mp.vs.shape)
+    c.mp.vw[:] = rng.uniform(-0.05, 0.05, c.mp.vw.shape)
+    o = orc.Oracle(c.args, c.grid, c.mp, c.attr, c.bc)
+    py = PyModelTS(c.args, c.grid, c.mp, c.attr, c.bc)
+    n = 12 if dim == 2 else 6
+    o.run(c.dt, 0.0, n)
+    py.run(c.dt, 0.0, n)
+    for k in FIELDS:
+        a, b = getattr(o, k), getattr(py, k)
+        if k == "xi":
+            a, b = a - c.mp.xi, b - c.mp.xi
+        assert rel(a, b) < 1e-12, (k, rel(a, b))
+    assert np.abs(o.sigw).max() > 0 and np.abs(o.vw - c.mp.vw).max() > 0
+
+
+def test_p2g_conserves_masses(pkg, orc):
+    c = case2d(pkg)
+    o = orc.Oracle(c.args, c.grid, c.mp, c.attr, c.bc)
+    o.stage("resetgrid")
+    o.stage("resetmp_ts")
+    o.stage("p2g_ts", -9.81)
+    n = c.mp.n.astype(np.float64)
+    ms = c.mp.Omega * c.mp.rho
+    mw = c.mp.Omega * c.mp.rho_w
+    assert np.isclose(o.g_ms.sum(), (ms * (1 - n)).sum(), rtol=1e-12)
+    assert np.isclose(o.g_mi.sum(), (mw * n).sum(), rtol=1e-12)
+    assert np.isclose(o.g_mw.sum(), mw.sum(), rtol=1e-12)
+    # the total gravity force on the mixture and on the water
+    mi = c.mp.Omega * ((1 - n) * c.mp.rho + n * c.mp.rho_w)
+    assert np.isclose(o.g_fs[:, 1].sum(), (mi * -9.81).sum(), rtol=1e-9)
+    assert np.isclose(o.g_fw[:, 1].sum(), (mw * -9.81).sum(), rtol=1e-9)
+
+
+def test_descriptor_and_views(pkg):
+    c = case3d(pkg)
+    d = pkg.solver.make_desc(c.args, c.grid, c.mp, c.attr)
+    assert d.coupling == pkg._lib.COUPLING_TS and d.zeta_w == c.args.zeta_w
+    hv = pkg.solver.host_views(c.grid, c.mp, c.attr, c.bc)
+    assert hv.n.ptr == c.mp.n.ctypes.data and hv.n.ld == c.mp.np
+    assert hv.vw.ld == c.mp.np and hv.epsw.ptr == c.mp.epsw.ctypes.data
+    assert hv.Kw.ptr == c.attr.Kw.ctypes.data and hv.kperm.ptr == c.attr.k.ctypes.data
+    assert hv.vzw_idx.ptr == c.bc.vz_w_idx.ctypes.data and hv.vzw_idx.ld == c.grid.ni
+    one = pkg.workloads.column_collapse_2d(h=0.02)
+    hv1 = pkg.solver.host_views(one.grid, one.mp, one.attr, one.bc)
+    assert not hv1.n.ptr and pkg.solver.make_desc(one.args, one.grid, one.mp, one.attr).coupling == 0
+
+
+def test_entry_point_accepts_two_phase_musl_only(pkg, tmp_path):
+    c = case2d(pkg, scheme="USL", project_path=str(tmp_path))
+    with pytest.raises(NotImplementedError, match="two-phase MUSL"):
+        pkg.materialpointsolver(c.args, c.grid, c.mp, c.attr, c.bc)
+
+
+# ---- GPU -------------------------------------------------------------------------
+
+def run_both(pkg, orc, c, nsteps, sort_every=None):
+    lib = pkg._lib
+    if sort_every:
+        c.args.sort_every = sort_every
+    dev = pkg.DeviceModel(c.args, c.grid, c.mp, c.attr, c.bc)
+    try:
+        dev.step(c.dt, 0.0, nsteps)
+        out = fresh_particles(pkg, c.mp)
+        dev.download(lib.F_REFERENCE_TS | lib.F_F | lib.F_RHOW, out)
+    finally:
+        dev.close()
+    o = orc.Oracle(c.args, c.grid, c.mp, c.attr, c.bc)
+    o.run(c.dt, 0.0, nsteps)
+    return out, o
+
+
+def check(out, o, mp0, tol):
+    ts = TOL32_STRESS if tol == TOL32 else tol
+    assert rel(out.xi - mp0.xi, o.xi - mp0.xi) < tol, ("displacement", rel(out.xi - mp0.xi, o.xi - mp0.xi))
+    for k, t in (("vs", tol), ("vw", tol), ("F", tol), ("Omega", tol), ("sig", ts), ("sigw", ts),
+                 ("eps", ts), ("epsw", ts)):
+        assert rel(getattr(out, k), getattr(o, k)) < t, (k, rel(getattr(out, k), getattr(o, k)))
+    assert rel(out.n - mp0.n, o.n - mp0.n) < ts, ("porosity change", rel(out.n - mp0.n, o.n - mp0.n))
+    assert rel(out.rho_w, o.rhow) < tol, ("ρw", rel(out.rho_w, o.rhow))
+    if np.abs(o.epsq).max() > 0:
+        assert rel(out.epsq, o.epsq) < ts * 10, ("epsq", rel(out.epsq, o.epsq))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+def test_device_matches_oracle(pkg, orc, gpu_lib, dim, prec, tol):
+    mk = case2d if dim == 2 else case3d
+    c = mk(pkg, gpu_precision=prec, Te=0.0005, PIC=0.05, FLIP=0.95)
+    out, o = run_both(pkg, orc, c, 60 if dim == 2 else 30)
+    check(out, o, c.mp, tol)
+    assert np.abs(o.sigw).max() > 10.0   # the pore pressure built up
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
+def test_device_resorts_and_graph_blocks(pkg, orc, gpu_lib, prec, tol):
+    """Re-sorting every 2 steps (the two-phase arrays travel with the
+    particles) and graph-replayed blocks over 96 steps."""
+    c = case2d(pkg, gpu_precision=prec)
+    out, o = run_both(pkg, orc, c, 96, sort_every=2)
+    check(out, o, c.mp, tol)
+
+
+@pytest.mark.gpu
+def test_two_phase_mohr_coulomb_3d_restated(pkg, orc, gpu_lib):
+    c = case3d(pkg, gpu_precision="fp64", constitutive="mohrcoulomb", mc3d="restated", c=2e3)
+    out, o = run_both(pkg, orc, c, 20)
+    check(out, o, c.mp, TOL64)
+
+
+@pytest.mark.gpu
+def test_two_phase_snapshots(pkg, gpu_lib, tmp_path):
+    c = case2d(pkg, hdf5=True, hdf5_step=10, Ttol=30 * 1e-5, project_path=str(tmp_path))
+    c.args.Ttol = 30 * c.dt
+    pkg.materialpointsolver(c.args, c.grid, c.mp, c.attr, c.bc)
+    t = pkg.hdf5.read(pkg.snapshot_path(c.args))
+    g = t["group2"]
+    assert {"pressure_w", "strain_w", "velocity_w", "porosity", "stress"} <= set(g)
+    assert g["velocity_w"].shape == (2, c.mp.np) and g["strain_w"].shape == (4, c.mp.np)
+    assert np.abs(g["pressure_w"]).max() > 0
+    assert "vbc_xw_idx" in t and "vbc_yw_val" in t
+    # the final state came back with the two-phase fields
+    assert np.abs(c.mp.sigw).max() > 0 and np.all((c.mp.n > 0) & (c.mp.n < 1))
