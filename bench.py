@@ -41,11 +41,13 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mc3d", default="literal", choices=["literal", "restated"])
-    ap.add_argument("--workload", default="column3d", choices=["column3d", "slope3d", "batch2d", "column2d"],
+    ap.add_argument("--workload", default="column3d",
+                    choices=["column3d", "slope3d", "batch2d", "column2d", "saturated3d"],
                     help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
                          "3D slope with a lognormal cohesion field; batch2d: 256 independent 2D slopes "
                          "(15.5 M particles) advanced together, autotuned during warm-up; column2d: the 3 200-"
-                         "particle 2D column in FP64 (launch-bound; CUDA graph replay)")
+                         "particle 2D column in FP64 (launch-bound; CUDA graph replay); saturated3d: the 2.56 M-particle column "
+                         "as a two-phase (solid + water) saturated soil, coupling TS")
     ap.add_argument("--surrogate", action="store_true",
                     help="slope3d: train the stress-return surrogate on samples logged from plain steps "
                          "(untimed) and time steps with it")
@@ -139,6 +141,8 @@ WORKLOADS = {
                 "constitutive": "druckerprager"},
     "column2d": {"workload": "2D granular column collapse (3 200 particles), uGIMP, MUSL va=:a, all FP64",
                  "constitutive": "druckerprager"},
+    "saturated3d": {"workload": "3D saturated soil column collapse, two-phase (coupling TS), uGIMP, MUSL",
+                    "constitutive": "druckerprager"},
 }
 
 
@@ -153,6 +157,9 @@ def make_case(mc3d, workload="column3d", surrogate=False):
         case = pkg.workloads.slope_batch_2d()
     elif workload == "column2d":
         case = pkg.workloads.column_collapse_2d(gpu_precision="fp64")
+    elif workload == "saturated3d":
+        case = pkg.workloads.saturated_column(dim=3, h=0.005, size=(0.5, 0.2, 0.4), box=(1.2, 0.4, 0.6),
+                                              constitutive="druckerprager", seed=1002)
     else:
         case = pkg.workloads.column_collapse_3d(mc3d=mc3d)
     return pkg, case
@@ -165,8 +172,10 @@ def pin_particles(mp):
         import torch
     except ImportError:
         return
-    for name in ("xi", "vs", "sig", "eps", "epsq", "epsk", "epsv", "Omega", "Omega0", "rho", "rho0", "F",
-                 "ms", "sigm"):
+    names = ["xi", "vs", "sig", "eps", "epsq", "epsk", "epsv", "Omega", "Omega0", "rho", "rho0", "F", "ms", "sigm"]
+    if getattr(mp, "phase", 1) == 2:
+        names += ["n", "rho_w", "sigw", "vw", "epsw", "mw"]
+    for name in names:
         a = getattr(mp, name)
         t = torch.empty(a.size, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
         b = t.numpy()
@@ -184,6 +193,13 @@ BP_STEP_3D = 212       # particle state read + written once per step
 BN_STEP_3D = 156       # compulsory grid traffic per active node per step
 BP_G2P_3D = 200        # fused G2P+stress+P2G kernel: its own particle bytes
 BN_G2P_3D = 40         # Δu read (3 floats) + m, p, f written (7 floats)
+# two-phase: the water phase's particle fields (n, σw, mw, vw, ϵijw read; n, σw,
+# vw, ϵijw written) and node records (Δus, Δuw, vsT read; ms, ps, fs, mi, mw,
+# pw, fw, fd written in the fused pass; all the water records in the step)
+BP_STEP_TS = 304
+BN_STEP_TS = 344
+BP_G2P_TS = 280
+BN_G2P_TS = 108
 BP_STEP_2D = 132
 BN_STEP_2D = 108
 BP_G2P_2D = 128
@@ -206,17 +222,20 @@ def run_b200(args):
 
     # ---- end to end through the public API: host arrays -> device -> host ----
     pin_particles(case.mp)
+    ts = getattr(case.mp, "phase", 1) == 2
+    wkw = dict(phase=2, n=case.mp.n, rho_w=case.mp.rho_w) if ts else {}
     if case.grid.dim == 3:
-        out = pkg.Particle3D(dx=case.mp.dx, dy=case.mp.dy, dz=case.mp.dz, xi=case.mp.xi, rho=case.mp.rho)
+        out = pkg.Particle3D(dx=case.mp.dx, dy=case.mp.dy, dz=case.mp.dz, xi=case.mp.xi, rho=case.mp.rho, **wkw)
     else:
-        out = pkg.Particle2D(dx=case.mp.dx, dy=case.mp.dy, xi=case.mp.xi, rho=case.mp.rho)
+        out = pkg.Particle2D(dx=case.mp.dx, dy=case.mp.dy, xi=case.mp.xi, rho=case.mp.rho, **wkw)
     pin_particles(out)
+    ref_mask = lib.F_REFERENCE_TS if ts else lib.F_REFERENCE
 
     def e2e_once(nsteps):
         t0 = time.perf_counter()
         dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
         dev.step(dt, 0.0, nsteps)
-        dev.download(lib.F_REFERENCE, out)
+        dev.download(ref_mask, out)
         t1 = time.perf_counter()
         dev.close()
         return t1 - t0
@@ -229,6 +248,9 @@ def run_b200(args):
     h2d = npart * 8 * (D + D + nv + nv + 3 + 4 + D * D) + npart * 8
     # device2host! field set (FP64: sigm, vs, xi, Omega, sig, epsk, epsq, epsv, eps, ms)
     d2h = npart * 8 * (1 + D + D + 1 + nv + 1 + 1 + 1 + nv + 1)
+    if ts:   # + n, ρw, σw, vw, ϵijw up; mw, vw, σw, ϵijw, n down
+        h2d += npart * 8 * (3 + D + nv)
+        d2h += npart * 8 * (3 + D + nv)
 
     # ---- device-timed region (inputs resident in HBM) ----
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
@@ -300,6 +322,8 @@ def run_b200(args):
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     bp_g2p, bn_g2p = (BP_G2P_3D, BN_G2P_3D) if D == 3 else (BP_G2P_2D, BN_G2P_2D)
     bp_step, bn_step = (BP_STEP_3D, BN_STEP_3D) if D == 3 else (BP_STEP_2D, BN_STEP_2D)
+    if args.workload == "saturated3d":
+        bp_g2p, bn_g2p, bp_step, bn_step = BP_G2P_TS, BN_G2P_TS, BP_STEP_TS, BN_STEP_TS
     alg_bytes = npart * bp_g2p + na * bn_g2p
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
     step_bytes = npart * bp_step + na * bn_step
