@@ -149,8 +149,14 @@ __device__ __forceinline__ MarkState mark_begin(const GDev<R> &g, const AxisW<R>
     if (total <= 64) {
         const int lane = threadIdx.x & 31;
         const int rank = __popc(mask & ((1u << lane) - 1u)), cnt = __popc(mask);
+        // decode k -> (by, bx, bz) without integer division: for k < 64 and box
+        // sides <= 64, (k + 1/2)·(1/n) is at least 1/128 away from an integer,
+        // far beyond the error of the approximate reciprocal
+        const float rny = __fdividef(1.0f, (float)ny), rnx = __fdividef(1.0f, (float)nx);
         for (int k = rank; k < total; k += cnt) {
-            int by = blo[1] + k % ny, r = k / ny, bx = blo[0] + r % nx, bz = blo[2] + r / nx;
+            const int r = __float2int_rz(((float)k + 0.5f) * rny);
+            const int q = __float2int_rz(((float)r + 0.5f) * rnx);
+            const int by = blo[1] + (k - r * ny), bx = blo[0] + (r - q * nx), bz = blo[2] + q;
             const int b = (bz * g.nbx + bx) * g.nby + by;
             if (st.n < 2) {
                 st.b[st.n] = b;
