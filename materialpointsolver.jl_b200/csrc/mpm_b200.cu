@@ -20,6 +20,7 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 using namespace mpm;
@@ -112,6 +113,7 @@ struct mpm_handle {
     bool use_graphs = true;  // replay captured step blocks (MPM_B200_GRAPHS=0 turns it off)
     bool prefetch = true;    // FP32 particle pass stages fields by cp.async (MPM_B200_PREFETCH=0 turns it off)
     bool cell_major = false; // order inside a tile: rank-major (default) or cell-major (MPM_B200_ORDER=cell)
+    bool chain = true;       // FP32 scatters merge chained warp lanes (MPM_B200_CHAIN=0 turns it off)
     GraphCache graph;
     int64_t graph_launches = 0;
     // stress-return surrogate: 1 = log samples into caller buffers, 2 = infer
@@ -624,6 +626,13 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
             L.run("mvl_p2g", [&] { k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
         } else {
             L.run("g2p_p2g", [&] {
+                if constexpr (std::is_same<R, float>::value) {
+                    if (h->chain) {
+                        if (mc3) k_g2p_chain<D, D == 3, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                        else k_g2p_chain<D, false, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                        return;
+                    }
+                }
                 if (mc3) k_g2p<D, R, true, D == 3, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
                 else k_g2p<D, R, true, false, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
             });
@@ -660,10 +669,26 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         }
         L.run("p2g", [&] { k_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
     } else {
-        if (np) L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        const bool chain = h->chain && std::is_same<R, float>::value;
+        if (np) L.run("dmap", [&] {
+            if constexpr (std::is_same<R, float>::value) {
+                if (chain) {
+                    k_dmap_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    return;
+                }
+            }
+            k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+        });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         if (np) L.run("g2p_p2g", [&] {
+            if constexpr (std::is_same<R, float>::value) {
+                if (chain) {
+                    if (mc3) k_g2p_chain<D, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    else k_g2p_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    return;
+                }
+            }
             if (mc3) k_g2p<D, R, true, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
             else k_g2p<D, R, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
         });
@@ -1400,6 +1425,7 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         if (const char *e = getenv("MPM_B200_GRAPHS")) h->use_graphs = (e[0] != '0');
         if (const char *e = getenv("MPM_B200_PREFETCH")) h->prefetch = (e[0] != '0');
         if (const char *e = getenv("MPM_B200_ORDER")) h->cell_major = (std::string(e) == "cell");
+        if (const char *e = getenv("MPM_B200_CHAIN")) h->chain = std::atoi(e) != 0;
         *out = h;
         return MPM_OK;
     } catch (const Err &e) {

@@ -25,6 +25,8 @@
 #include "mpm_device.cuh"
 #include "mpm_mc3d.cuh"
 
+#include <climits>
+
 // resident CTAs of 256 threads per SM the particle passes are register-capped for
 #ifndef MPM_P_MINB
 #define MPM_P_MINB 4
@@ -452,15 +454,161 @@ __global__ void __launch_bounds__(128) k_solve(GDev<R> g, StepParams sp) {
 }
 
 // ---------------------------------------------------------------------------
+// Warp-level merging of the scatters (FP32).  After the cell sort the lanes of
+// a warp hold the particles of equal rank in consecutive cells of a tile, y
+// fastest, so lane L's window usually starts one node above lane L-1's in y
+// with the same x and z (a "chain" of up to 8 lanes).  Then the node at
+// window row b = 0 of lane L is also row 1 of lane L-1 and row 2 of lane L-2:
+// lane L adds those two contributions (shuffled up) to its own and reduces
+// the sum into global memory once, and only the last lane of a chain also
+// reduces rows 1 and 2.  A chain of 8 lanes issues 10 node reductions per
+// (x, z) window column instead of 24.  Lanes that are not chained (any other
+// window offset, dead or out-of-grid lanes) simply emit all three rows.  All
+// 32 lanes of the warp must call these functions.
+// ---------------------------------------------------------------------------
+// chain key of a lane without a particle: never one more than another key
+__device__ __forceinline__ int dead_key() { return -(1 << 30) - 4 * (int)(threadIdx.x & 31); }
+
+struct Chain {
+    bool c1;    // lane L-1's window is this window shifted by -1 in y
+    bool c2;    // ... and lane L-2's by -2
+    bool end;   // lane L+1 does not continue the chain
+};
+
+__device__ __forceinline__ Chain chain_of(int n0) {
+    const int lane = threadIdx.x & 31;
+    const int p1 = __shfl_up_sync(0xffffffffu, n0, 1), p2 = __shfl_up_sync(0xffffffffu, n0, 2);
+    const int q1 = __shfl_down_sync(0xffffffffu, n0, 1);
+    Chain c;
+    c.c1 = lane >= 1 && p1 == n0 - 1;
+    c.c2 = c.c1 && lane >= 2 && p2 == n0 - 2;
+    c.end = !(lane <= 30 && q1 == n0 + 1);
+    return c;
+}
+
+// doublemapping2 (momentum N·p) with chained lanes merged; n0 = window corner,
+// key = n0 for a live lane, a value no other lane's key follows for a dead one
+template <int D>
+__device__ __forceinline__ void dm2_scatter_chain(const GDev<float> &g, const AxisW<float> *w, int n0, int key,
+                                                  const float *p) {
+    const Chain ch = chain_of(key);
+    const unsigned F = 0xffffffffu;
+    float p1[3], p2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        p1[k] = __shfl_up_sync(F, p[k], 1);
+        p2[k] = __shfl_up_sync(F, p[k], 2);
+    }
+    const int plane = g.nnx * g.nny;
+    constexpr int NC = D == 3 ? 3 : 1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const float wz = D == 3 ? w[2].N[c] : 1.0f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float wxz = w[0].N[a] * wz;
+            const float N0 = wxz * w[1].N[0], N1 = wxz * w[1].N[1], N2 = wxz * w[1].N[2];
+            const float u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2), v2 = __shfl_up_sync(F, N2, 1);
+            const float a1 = ch.c1 ? u1 : 0.0f, a2 = ch.c2 ? u2 : 0.0f, b2 = ch.c1 ? v2 : 0.0f;
+            Node8<float> *col = g.acc + (n0 + a * g.nny + c * plane);
+            if (N0 + a1 + a2 != 0.0f)
+                red_add4(&col[0].a, 0.0f, N0 * p[0] + a1 * p1[0] + a2 * p2[0], N0 * p[1] + a1 * p1[1] + a2 * p2[1],
+                         N0 * p[2] + a1 * p1[2] + a2 * p2[2]);
+            if (ch.end) {
+                if (N1 + b2 != 0.0f)
+                    red_add4(&col[1].a, 0.0f, N1 * p[0] + b2 * p1[0], N1 * p[1] + b2 * p1[1], N1 * p[2] + b2 * p1[2]);
+                if (N2 != 0.0f) red_add4(&col[2].a, 0.0f, N2 * p[0], N2 * p[1], N2 * p[2]);
+            }
+        }
+    }
+}
+
+// P2G_OS! of one particle with chained lanes merged (the arithmetic of
+// p2g_scatter; 7 components per node: m, p, f)
+template <int D>
+__device__ __forceinline__ void p2g_scatter_chain(const GDev<float> &g, const AxisW<float> *w, int n0, int key,
+                                                  float m, float vol, const float *v, const float *s, float G) {
+    const Chain ch = chain_of(key);
+    const unsigned F = 0xffffffffu;
+    const float p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : 0.0f};
+    const int plane = g.nnx * g.nny;
+    constexpr int NC = D == 3 ? 3 : 1;
+    float sv[6];
+    if (D == 2) {
+        sv[0] = -vol * s[0]; sv[1] = -vol * s[1]; sv[3] = -vol * s[3];
+        sv[2] = sv[4] = sv[5] = 0.0f;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sv[k] = -vol * s[k];
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const float wz = D == 3 ? w[2].N[c] : 1.0f, gz = D == 3 ? w[2].dN[c] : 0.0f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float wx = w[0].N[a];
+            const float wxz = wx * wz, gxz = w[0].dN[a] * wz, xdz = wx * gz;
+            // per column: node value = Ny·(M, P, X) + dNy·(0, 0, Y)
+            float U[7], Y[3];
+            U[0] = m * wxz;
+            U[1] = p[0] * wxz; U[2] = p[1] * wxz; U[3] = p[2] * wxz;
+            if (D == 2) {
+                U[4] = sv[0] * gxz; U[5] = sv[3] * gxz + U[0] * G; U[6] = 0.0f;
+                Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = 0.0f;
+            } else {
+                U[4] = sv[0] * gxz + sv[5] * xdz;
+                U[5] = sv[3] * gxz + sv[4] * xdz;
+                U[6] = sv[5] * gxz + sv[2] * xdz + U[0] * G;
+                Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = sv[4] * wxz;
+            }
+            float r0[7], r1[7], r2[7];   // this lane's rows b = 0, 1, 2
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const float wy = w[1].N[b], gy = w[1].dN[b];
+                float *r = b == 0 ? r0 : (b == 1 ? r1 : r2);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) r[k] = wy * U[k];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) r[4 + k] = wy * U[4 + k] + gy * Y[k];
+            }
+            // row 0 += lane L-1's row 1 + lane L-2's row 2; chain ends: row 1 += lane L-1's row 2
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                const float x1 = __shfl_up_sync(F, r1[k], 1), x2 = __shfl_up_sync(F, r2[k], 2);
+                const float y2 = __shfl_up_sync(F, r2[k], 1);
+                r0[k] += (ch.c1 ? x1 : 0.0f) + (ch.c2 ? x2 : 0.0f);
+                r1[k] += ch.c1 ? y2 : 0.0f;
+            }
+            Node8<float> *col = g.acc + (n0 + a * g.nny + c * plane);
+            if (r0[0] != 0.0f) {
+                red_add4(&col[0].a, r0[0], r0[1], r0[2], r0[3]);
+                red_add4(&col[0].b, r0[4], r0[5], r0[6], 0.0f);
+            }
+            if (ch.end) {
+                if (r1[0] != 0.0f) {
+                    red_add4(&col[1].a, r1[0], r1[1], r1[2], r1[3]);
+                    red_add4(&col[1].b, r1[4], r1[5], r1[6], 0.0f);
+                }
+                if (r2[0] != 0.0f) {
+                    red_add4(&col[2].a, r2[0], r2[1], r2[2], r2[3]);
+                    red_add4(&col[2].b, r2[4], r2[5], r2[6], 0.0f);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Double mapping: doublemapping1_a_OS! / doublemapping1_OS! (new particle
 // velocity from the grid) fused with doublemapping2_OS! (re-scatter of the
 // particle momentum with the same weights).  The position update of DM1 is
 // carried out by k_g2p, which gathers the same ΣN·vsT with the same weights.
 // ---------------------------------------------------------------------------
+// doublemapping1 of one particle: gathers, new velocity (stored), momentum p
+// for the re-scatter; w receives the particle's window.
 template <int D, typename R>
-__global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<R> g, StepParams sp) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= sp.np) return;
+__device__ __forceinline__ void dmap_core(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp, int64_t i,
+                                          AxisW<R> *w, R *p) {
     using T4 = typename Vec<R>::T4;
     double x[3];
     load_x<D, R>(P, i, x);
@@ -468,7 +616,6 @@ __global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<
 #pragma unroll
     for (int d = 0; d < D; ++d) vo[d] = ldcs(P.v[d] + i);
     const R m = ldcs(P.m + i);
-    AxisW<R> w[3];
     particle_weights<D, R>(x, g, w);   // out-of-grid particles get zero weights
     const int n0 = window_n0<D, R>(g, w);
     const int plane = g.nnx * g.nny;
@@ -518,7 +665,15 @@ __global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<
         else vn[d] = FLIP * (vo[d] + (tT[d] - tv[d])) + PIC * tT[d];
         stcs(P.v[d] + i, vn[d]);
     }
-    const R p[3] = {m * vn[0], m * vn[1], D == 3 ? m * vn[2] : R(0)};
+    p[0] = m * vn[0]; p[1] = m * vn[1]; p[2] = D == 3 ? m * vn[2] : R(0);
+}
+
+// doublemapping2 of one particle: p·N into the momentum of the window nodes
+template <int D, typename R>
+__device__ __forceinline__ void dm2_scatter(const GDev<R> &g, const AxisW<R> *w, const R *p) {
+    const int n0 = window_n0<D, R>(g, w);
+    const int plane = g.nnx * g.nny;
+    constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         const R wz = D == 3 ? w[2].N[c] : R(1);
@@ -537,6 +692,38 @@ __global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<
             }
         }
     }
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    AxisW<R> w[3];
+    R p[3];
+    dmap_core<D, R>(P, g, sp, i, w, p);
+    dm2_scatter<D, R>(g, w, p);
+}
+
+// The same pass (FP32) with the re-scatter of chained lanes merged.
+template <int D>
+__global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < sp.np;
+    AxisW<float> w[3];
+    float p[3] = {0, 0, 0};
+    int n0 = 0, key = dead_key();
+    if (live) {
+        dmap_core<D, float>(P, g, sp, i, w, p);
+        n0 = key = window_n0<D, float>(g, w);
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            w[a].base = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+        }
+    }
+    dm2_scatter_chain<D>(g, w, n0, key, p);
 }
 
 // doublemapping3_OS!, utils_OS.jl:968-1016: grid velocity from the re-mapped
@@ -785,24 +972,13 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
     if (nan) atomicOr(g.err, ERR_NAN);
 }
 
-// ---------------------------------------------------------------------------
-// G2P_OS! (utils_OS.jl:1025-1153) + the position update of DM1 + liE! +
-// dpP!/mcP!.  With FUSE, the next step's P2G scatters the updated particle
-// (resetmpstatus_OS! + P2G_OS! at the new position, gravity sp.G).
-// ---------------------------------------------------------------------------
-template <int D, typename R, bool FUSE, bool MC3 = false, bool USL = false>
-__global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g, StepParams sp) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= sp.np) return;
-    extern __shared__ float g2p_pre[];   // PF_N slots x 256 threads when sp.prefetch
-    float *pre = nullptr;
-    if (sizeof(R) == 4 && sp.prefetch) {
-        pre = g2p_pre + threadIdx.x;
-        prefetch_particle<D, R>(pre, P, i);
-    }
-    double x[3];
+// The per-particle body of the G2P pass: gathers, DM1 velocity (USL), the
+// update (update_particle) and, without FUSE, the MVL cell sums.  Returns the
+// updated position x, stress s and volume vol for the next scatter.
+template <int D, typename R, bool FUSE, bool MC3, bool USL>
+__device__ __forceinline__ void g2p_core(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp, int64_t i,
+                                         float *pre, double *x, AxisW<R> *w, R *s, R &vol) {
     load_x<D, R>(P, i, x);
-    AxisW<R> w[3];
     particle_weights<D, R>(x, g, w);
     const int n0 = window_n0<D, R>(g, w);
     const int plane = g.nnx * g.nny;
@@ -885,7 +1061,6 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
             if (pre) pre[(PF_V + d) * PF_T] = (float)vn;
         }
     }
-    R s[6], vol;
     int cell = 0;
     if (!FUSE && sp.mvl) {
         // vollock1_OS!: the cell of the step's start (the reference's p2c)
@@ -903,6 +1078,27 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
         atomicAdd(&g.comega[cell], vol);
         g.pcell[i] = (uint32_t)cell;
     }
+}
+
+// ---------------------------------------------------------------------------
+// G2P_OS! (utils_OS.jl:1025-1153) + the position update of DM1 + liE! +
+// dpP!/mcP!.  With FUSE, the next step's P2G scatters the updated particle
+// (resetmpstatus_OS! + P2G_OS! at the new position, gravity sp.G).
+// ---------------------------------------------------------------------------
+template <int D, typename R, bool FUSE, bool MC3 = false, bool USL = false>
+__global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    extern __shared__ float g2p_pre[];   // PF_N slots x 256 threads when sp.prefetch
+    float *pre = nullptr;
+    if (sizeof(R) == 4 && sp.prefetch) {
+        pre = g2p_pre + threadIdx.x;
+        prefetch_particle<D, R>(pre, P, i);
+    }
+    double x[3];
+    AxisW<R> w[3];
+    R s[6], vol;
+    g2p_core<D, R, FUSE, MC3, USL>(P, g, sp, i, pre, x, w, s, vol);
     if (FUSE) {
         if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); return; }
         R v[3];
@@ -911,6 +1107,43 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
         if (D == 2) v[2] = R(0);
         p2g_scatter<D, R>(g, w, pf(pre, PF_M, P.m + i), vol, v, s, (R)sp.G);
     }
+}
+
+// The same pass (FP32, FUSE) with the scatter of chained lanes merged.
+template <int D, bool MC3 = false, bool USL = false>
+__global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool live = i < sp.np;
+    double x[3];
+    AxisW<float> w[3];
+    float s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, v[3] = {0, 0, 0}, m = 0;
+    if (live) {
+        g2p_core<D, float, true, MC3, USL>(P, g, sp, i, nullptr, x, w, s, vol);
+        if (!particle_weights<D, float>(x, g, w)) {
+            atomicOr(g.err, ERR_OOG);
+            live = false;
+        } else {
+#pragma unroll
+            for (int d = 0; d < D; ++d) v[d] = P.v[d][i];
+            m = P.m[i];
+        }
+    }
+    int n0 = 0, key = dead_key();
+    if (live) {
+        n0 = key = window_n0<D, float>(g, w);
+    } else {
+        m = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            w[a].base = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+        }
+    }
+    MarkState mk;
+    if (live) mk = mark_begin<D, float>(g, w);
+    p2g_scatter_chain<D>(g, w, n0, key, m, vol, v, s, (float)sp.G);
+    if (live) mark_end<float>(g, mk);
 }
 
 // vollock2_OS! + the next step's P2G: the particle's mean stress is replaced by
