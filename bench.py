@@ -186,7 +186,7 @@ def pin_particles(mp):
         setattr(mp, name, b)
 
 
-G2P_TRAFFIC_PER_PARTICLE = 242.9   # B, dram__bytes_read.sum + dram__bytes_write.sum / np
+G2P_TRAFFIC_PER_PARTICLE = 244.5   # B, dram__bytes_read.sum + dram__bytes_write.sum / np
 
 # algorithmic bytes per particle / per active node
 BP_STEP_3D = 212       # particle state read + written once per step
@@ -328,8 +328,8 @@ def run_b200(args):
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
     step_bytes = npart * bp_step + na * bn_step
     step_achieved = step_bytes / (ms * 1e-3 / K) / 1e9
-    # DRAM bytes (read + write) per launch of the fused kernel from one ncu
-    # capture of this workload (profiles/k_g2p_column3d_2.56M.md), per particle
+    # DRAM bytes (read + write) per launch of the fused kernel, from one ncu
+    # capture of this workload (--set full on k_g2p_chain), per particle
     traffic = G2P_TRAFFIC_PER_PARTICLE * npart if args.workload == "column3d" else None
 
     result = {
