@@ -387,6 +387,34 @@ def test_graph_replay_matches_direct_launches(pkg, orc, gpu_lib, dim, monkeypatc
     check_fields(outs[0], o, case.mp, TOL64)
 
 
+@pytest.mark.parametrize("scheme", ["MUSL", "USL"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_lane_merged_scatter_matches_plain(pkg, orc, gpu_lib, dim, scheme, monkeypatch):
+    """The FP32 particle passes merge the scatters of warp lanes whose windows
+    are consecutive in y (k_g2p_chain / k_dmap_chain); with the merging off
+    (MPM_B200_CHAIN=0) the plain per-lane reductions run.  Both are the same
+    sums in another order: they agree to FP32 rounding, and both match the
+    oracle to the mixed-mode tolerance."""
+    mk = small2d if dim == 2 else small3d
+    outs = []
+    for chain in ("1", "0"):
+        monkeypatch.setenv("MPM_B200_CHAIN", chain)
+        case = mk(pkg, constitutive="druckerprager", gpu_precision="mixed", scheme=scheme)
+        dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+        dev.step(case.dt, 0.0, 24)
+        out = fresh_particles(pkg, case.mp)
+        dev.download(pkg._lib.F_REFERENCE | pkg._lib.F_F, out)
+        dev.close()
+        outs.append(out)
+    assert rel(outs[0].xi - case.mp.xi, outs[1].xi - case.mp.xi) < 1e-5
+    for f in ("vs", "F", "Omega"):
+        assert rel(getattr(outs[0], f), getattr(outs[1], f)) < 1e-5, f
+    o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc)
+    o.run(case.dt, 0.0, 24)
+    for out in outs:
+        check_fields(out, o, case.mp, TOL32, TOL32_STRESS)
+
+
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
 @pytest.mark.parametrize("dim", [2, 3])
 def test_mvl(pkg, orc, gpu_lib, dim, prec, tol):
