@@ -187,13 +187,13 @@ __global__ void __launch_bounds__(128) k_solve_ts(GDev<R> g, StepParams sp) {
 // doublemapping1_TS! (utils_TS.jl:543-648, velocities of both phases) fused
 // with doublemapping2_TS! (utils_TS.jl:657-704, re-scatter of both momenta).
 // The position update of DM1 is done by k_g2p_ts from the same ΣN·vsT.
+// doublemapping1_TS! of one particle: gathers, both velocities (stored), both
+// momenta for the re-scatter; w receives the particle's window.
 template <int D, typename R>
-__global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepParams sp) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= sp.np) return;
+__device__ __forceinline__ void dmap_ts_core(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp, int64_t i,
+                                             AxisW<R> *w, R *ps, R *pw) {
     double x[3];
     load_x<D, R>(P, i, x);
-    AxisW<R> w[3];
     particle_weights<D, R>(x, g, w);   // out-of-grid particles get zero weights
     const int n0 = window_n0<D, R>(g, w);
     const int plane = g.nnx * g.nny;
@@ -228,7 +228,8 @@ __global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepPa
     }
     const R FLIP = (R)sp.FLIP, PIC = (R)sp.PIC;
     const R n = P.n[i], ms = P.m[i], mw = P.mw[i];
-    R ps[3] = {0, 0, 0}, pw[3] = {0, 0, 0};
+    ps[0] = ps[1] = ps[2] = R(0);
+    pw[0] = pw[1] = pw[2] = R(0);
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         const R vs = FLIP * (P.v[d][i] + s1[d]) + PIC * s2[d];
@@ -238,6 +239,21 @@ __global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepPa
         ps[d] = ms * vs * (R(1) - n);
         pw[d] = mw * vw * n;
     }
+}
+
+// doublemapping1_TS! (utils_TS.jl:543-648, velocities of both phases) fused
+// with doublemapping2_TS! (utils_TS.jl:657-704, re-scatter of both momenta).
+// The position update of DM1 is done by k_g2p_ts from the same ΣN·vsT.
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sp.np) return;
+    AxisW<R> w[3];
+    R ps[3], pw[3];
+    dmap_ts_core<D, R>(P, g, sp, i, w, ps, pw);
+    const int n0 = window_n0<D, R>(g, w);
+    const int plane = g.nnx * g.nny;
+    constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         const R wz = D == 3 ? w[2].N[c] : R(1);
@@ -254,6 +270,69 @@ __global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepPa
                 const R N = wxz * wy;
                 red_add4(&g.acc[col + b].a, R(0), N * ps[0], N * ps[1], N * ps[2]);
                 red_add4(&g.accw[col + b].a, R(0), N * pw[0], N * pw[1], N * pw[2]);
+            }
+        }
+    }
+}
+
+// The same pass (FP32) with the re-scatter of chained warp lanes merged (the
+// momenta are lane constants, so only the weights are shuffled; see
+// dm2_scatter_chain).
+template <int D>
+__global__ void __launch_bounds__(256) k_dmap_ts_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < sp.np;
+    AxisW<float> w[3];
+    float ps[3] = {0, 0, 0}, pw[3] = {0, 0, 0};
+    int n0 = 0, key = dead_key();
+    if (live) {
+        dmap_ts_core<D, float>(P, g, sp, i, w, ps, pw);
+        n0 = key = window_n0<D, float>(g, w);
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            w[a].base = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+        }
+    }
+    const Chain ch = chain_of(key);
+    const unsigned F = 0xffffffffu;
+    float s1[3], s2[3], q1[3], q2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s1[k] = __shfl_up_sync(F, ps[k], 1); s2[k] = __shfl_up_sync(F, ps[k], 2);
+        q1[k] = __shfl_up_sync(F, pw[k], 1); q2[k] = __shfl_up_sync(F, pw[k], 2);
+    }
+    const int plane = g.nnx * g.nny;
+    constexpr int NC = D == 3 ? 3 : 1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const float wz = D == 3 ? w[2].N[c] : 1.0f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float wxz = w[0].N[a] * wz;
+            const float N0 = wxz * w[1].N[0], N1 = wxz * w[1].N[1], N2 = wxz * w[1].N[2];
+            const float u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2), v2 = __shfl_up_sync(F, N2, 1);
+            const float a1 = ch.c1 ? u1 : 0.0f, a2 = ch.c2 ? u2 : 0.0f, b2 = ch.c1 ? v2 : 0.0f;
+            const int col = n0 + a * g.nny + c * plane;
+            if (N0 + a1 + a2 != 0.0f) {
+                red_add4(&g.acc[col].a, 0.0f, N0 * ps[0] + a1 * s1[0] + a2 * s2[0], N0 * ps[1] + a1 * s1[1] + a2 * s2[1],
+                         N0 * ps[2] + a1 * s1[2] + a2 * s2[2]);
+                red_add4(&g.accw[col].a, 0.0f, N0 * pw[0] + a1 * q1[0] + a2 * q2[0],
+                         N0 * pw[1] + a1 * q1[1] + a2 * q2[1], N0 * pw[2] + a1 * q1[2] + a2 * q2[2]);
+            }
+            if (ch.end) {
+                if (N1 + b2 != 0.0f) {
+                    red_add4(&g.acc[col + 1].a, 0.0f, N1 * ps[0] + b2 * s1[0], N1 * ps[1] + b2 * s1[1],
+                             N1 * ps[2] + b2 * s1[2]);
+                    red_add4(&g.accw[col + 1].a, 0.0f, N1 * pw[0] + b2 * q1[0], N1 * pw[1] + b2 * q1[1],
+                             N1 * pw[2] + b2 * q1[2]);
+                }
+                if (N2 != 0.0f) {
+                    red_add4(&g.acc[col + 2].a, 0.0f, N2 * ps[0], N2 * ps[1], N2 * ps[2]);
+                    red_add4(&g.accw[col + 2].a, 0.0f, N2 * pw[0], N2 * pw[1], N2 * pw[2]);
+                }
             }
         }
     }
