@@ -92,7 +92,7 @@ class Stats(C.Structure):
 
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp", "-shared", "-lgomp"]
 
 
 TRANSLATION_UNITS = ["mpm_b200.cu", "mpm_noalloc.cu", "mpm_grf.cu", "mpm_mlp.cu", "mpm_h5.cpp"]

@@ -857,6 +857,7 @@ template <int D, typename R> struct Upload {
             // Ω·ρs = (J Ω0)(ρs0 / J) is invariant through the run.
             {
                 std::vector<R> m(np);
+#pragma omp parallel for schedule(static)
                 for (int64_t i = 0; i < np; ++i) m[i] = (R)(view_get(v->Omega, i, 0) * view_get(v->rho, i, 0));
                 CK(cudaMemcpy(P.m, m.data(), np * sizeof(R), cudaMemcpyHostToDevice));
             }
@@ -885,14 +886,18 @@ template <int D, typename R> struct Upload {
             }
             {
                 std::vector<uint32_t> mid(np);
+                int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
                 for (int64_t i = 0; i < np; ++i) {
-                    int64_t q = view_geti(v->nid, i);
-                    if (q < 1 || q > h->d.nmat) throw Err{MPM_E_ARG, "nid out of range 1..nmat"};
+                    const int64_t q = view_geti(v->nid, i);
+                    if (q < 1 || q > h->d.nmat) bad = 1;
                     mid[i] = (uint32_t)(q - 1);
                 }
+                if (bad) throw Err{MPM_E_ARG, "nid out of range 1..nmat"};
                 if (h->coh_mode) {
                     // one shared material record; the cohesion travels with the particle
                     std::vector<R> coh(np);
+#pragma omp parallel for schedule(static)
                     for (int64_t i = 0; i < np; ++i) coh[i] = (R)view_get(v->c, mid[i], 0);
                     CK(cudaMemcpy(P.coh, coh.data(), np * sizeof(R), cudaMemcpyHostToDevice));
                     std::fill(mid.begin(), mid.end(), 0u);
@@ -917,6 +922,8 @@ template <int D, typename R> struct Upload {
         const mpm_view *wv[3] = {&v->vxw_val, &v->vyw_val, &v->vzw_val};
         std::vector<T4> valw(h->ts ? ni : 0);
         bool anyw = false;
+        const bool ts = h->ts;
+#pragma omp parallel for schedule(static) reduction(|| : anyval, anyw)
         for (int64_t r = 0; r < ni; ++r) {
             int64_t inode = r;
             if (D == 2) {  // reference 2D: y descending inside a column
@@ -932,7 +939,7 @@ template <int D, typename R> struct Upload {
                     if (vals[d] != R(0)) anyval = true;
                 }
             }
-            if (h->ts) {
+            if (ts) {
                 R wvals[3] = {0, 0, 0};
                 for (int d = 0; d < D; ++d) {
                     if (widx[d]->ptr && widx[d]->ld >= ni && view_geti(*widx[d], r) != 0) {
