@@ -128,7 +128,7 @@ struct mpm_handle {
     bool acc_valid = false;     // grid accumulators hold the P2G of the current particles
     double acc_Ti = 0.0;
     int64_t steps_done = 0, sorts_done = 0, since_sort = 1 << 30;
-    int sort_every = 8;
+    int sort_every = 16;
     int err_host = 0;
     double last_step_ms = 0;
     size_t bytes = 0;
@@ -1352,7 +1352,9 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         h->ts = d->coupling == MPM_COUPLING_TS;
         if (h->d.dim == 2) { h->d.nnz = 1; h->d.z1 = 0; h->d.dz = 1; h->d.lpz = 1; }
         h->fp64 = d->precision == MPM_PREC_FP64;
-        h->sort_every = d->sort_every > 0 ? d->sort_every : 8;
+        // re-sort period: particles move far less than a cell per step (CFL 0.2
+        // on the wave speed), and 16 measured faster than 8 with the lane merging
+        h->sort_every = d->sort_every > 0 ? d->sort_every : 16;
         h->ni = ni;
         CK(cudaSetDevice(d->device));
         h->dev = d->device;

@@ -477,17 +477,48 @@ struct Chain {
     bool c1;    // lane L-1's window is this window shifted by -1 in y
     bool c2;    // ... and lane L-2's by -2
     bool end;   // lane L+1 does not continue the chain
+    bool x1;    // lane L-8's window is this window shifted by -1 in x
+    bool x2;    // ... and lane L-16's by -2
+    bool xend;  // lane L+8 does not continue the x chain
 };
 
-__device__ __forceinline__ Chain chain_of(int n0) {
+// nny = nodes along y: the x step of a window corner
+__device__ __forceinline__ Chain chain_of(int n0, int nny) {
     const int lane = threadIdx.x & 31;
-    const int p1 = __shfl_up_sync(0xffffffffu, n0, 1), p2 = __shfl_up_sync(0xffffffffu, n0, 2);
-    const int q1 = __shfl_down_sync(0xffffffffu, n0, 1);
+    const unsigned F = 0xffffffffu;
+    const int p1 = __shfl_up_sync(F, n0, 1), p2 = __shfl_up_sync(F, n0, 2);
+    const int q1 = __shfl_down_sync(F, n0, 1);
+    const int r1 = __shfl_up_sync(F, n0, 8), r2 = __shfl_up_sync(F, n0, 16);
+    const int s1 = __shfl_down_sync(F, n0, 8);
     Chain c;
     c.c1 = lane >= 1 && p1 == n0 - 1;
     c.c2 = c.c1 && lane >= 2 && p2 == n0 - 2;
     c.end = !(lane <= 30 && q1 == n0 + 1);
+    c.x1 = lane >= 8 && r1 == n0 - nny;
+    c.x2 = c.x1 && lane >= 16 && r2 == n0 - 2 * nny;
+    c.xend = !(lane < 24 && s1 == n0 + nny);
     return c;
+}
+
+// Merge of row 0 across x: the three window columns a = 0, 1, 2 of row 0 (already
+// merged along y) of lane L are columns 1 and 2 of lanes L-8 and L-16 when those
+// lanes sit one and two cells lower in x (the cell order of a tile puts 8 cells
+// along y, so lane L-8 holds the same rank in the x-neighbouring cell).  Column
+// 0 takes the two shuffled contributions; only the last lane of an x chain also
+// emits columns 1 and 2.  v[a][k]: k-th component of column a; returns whether
+// column a is emitted by this lane.
+template <int K>
+__device__ __forceinline__ void xmerge_row0(const Chain &ch, float (*v)[K], bool *emit) {
+    const unsigned F = 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const float a1 = __shfl_up_sync(F, v[1][k], 8), a2 = __shfl_up_sync(F, v[2][k], 16);
+        const float b2 = __shfl_up_sync(F, v[2][k], 8);
+        v[0][k] += (ch.x1 ? a1 : 0.0f) + (ch.x2 ? a2 : 0.0f);
+        v[1][k] += ch.x1 ? b2 : 0.0f;
+    }
+    emit[0] = true;
+    emit[1] = emit[2] = ch.xend;
 }
 
 // doublemapping2 (momentum N·p) with chained lanes merged; n0 = window corner,
@@ -495,7 +526,7 @@ __device__ __forceinline__ Chain chain_of(int n0) {
 template <int D>
 __device__ __forceinline__ void dm2_scatter_chain(const GDev<float> &g, const AxisW<float> *w, int n0, int key,
                                                   const float *p) {
-    const Chain ch = chain_of(key);
+    const Chain ch = chain_of(key, g.nny);
     const unsigned F = 0xffffffffu;
     float p1[3], p2[3];
 #pragma unroll
@@ -508,21 +539,28 @@ __device__ __forceinline__ void dm2_scatter_chain(const GDev<float> &g, const Ax
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         const float wz = D == 3 ? w[2].N[c] : 1.0f;
+        float r0[3][3];   // row 0 of columns a = 0..2 (merged along y)
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const float wxz = w[0].N[a] * wz;
             const float N0 = wxz * w[1].N[0], N1 = wxz * w[1].N[1], N2 = wxz * w[1].N[2];
             const float u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2), v2 = __shfl_up_sync(F, N2, 1);
             const float a1 = ch.c1 ? u1 : 0.0f, a2 = ch.c2 ? u2 : 0.0f, b2 = ch.c1 ? v2 : 0.0f;
-            Node8<float> *col = g.acc + (n0 + a * g.nny + c * plane);
-            if (N0 + a1 + a2 != 0.0f)
-                red_add4(&col[0].a, 0.0f, N0 * p[0] + a1 * p1[0] + a2 * p2[0], N0 * p[1] + a1 * p1[1] + a2 * p2[1],
-                         N0 * p[2] + a1 * p1[2] + a2 * p2[2]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) r0[a][k] = N0 * p[k] + a1 * p1[k] + a2 * p2[k];
             if (ch.end) {
+                Node8<float> *col = g.acc + (n0 + a * g.nny + c * plane);
                 if (N1 + b2 != 0.0f)
                     red_add4(&col[1].a, 0.0f, N1 * p[0] + b2 * p1[0], N1 * p[1] + b2 * p1[1], N1 * p[2] + b2 * p1[2]);
                 if (N2 != 0.0f) red_add4(&col[2].a, 0.0f, N2 * p[0], N2 * p[1], N2 * p[2]);
             }
+        }
+        bool emit[3];
+        xmerge_row0<3>(ch, r0, emit);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (!emit[a] || (r0[a][0] == 0.0f && r0[a][1] == 0.0f && r0[a][2] == 0.0f)) continue;
+            red_add4(&g.acc[n0 + a * g.nny + c * plane].a, 0.0f, r0[a][0], r0[a][1], r0[a][2]);
         }
     }
 }
@@ -532,7 +570,7 @@ __device__ __forceinline__ void dm2_scatter_chain(const GDev<float> &g, const Ax
 template <int D>
 __device__ __forceinline__ void p2g_scatter_chain(const GDev<float> &g, const AxisW<float> *w, int n0, int key,
                                                   float m, float vol, const float *v, const float *s, float G) {
-    const Chain ch = chain_of(key);
+    const Chain ch = chain_of(key, g.nny);
     const unsigned F = 0xffffffffu;
     const float p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : 0.0f};
     const int plane = g.nnx * g.nny;

@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(256) k_dmap_ts_chain(PDev<D, float> P, GDev<fl
             for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
         }
     }
-    const Chain ch = chain_of(key);
+    const Chain ch = chain_of(key, g.nny);
     const unsigned F = 0xffffffffu;
     float s1[3], s2[3], q1[3], q2[3];
 #pragma unroll
