@@ -26,6 +26,7 @@
 #include "mpm_mc3d.cuh"
 
 #include <climits>
+#include <type_traits>
 
 // resident CTAs of 256 threads per SM the particle passes are register-capped for
 #ifndef MPM_P_MINB
@@ -603,37 +604,45 @@ __device__ __forceinline__ void p2g_scatter_chain(const GDev<float> &g, const Ax
                 U[6] = sv[5] * gxz + sv[2] * xdz + U[0] * G;
                 Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = sv[4] * wxz;
             }
-            float r0[7], r1[7], r2[7];   // this lane's rows b = 0, 1, 2
+            // this lane's rows b = 0, 1, 2 as component pairs (packed FP32 arithmetic):
+            // (m, px), (py, pz), (fx, fy), (fz, 0)
+            float2 r0[4], r1[4], r2[4];
+            const float2 U01 = make_float2(U[0], U[1]), U23 = make_float2(U[2], U[3]);
+            const float2 U45 = make_float2(U[4], U[5]), Y01 = make_float2(Y[0], Y[1]);
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 const float wy = w[1].N[b], gy = w[1].dN[b];
-                float *r = b == 0 ? r0 : (b == 1 ? r1 : r2);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) r[k] = wy * U[k];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) r[4 + k] = wy * U[4 + k] + gy * Y[k];
+                const float2 w2 = make_float2(wy, wy), g2 = make_float2(gy, gy);
+                float2 *r = b == 0 ? r0 : (b == 1 ? r1 : r2);
+                r[0] = __fmul2_rn(w2, U01);
+                r[1] = __fmul2_rn(w2, U23);
+                r[2] = __ffma2_rn(w2, U45, __fmul2_rn(g2, Y01));
+                r[3] = make_float2(wy * U[6] + gy * Y[2], 0.0f);
             }
             // row 0 += lane L-1's row 1 + lane L-2's row 2; chain ends: row 1 += lane L-1's row 2
+            const float f1 = ch.c1 ? 1.0f : 0.0f, f2 = ch.c2 ? 1.0f : 0.0f;
+            const float2 c1 = make_float2(f1, f1), c2 = make_float2(f2, f2);
 #pragma unroll
-            for (int k = 0; k < 7; ++k) {
-                const float x1 = __shfl_up_sync(F, r1[k], 1), x2 = __shfl_up_sync(F, r2[k], 2);
-                const float y2 = __shfl_up_sync(F, r2[k], 1);
-                r0[k] += (ch.c1 ? x1 : 0.0f) + (ch.c2 ? x2 : 0.0f);
-                r1[k] += ch.c1 ? y2 : 0.0f;
+            for (int j = 0; j < 4; ++j) {
+                const float2 x1 = make_float2(__shfl_up_sync(F, r1[j].x, 1), __shfl_up_sync(F, r1[j].y, 1));
+                const float2 x2 = make_float2(__shfl_up_sync(F, r2[j].x, 2), __shfl_up_sync(F, r2[j].y, 2));
+                const float2 y2 = make_float2(__shfl_up_sync(F, r2[j].x, 1), __shfl_up_sync(F, r2[j].y, 1));
+                r0[j] = __ffma2_rn(c2, x2, __ffma2_rn(c1, x1, r0[j]));
+                r1[j] = __ffma2_rn(c1, y2, r1[j]);
             }
             Node8<float> *col = g.acc + (n0 + a * g.nny + c * plane);
-            if (r0[0] != 0.0f) {
-                red_add4(&col[0].a, r0[0], r0[1], r0[2], r0[3]);
-                red_add4(&col[0].b, r0[4], r0[5], r0[6], 0.0f);
+            if (r0[0].x != 0.0f) {
+                red_add4(&col[0].a, r0[0].x, r0[0].y, r0[1].x, r0[1].y);
+                red_add4(&col[0].b, r0[2].x, r0[2].y, r0[3].x, 0.0f);
             }
             if (ch.end) {
-                if (r1[0] != 0.0f) {
-                    red_add4(&col[1].a, r1[0], r1[1], r1[2], r1[3]);
-                    red_add4(&col[1].b, r1[4], r1[5], r1[6], 0.0f);
+                if (r1[0].x != 0.0f) {
+                    red_add4(&col[1].a, r1[0].x, r1[0].y, r1[1].x, r1[1].y);
+                    red_add4(&col[1].b, r1[2].x, r1[2].y, r1[3].x, 0.0f);
                 }
-                if (r2[0] != 0.0f) {
-                    red_add4(&col[2].a, r2[0], r2[1], r2[2], r2[3]);
-                    red_add4(&col[2].b, r2[4], r2[5], r2[6], 0.0f);
+                if (r2[0].x != 0.0f) {
+                    red_add4(&col[2].a, r2[0].x, r2[0].y, r2[1].x, r2[1].y);
+                    red_add4(&col[2].b, r2[2].x, r2[2].y, r2[3].x, 0.0f);
                 }
             }
         }
@@ -1054,10 +1063,25 @@ __device__ __forceinline__ void g2p_core(const PDev<D, R> &P, const GDev<R> &g, 
                 if (wy == R(0)) continue;
                 const Node8<R> q = g.gat[col + b];
                 const auto du = USL ? q.a : q.b;
-                const R u[3] = {du.x - duc.x, du.y - duc.y, du.z - duc.z};
-                T[0] += wy * q.a.x; T[1] += wy * q.a.y; T[2] += wy * q.a.z;
+                if constexpr (std::is_same<R, float>::value) {
+                    // x and y components as packed FP32 pairs
+                    const float2 w2 = make_float2(wy, wy), g2 = make_float2(gy, gy);
+                    const float2 u01 = __fadd2_rn(make_float2(du.x, du.y), make_float2(-duc.x, -duc.y));
+                    const float2 t01 = __ffma2_rn(w2, make_float2(q.a.x, q.a.y), make_float2(T[0], T[1]));
+                    const float2 a01 = __ffma2_rn(w2, u01, make_float2(A[0], A[1]));
+                    const float2 b01 = __ffma2_rn(g2, u01, make_float2(B[0], B[1]));
+                    T[0] = t01.x; T[1] = t01.y; T[2] += wy * q.a.z;
+                    A[0] = a01.x; A[1] = a01.y; B[0] = b01.x; B[1] = b01.y;
+                    if (D == 3) {
+                        const float u2 = du.z - duc.z;
+                        A[2] += wy * u2; B[2] += gy * u2;
+                    }
+                } else {
+                    const R u[3] = {du.x - duc.x, du.y - duc.y, du.z - duc.z};
+                    T[0] += wy * q.a.x; T[1] += wy * q.a.y; T[2] += wy * q.a.z;
 #pragma unroll
-                for (int k = 0; k < D; ++k) { A[k] += wy * u[k]; B[k] += gy * u[k]; }
+                    for (int k = 0; k < D; ++k) { A[k] += wy * u[k]; B[k] += gy * u[k]; }
+                }
                 if (USL) {
                     Sa[0] += wy * q.b.x; Sa[1] += wy * q.b.y; Sa[2] += wy * q.b.z;
                     if (sp.need_vs) {
