@@ -603,6 +603,13 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         L.run("dm3", [&] { k_dm3_ts<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         if (np) L.run("g2p_p2g", [&] {
+            if constexpr (std::is_same<R, float>::value) {
+                if (h->chain) {
+                    if (mc3) k_g2p_ts_chain<D, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    else k_g2p_ts_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    return;
+                }
+            }
             if (mc3) k_g2p_ts<D, R, true, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
             else k_g2p_ts<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
         });
