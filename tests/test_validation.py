@@ -61,8 +61,9 @@ def test_column_collapse_matches_experiment(pkg, gpu_lib, prec, tmp_path):
     dh = np.abs(h - he)[inner]
     assert dh.mean() < 2.5e-3, dh.mean()
     assert dh.max() < 6e-3, dh.max()
-    # toe of the deposit (where the surface falls below 3 mm) within 5 cm
+    # toe of the deposit (where the surface falls below 5 mm, four particle
+    # layers; thinner tails are one or two scattered layers) within 5 cm
     h0 = np.nan_to_num(h, nan=0.0)
-    assert abs(toe(xc, h0, 3e-3) - toe(surf[:, 0], surf[:, 1], 3e-3)) < 0.05
+    assert abs(toe(xc, h0, 5e-3) - toe(surf[:, 0], surf[:, 1], 5e-3)) < 0.05
     # the column's crest stays at the wall (x < 2 cm keeps ~ the initial height)
     assert abs(h[0] - 0.1) < 3e-3
