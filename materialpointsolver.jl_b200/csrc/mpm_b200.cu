@@ -16,6 +16,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -160,9 +161,7 @@ struct mpm_handle {
     int nsm = 148;
     bool tiled = false;
     SortGeom sg{};
-    // staging
-    void *stage = nullptr;
-    size_t stage_bytes = 0;
+    size_t pbuf_size = 0;   // bytes of each particle buffer
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool profiling = false;
     std::vector<KTimer> ktimes;
@@ -350,53 +349,70 @@ __global__ void k_derived(PDev<D, R> P, int64_t np, int what, double *out) {
     out[P.orig[i]] = v;
 }
 
-void ensure_stage(mpm_handle *h, size_t bytes) {
-    if (h->stage_bytes >= bytes) return;
-    if (h->stage) {
-        cudaFree(h->stage);
-        h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), h->stage), h->allocs.end());
-        h->bytes -= h->stage_bytes;
-    }
-    h->stage = dalloc(h, bytes);
-    h->stage_bytes = bytes;
+// Synchronises a stream when it leaves scope (host buffers of pending copies).
+struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamSynchronize(s); }
+};
+
+// Host <-> device staging.  The sort's target buffer (pbuf[1]) holds nothing
+// between sorts, and every staged copy below is ordered on h->stream with the
+// sorts, so it serves as the staging area: at least 24 bytes per particle
+// (positions alone take 8 per axis), i.e. three FP64 columns.
+char *stage_area(mpm_handle *h, size_t bytes) {
+    if (bytes > h->pbuf_size) throw Err{MPM_E_ARG, "staging request larger than a particle buffer"};
+    return (char *)h->pbuf[1];
 }
 
+// Stage host column k of view v (any element type) into the first np x 8
+// bytes of the staging area and convert it into dst.  No host synchronisation:
+// the staging slot is reused only by later work on the same stream, and the
+// caller synchronises once after its last copy.
 template <typename T>
 void upload_col(mpm_handle *h, const mpm_view &v, int64_t k, T *dst, int64_t n) {
     size_t es = type_size(v.type);
-    ensure_stage(h, n * 8);
+    char *stage = stage_area(h, n * 8);
     const char *src = (const char *)v.ptr + (size_t)(v.ld * k) * es;
-    CK(cudaMemcpyAsync(h->stage, src, n * es, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(stage, src, n * es, cudaMemcpyHostToDevice, h->stream));
     int64_t nb = cdiv(n, 256);
     switch (v.type) {
-        case MPM_T_F64: k_convert<double, T><<<nb, 256, 0, h->stream>>>((const double *)h->stage, dst, n); break;
-        case MPM_T_F32: k_convert<float, T><<<nb, 256, 0, h->stream>>>((const float *)h->stage, dst, n); break;
-        case MPM_T_I64: k_convert<long long, T><<<nb, 256, 0, h->stream>>>((const long long *)h->stage, dst, n); break;
-        case MPM_T_I32: k_convert<int, T><<<nb, 256, 0, h->stream>>>((const int *)h->stage, dst, n); break;
+        case MPM_T_F64: k_convert<double, T><<<nb, 256, 0, h->stream>>>((const double *)stage, dst, n); break;
+        case MPM_T_F32: k_convert<float, T><<<nb, 256, 0, h->stream>>>((const float *)stage, dst, n); break;
+        case MPM_T_I64: k_convert<long long, T><<<nb, 256, 0, h->stream>>>((const long long *)stage, dst, n); break;
+        case MPM_T_I32: k_convert<int, T><<<nb, 256, 0, h->stream>>>((const int *)stage, dst, n); break;
     }
     LAUNCH_CHECK();
-    CK(cudaStreamSynchronize(h->stream));
 }
 
-// download a state array in original order into host column k of view v
+// Download a state array in original order into host column k of view v.
+// A copy into pageable host memory returns once it has landed; into pinned
+// memory it is asynchronous and the caller synchronises after its last copy.
 template <typename S>
 void download_col(mpm_handle *h, const S *src, const uint32_t *orig, const mpm_view &v, int64_t k, int64_t n) {
     size_t es = type_size(v.type);
-    ensure_stage(h, n * 8);
+    char *stage = stage_area(h, n * 8);
     int64_t nb = cdiv(n, 256);
-    if (v.type == MPM_T_F64) k_unpermute<S, double><<<nb, 256, 0, h->stream>>>(src, orig, (double *)h->stage, n);
-    else if (v.type == MPM_T_F32) k_unpermute<S, float><<<nb, 256, 0, h->stream>>>(src, orig, (float *)h->stage, n);
+    if (v.type == MPM_T_F64) k_unpermute<S, double><<<nb, 256, 0, h->stream>>>(src, orig, (double *)stage, n);
+    else if (v.type == MPM_T_F32) k_unpermute<S, float><<<nb, 256, 0, h->stream>>>(src, orig, (float *)stage, n);
     else throw Err{MPM_E_ARG, "float field requested into an integer view"};
     LAUNCH_CHECK();
     char *dst = (char *)v.ptr + (size_t)(v.ld * k) * es;
-    CK(cudaMemcpyAsync(dst, h->stage, n * es, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpyAsync(dst, stage, n * es, cudaMemcpyDeviceToHost, h->stream));
+}
+
+// m = (R)(a * b) from two staged FP64 columns: the particle mass Ω·ρ rounded
+// once from FP64, as the host product would be
+template <typename R>
+__global__ void k_mass(const double *a, const double *b, R *m, int64_t n) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) m[i] = (R)(a[i] * b[i]);
 }
 
 // ---- materials ---------------------------------------------------------------------
-template <typename R> void build_materials(mpm_handle *h, const mpm_host_views *v) {
+// M is the caller's: it must outlive the asynchronous copy
+template <typename R> void build_materials(mpm_handle *h, const mpm_host_views *v, std::vector<Mat<R>> &M) {
     const int64_t nm = h->coh_mode ? 1 : h->d.nmat;
-    std::vector<Mat<R>> M(nm);
+    M.assign(nm, Mat<R>{});
     auto get = [&](const mpm_view &vw, int64_t i) { return vw.ptr ? view_get(vw, i, 0) : 0.0; };
     for (int64_t i = 0; i < nm; ++i) {
         double K = get(v->Ks, i), G = get(v->Gs, i), c = get(v->c, i), phi = get(v->phi, i),
@@ -426,7 +442,7 @@ template <typename R> void build_materials(mpm_handle *h, const mpm_host_views *
             if (!(m.kperm != R(0))) throw Err{MPM_E_ARG, "two-phase model needs a non-zero permeability k"};
         }
     }
-    CK(cudaMemcpy(h->mat, M.data(), nm * sizeof(Mat<R>), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->mat, M.data(), nm * sizeof(Mat<R>), cudaMemcpyHostToDevice, h->stream));
 }
 
 // ---- the sort ----------------------------------------------------------------------
@@ -842,6 +858,20 @@ template <int D, typename R> struct Upload {
             h->coh_mode = same;
         }
         P = pdev_from<D, R>(h, 0);
+        // host arrays handed to asynchronous copies outlive them: the guard,
+        // declared after them, synchronises the stream before they are freed,
+        // on the error paths too
+        // (left uninitialised: the parallel loops below write every entry, so
+        // their pages are first touched by the threads that fill them)
+        const int64_t ni = h->ni, nny = h->d.nny;
+        using T4 = typename Vec<R>::T4;
+        std::unique_ptr<uint32_t[]> mid(new uint32_t[np]);
+        std::unique_ptr<R[]> coh;
+        std::unique_ptr<uint8_t[]> mask(new uint8_t[ni]);
+        std::unique_ptr<T4[]> val(new T4[ni]);
+        std::unique_ptr<T4[]> valw(h->ts ? new T4[ni] : nullptr);
+        std::vector<Mat<R>> M;
+        StreamGuard guard{h->stream};
         if (np) {
             for (int d = 0; d < D; ++d) upload_col<double>(h, v->xi, d, P.x[d], np);
             for (int d = 0; d < D; ++d) upload_col<R>(h, v->vs, d, P.v[d], np);
@@ -859,19 +889,28 @@ template <int D, typename R> struct Upload {
             opt(v->epsk, P.epsk);
             opt(v->epsv, P.epsv);
             upload_col<R>(h, v->Omega0, 0, P.vol0, np);
-            upload_col<R>(h, v->Omega, 0, P.vol, np);
             // particle mass ms = Ω·ρs (resetmpstatus_OS!, utils_OS.jl:199), kept per particle:
-            // Ω·ρs = (J Ω0)(ρs0 / J) is invariant through the run.
-            {
-                std::vector<R> m(np);
-#pragma omp parallel for schedule(static)
-                for (int64_t i = 0; i < np; ++i) m[i] = (R)(view_get(v->Omega, i, 0) * view_get(v->rho, i, 0));
-                CK(cudaMemcpy(P.m, m.data(), np * sizeof(R), cudaMemcpyHostToDevice));
-            }
+            // Ω·ρs = (J Ω0)(ρs0 / J) is invariant through the run.  Ω and ρs are staged
+            // in FP64 behind the staging slot and multiplied on the device.
+            double *om = (double *)(stage_area(h, np * 24) + np * 8), *rh = om + np;
+            const int64_t nb = cdiv(np, 256);
+            upload_col<double>(h, v->Omega, 0, om, np);
+            k_convert<double, R><<<nb, 256, 0, h->stream>>>(om, P.vol, np);
+            upload_col<double>(h, v->rho, 0, rh, np);
+            k_mass<R><<<nb, 256, 0, h->stream>>>(om, rh, P.m, np);
+            LAUNCH_CHECK();
             if (h->ts) {
                 // two-phase fields (particle.jl:103-128); mw = Ω·ρw is invariant like ms
                 req(v->n, "n");
                 req(v->rhow, "rhow");
+                if (!v->Kw.ptr || !v->kperm.ptr) throw Err{MPM_E_ARG, "two-phase model needs the Kw and k arrays"};
+                int badn = 0;
+#pragma omp parallel for schedule(static) reduction(| : badn)
+                for (int64_t i = 0; i < np; ++i) {
+                    const double n = view_get(v->n, i, 0);
+                    if (!(n > 0.0 && n < 1.0)) badn = 1;
+                }
+                if (badn) throw Err{MPM_E_ARG, "two-phase porosity n must lie in (0, 1)"};
                 upload_col<R>(h, v->n, 0, P.n, np);
                 opt(v->sigw, P.sigw);
                 for (int d = 0; d < D; ++d) {
@@ -882,44 +921,33 @@ template <int D, typename R> struct Upload {
                     if (v->epsw.ptr) upload_col<R>(h, v->epsw, c, P.epsw[c], np);
                     else CK(cudaMemsetAsync(P.epsw[c], 0, np * sizeof(R), h->stream));
                 }
-                std::vector<R> mw(np);
-                for (int64_t i = 0; i < np; ++i) {
-                    const double n = view_get(v->n, i, 0);
-                    if (!(n > 0.0 && n < 1.0)) throw Err{MPM_E_ARG, "two-phase porosity n must lie in (0, 1)"};
-                    mw[i] = (R)(view_get(v->Omega, i, 0) * view_get(v->rhow, i, 0));
-                }
-                CK(cudaMemcpy(P.mw, mw.data(), np * sizeof(R), cudaMemcpyHostToDevice));
-                if (!v->Kw.ptr || !v->kperm.ptr) throw Err{MPM_E_ARG, "two-phase model needs the Kw and k arrays"};
+                upload_col<double>(h, v->rhow, 0, rh, np);
+                k_mass<R><<<nb, 256, 0, h->stream>>>(om, rh, P.mw, np);
+                LAUNCH_CHECK();
             }
-            {
-                std::vector<uint32_t> mid(np);
-                int bad = 0;
+            // host-side conversions run while the column copies above are in flight;
+            // their (pageable) copies are enqueued after the boundary loop
+            int bad = 0;
 #pragma omp parallel for schedule(static) reduction(| : bad)
-                for (int64_t i = 0; i < np; ++i) {
-                    const int64_t q = view_geti(v->nid, i);
-                    if (q < 1 || q > h->d.nmat) bad = 1;
-                    mid[i] = (uint32_t)(q - 1);
-                }
-                if (bad) throw Err{MPM_E_ARG, "nid out of range 1..nmat"};
-                if (h->coh_mode) {
-                    // one shared material record; the cohesion travels with the particle
-                    std::vector<R> coh(np);
+            for (int64_t i = 0; i < np; ++i) {
+                const int64_t q = view_geti(v->nid, i);
+                if (q < 1 || q > h->d.nmat) bad = 1;
+                mid[i] = (uint32_t)(q - 1);
+            }
+            if (bad) throw Err{MPM_E_ARG, "nid out of range 1..nmat"};
+            if (h->coh_mode) {
+                // one shared material record; the cohesion travels with the particle
+                coh.reset(new R[np]);
 #pragma omp parallel for schedule(static)
-                    for (int64_t i = 0; i < np; ++i) coh[i] = (R)view_get(v->c, mid[i], 0);
-                    CK(cudaMemcpy(P.coh, coh.data(), np * sizeof(R), cudaMemcpyHostToDevice));
-                    std::fill(mid.begin(), mid.end(), 0u);
+                for (int64_t i = 0; i < np; ++i) {
+                    coh[i] = (R)view_get(v->c, mid[i], 0);
+                    mid[i] = 0u;
                 }
-                CK(cudaMemcpy(P.mat, mid.data(), np * 4, cudaMemcpyHostToDevice));
             }
             k_iota<<<cdiv(np, 256), 256, 0, h->stream>>>(P.orig, np);
             LAUNCH_CHECK();
         }
-        build_materials<R>(h, v);
         // boundary: per node in the reference's node order -> internal order
-        using T4 = typename Vec<R>::T4;
-        const int64_t ni = h->ni, nny = h->d.nny;
-        std::vector<uint8_t> mask(ni, 0);
-        std::vector<T4> val(ni);
         bool anyval = false;
         const mpm_view *idx[3] = {&v->vx_idx, &v->vy_idx, &v->vz_idx};
         const mpm_view *vv[3] = {&v->vx_val, &v->vy_val, &v->vz_val};
@@ -927,7 +955,6 @@ template <int D, typename R> struct Upload {
         // reference's [0] default) mean none
         const mpm_view *widx[3] = {&v->vxw_idx, &v->vyw_idx, &v->vzw_idx};
         const mpm_view *wv[3] = {&v->vxw_val, &v->vyw_val, &v->vzw_val};
-        std::vector<T4> valw(h->ts ? ni : 0);
         bool anyw = false;
         const bool ts = h->ts;
 #pragma omp parallel for schedule(static) reduction(|| : anyval, anyw)
@@ -960,16 +987,21 @@ template <int D, typename R> struct Upload {
             mask[inode] = mk;
             val[inode].x = vals[0]; val[inode].y = vals[1]; val[inode].z = vals[2]; val[inode].w = 0;
         }
+        if (np) {
+            if (coh) CK(cudaMemcpyAsync(P.coh, coh.get(), np * sizeof(R), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(P.mat, mid.get(), np * 4, cudaMemcpyHostToDevice, h->stream));
+        }
+        build_materials<R>(h, v, M);
         if (anyw) {
             if (!h->bcvalw) h->bcvalw = dalloc(h, ni * sizeof(T4));
-            CK(cudaMemcpy(h->bcvalw, valw.data(), ni * sizeof(T4), cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(h->bcvalw, valw.get(), ni * sizeof(T4), cudaMemcpyHostToDevice, h->stream));
         } else {
             h->bcvalw = nullptr;
         }
-        CK(cudaMemcpy(h->bcmask, mask.data(), ni, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(h->bcmask, mask.get(), ni, cudaMemcpyHostToDevice, h->stream));
         if (anyval) {
             if (!h->bcval) h->bcval = dalloc(h, ni * sizeof(T4));
-            CK(cudaMemcpy(h->bcval, val.data(), ni * sizeof(T4), cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(h->bcval, val.get(), ni * sizeof(T4), cudaMemcpyHostToDevice, h->stream));
         } else {
             h->bcval = nullptr;
         }
@@ -985,6 +1017,7 @@ template <int D, typename R> struct Download {
         const int64_t np = h->d.np;
         if (!np) return;
         PDev<D, R> P = pdev_from<D, R>(h, 0);
+        StreamGuard guard{h->stream};   // no copy into the caller's arrays outlives the call
         constexpr int NV = PDev<D, R>::NV, NF = PDev<D, R>::NF;
         auto chk = [&](const mpm_view &vw, const char *name) {
             if (!vw.ptr) throw Err{MPM_E_ARG, std::string("missing host array for download: ") + name};
@@ -1006,19 +1039,24 @@ template <int D, typename R> struct Download {
         if (mask & MPM_F_SIGW) { chk(v->sigw, "sigw"); download_col<R>(h, P.sigw, P.orig, v->sigw, 0, np); }
         if (mask & MPM_F_VW) { chk(v->vw, "vw"); for (int d = 0; d < D; ++d) download_col<R>(h, P.vw[d], P.orig, v->vw, d, np); }
         if (mask & MPM_F_EPSW) { chk(v->epsw, "epsw"); for (int c = 0; c < NV; ++c) download_col<R>(h, P.epsw[c], P.orig, v->epsw, c, np); }
+        // derived fields: k_derived writes them in original order straight into
+        // the staging area; FP32 views take a converted copy behind it
         auto derived = [&](int what, const mpm_view &vw, const char *name) {
             chk(vw, name);
-            double *tmp = (double *)dalloc(h, np * 8);
-            k_derived<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, np, what, tmp);
+            double *st = (double *)stage_area(h, np * 12);
+            const int64_t nb = cdiv(np, 256);
+            k_derived<D, R><<<nb, 256, 0, h->stream>>>(P, np, what, st);
             LAUNCH_CHECK();
-            uint32_t *ident = (uint32_t *)dalloc(h, np * 4);
-            k_iota<<<cdiv(np, 256), 256, 0, h->stream>>>(ident, np);
-            download_col<double>(h, tmp, ident, vw, 0, np);
-            cudaFree(tmp);
-            cudaFree(ident);
-            h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)tmp), h->allocs.end());
-            h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)ident), h->allocs.end());
-            h->bytes -= np * 12;
+            if (vw.type == MPM_T_F64) {
+                CK(cudaMemcpyAsync(vw.ptr, st, np * 8, cudaMemcpyDeviceToHost, h->stream));
+            } else if (vw.type == MPM_T_F32) {
+                float *f = (float *)(st + np);
+                k_convert<double, float><<<nb, 256, 0, h->stream>>>(st, f, np);
+                LAUNCH_CHECK();
+                CK(cudaMemcpyAsync(vw.ptr, f, np * 4, cudaMemcpyDeviceToHost, h->stream));
+            } else {
+                throw Err{MPM_E_ARG, "float field requested into an integer view"};
+            }
         };
         if (mask & MPM_F_OMEGA) derived(0, v->Omega, "Omega");
         if (mask & MPM_F_SIGM) derived(1, v->sigm, "sigm");
@@ -1027,7 +1065,7 @@ template <int D, typename R> struct Download {
         if (mask & MPM_F_P2C) {
             chk(v->p2c, "p2c");
             if (v->p2c.type != MPM_T_I64 && v->p2c.type != MPM_T_I32) throw Err{MPM_E_ARG, "p2c view must be integer"};
-            int64_t *tmp = (int64_t *)dalloc(h, np * 8);
+            int64_t *tmp = (int64_t *)stage_area(h, np * 8);
             GDev<R> g = gdev_from<R>(h);
             k_p2c<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, np, tmp);
             LAUNCH_CHECK();
@@ -1038,10 +1076,8 @@ template <int D, typename R> struct Download {
                 if (v->p2c.type == MPM_T_I64) ((int64_t *)v->p2c.ptr)[i] = hv[i];
                 else ((int32_t *)v->p2c.ptr)[i] = (int32_t)hv[i];
             }
-            cudaFree(tmp);
-            h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)tmp), h->allocs.end());
-            h->bytes -= np * 8;
         }
+        CK(cudaStreamSynchronize(h->stream));
     }
 };
 
@@ -1124,9 +1160,7 @@ template <int D, typename R> struct P2CAll {
         if (!np) return;
         PDev<D, R> P = pdev_from<D, R>(h, 0);
         GDev<R> g = gdev_from<R>(h);
-        int64_t *tmp = (int64_t *)h->keys;  // reuse: keys (np x 4 B) is too small, use stage
-        ensure_stage(h, np * 8);
-        tmp = (int64_t *)h->stage;
+        int64_t *tmp = (int64_t *)stage_area(h, np * 8);
         k_p2c<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, np, tmp);
         LAUNCH_CHECK();
         CK(cudaMemcpyAsync(out, tmp, np * 8, cudaMemcpyDeviceToHost, h->stream));
@@ -1162,7 +1196,8 @@ template <int D, typename R> struct Order {
         if (!np) return;
         PDev<D, R> P = pdev_from<D, R>(h, 0);
         std::vector<uint32_t> o(np);
-        CK(cudaMemcpy(o.data(), P.orig, np * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(o.data(), P.orig, np * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
         for (int64_t i = 0; i < np; ++i) out[i] = o[i];
     }
 };
@@ -1373,6 +1408,7 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         size_t pb = pbuf_bytes(d->dim, h->fp64, d->np, h->ts);
         h->pbuf[0] = dalloc(h, pb);
         h->pbuf[1] = dalloc(h, pb);
+        h->pbuf_size = pb;
         h->acc = dalloc(h, ni * 2 * T4);
         h->gat = dalloc(h, ni * 2 * T4);
         h->gvs = (d->PIC != 0.0 || d->va == MPM_VA_V) ? dalloc(h, ni * T4) : nullptr;

@@ -67,3 +67,32 @@ def test_column_collapse_matches_experiment(pkg, gpu_lib, prec, tmp_path):
     assert abs(toe(xc, h0, 5e-3) - toe(surf[:, 0], surf[:, 1], 5e-3)) < 0.05
     # the column's crest stays at the wall (x < 2 cm keeps ~ the initial height)
     assert abs(h[0] - 0.1) < 3e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_saturated_column_consolidates_to_hydrostatic(pkg, gpu_lib, prec, tmp_path):
+    """Two-phase (coupling = :TS) physics: a 0.05 x 0.2 m saturated column,
+    laterally confined, impermeable floor, settles under gravity (0.3 s with
+    5 % damping of both phases).  At rest the pore pressure is hydrostatic,
+    dσw/dd = -ρw g, and the skeleton carries the buoyant weight, dσ'yy/dd =
+    -((1 - n) ρs + n ρw - ρw) g, with the lateral effective stress at the
+    confined-elastic ratio ν / (1 - ν).  Measured on B200 in FP64: -9835 vs
+    -9810 Pa/m for the water and -11322 vs -11331 Pa/m for the skeleton."""
+    c = pkg.workloads.saturated_column(dim=2, h=0.01, size=(0.05, 0.2), k=0.1, Te=0.01, zeta_s=0.05,
+                                       zeta_w=0.05, Ttol=0.3, gpu_precision=prec, project_path=str(tmp_path))
+    pkg.materialpointsolver(c.args, c.grid, c.mp, c.attr, c.bc)
+    g, n, rho_s, rho_w, nu = 9.81, c.meta["n"], 2650.0, c.meta["rho_w"], 0.3
+    d = c.meta["height"] - c.mp.xi[:, 1]
+    inner = d > 0.03                      # below the loosely packed top layers
+    A = np.vstack([d[inner], np.ones(inner.sum())]).T
+
+    def slope(v):
+        return np.linalg.lstsq(A, v[inner], rcond=None)[0][0]
+
+    sw, syy, sxx = slope(c.mp.sigw), slope(c.mp.sig[:, 1]), slope(c.mp.sig[:, 0])
+    assert abs(sw / (-rho_w * g) - 1) < 0.02, sw
+    buoyant = -((1 - n) * rho_s + n * rho_w - rho_w) * g
+    assert abs(syy / buoyant - 1) < 0.02, syy
+    assert abs(sxx / syy - nu / (1 - nu)) < 0.05, sxx / syy
+    assert np.abs(c.mp.vs).max() < 0.02 and np.abs(c.mp.vw).max() < 0.05
