@@ -470,7 +470,7 @@ def run_reference(args):
 
 def run_profile(args):
     """Minimal launch sequence for profilers: upload, W + K steps, exit."""
-    pkg, case = make_case(args.mc3d)
+    pkg, case = make_case(args.mc3d, args.workload)
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
     dev.step(case.dt, 0.0, args.warmup)
     dev.step(case.dt, args.warmup * case.dt, args.steps)

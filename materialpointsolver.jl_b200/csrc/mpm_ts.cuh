@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepPa
 // momenta are lane constants, so only the weights are shuffled; see
 // dm2_scatter_chain).
 template <int D>
-__global__ void __launch_bounds__(256) k_dmap_ts_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+__global__ void __launch_bounds__(256, MPM_TS_DMAP_CHAIN_MINB) k_dmap_ts_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < sp.np;
     AxisW<float> w[3];
@@ -485,110 +485,84 @@ __global__ void __launch_bounds__(256) k_g2p_ts(PDev<D, R> P, GDev<R> g, StepPar
 // water mass and momentum, drag -- merged over chained warp lanes (their
 // factors are lane constants, so the weights and those constants are
 // shuffled; see dm2_scatter_chain); the force records, which depend on ∇N,
-// are reduced per node as in p2g_scatter_ts.  All lanes call it.
+// are reduced per node as in p2g_scatter_ts.  The record groups are scattered
+// in separate sweeps over the window, so only one group's factors are live at
+// a time.  All lanes call it.
 template <int D>
 __device__ __forceinline__ void p2g_scatter_ts_chain(const GDev<float> &g, const AxisW<float> *w, int n0, int key,
                                                      float ms, float mw, float n, float vol, const float *vs,
                                                      const float *vw, const float *s, float sw, float G, float kperm) {
     const Chain ch = chain_of(key, g.nny);
-    const unsigned F = 0xffffffffu;
     const float one_n = 1.0f - n;
     const float mi = one_n * ms + n * mw;
-    const float tdg = kperm != 0.0f ? (n * mw * G) / kperm : 0.0f;
     const float mwn = mw * n;
-    // N-proportional record factors: acc.a = N·A, accw.a = N·B, accd = N·C
-    float A[4] = {ms * one_n, 0, 0, 0}, B[4] = {mw, 0, 0, 0}, C[3] = {0, 0, 0};
+    // force records, per node: σ̃ = -Ω (σ + σw I) by rows, σ̃w = -Ω σw
+    {
+        const float swv = -vol * sw;
+        float t[3][3];
+        if (D == 2) {
+            t[0][0] = -vol * s[0] + swv; t[0][1] = -vol * s[3]; t[0][2] = 0.0f;
+            t[1][0] = -vol * s[3]; t[1][1] = -vol * s[1] + swv; t[1][2] = 0.0f;
+            t[2][0] = t[2][1] = t[2][2] = 0.0f;
+        } else {
+            t[0][0] = -vol * s[0] + swv; t[0][1] = -vol * s[3]; t[0][2] = -vol * s[5];
+            t[1][0] = -vol * s[3]; t[1][1] = -vol * s[1] + swv; t[1][2] = -vol * s[4];
+            t[2][0] = -vol * s[5]; t[2][1] = -vol * s[4]; t[2][2] = -vol * s[2] + swv;
+        }
+        const int plane = g.nnx * g.nny;
+        constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-        A[1 + d] = ms * vs[d] * one_n;
-        B[1 + d] = mw * vw[d] * n;
-        C[d] = tdg * (vw[d] - vs[d]);
-    }
-    float A1[4], A2[4], B1[4], B2[4], C1[3], C2[3];
+        for (int c = 0; c < NC; ++c) {
+            const float wz = D == 3 ? w[2].N[c] : 1.0f, gz = D == 3 ? w[2].dN[c] : 0.0f;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        A1[k] = __shfl_up_sync(F, A[k], 1); A2[k] = __shfl_up_sync(F, A[k], 2);
-        B1[k] = __shfl_up_sync(F, B[k], 1); B2[k] = __shfl_up_sync(F, B[k], 2);
-    }
+            for (int a = 0; a < 3; ++a) {
+                const float wx = w[0].N[a], gx = w[0].dN[a];
+                const int col = n0 + a * g.nny + c * plane;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { C1[k] = __shfl_up_sync(F, C[k], 1); C2[k] = __shfl_up_sync(F, C[k], 2); }
-    // σ̃ = -Ω (σ + σw I) by rows, σ̃w = -Ω σw
-    const float swv = -vol * sw;
-    float t[3][3];
-    if (D == 2) {
-        t[0][0] = -vol * s[0] + swv; t[0][1] = -vol * s[3]; t[0][2] = 0.0f;
-        t[1][0] = -vol * s[3]; t[1][1] = -vol * s[1] + swv; t[1][2] = 0.0f;
-        t[2][0] = t[2][1] = t[2][2] = 0.0f;
-    } else {
-        t[0][0] = -vol * s[0] + swv; t[0][1] = -vol * s[3]; t[0][2] = -vol * s[5];
-        t[1][0] = -vol * s[3]; t[1][1] = -vol * s[1] + swv; t[1][2] = -vol * s[4];
-        t[2][0] = -vol * s[5]; t[2][1] = -vol * s[4]; t[2][2] = -vol * s[2] + swv;
-    }
-    const int plane = g.nnx * g.nny;
-    constexpr int NC = D == 3 ? 3 : 1;
+                for (int b = 0; b < 3; ++b) {
+                    const float wy = w[1].N[b], gy = w[1].dN[b];
+                    const float N = wx * wy * wz;
+                    if (N == 0.0f) continue;
+                    const float dN[3] = {gx * wy * wz, wx * gy * wz, wx * wy * gz};
+                    float fs[3], fw[3];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        const float wz = D == 3 ? w[2].N[c] : 1.0f, gz = D == 3 ? w[2].dN[c] : 0.0f;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float wx = w[0].N[a], gx = w[0].dN[a];
-            const int col = n0 + a * g.nny + c * plane;
-            float Nb[3];
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const float wy = w[1].N[b], gy = w[1].dN[b];
-                const float N = wx * wy * wz;
-                Nb[b] = N;
-                if (N == 0.0f) continue;
-                // force records, per node
-                const float dN[3] = {gx * wy * wz, wx * gy * wz, wx * wy * gz};
-                float fs[3], fw[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    fs[k] = dN[0] * t[k][0] + dN[1] * t[k][1] + dN[2] * t[k][2];
-                    fw[k] = k < D ? dN[k] * swv : 0.0f;
-                }
-                fs[D - 1] += N * mi * G;
-                fw[D - 1] += N * mw * G;
-                red_add4(&g.acc[col + b].b, fs[0], fs[1], fs[2], N * mwn);
-                red_add4(&g.accw[col + b].b, fw[0], fw[1], fw[2], 0.0f);
-            }
-            // N-proportional records: row 0 merged over the chain, rows 1, 2 by its last lane
-            const float u1 = __shfl_up_sync(F, Nb[1], 1), u2 = __shfl_up_sync(F, Nb[2], 2);
-            const float v2 = __shfl_up_sync(F, Nb[2], 1);
-            const float f1 = ch.c1 ? u1 : 0.0f, f2 = ch.c2 ? u2 : 0.0f, e1 = ch.c1 ? v2 : 0.0f;
-            if (Nb[0] + f1 + f2 != 0.0f) {
-                const float N0 = Nb[0];
-                red_add4(&g.acc[col].a, N0 * A[0] + f1 * A1[0] + f2 * A2[0], N0 * A[1] + f1 * A1[1] + f2 * A2[1],
-                         N0 * A[2] + f1 * A1[2] + f2 * A2[2], N0 * A[3] + f1 * A1[3] + f2 * A2[3]);
-                red_add4(&g.accw[col].a, N0 * B[0] + f1 * B1[0] + f2 * B2[0], N0 * B[1] + f1 * B1[1] + f2 * B2[1],
-                         N0 * B[2] + f1 * B1[2] + f2 * B2[2], N0 * B[3] + f1 * B1[3] + f2 * B2[3]);
-                red_add4(&g.accd[col], N0 * C[0] + f1 * C1[0] + f2 * C2[0], N0 * C[1] + f1 * C1[1] + f2 * C2[1],
-                         N0 * C[2] + f1 * C1[2] + f2 * C2[2], 0.0f);
-            }
-            if (ch.end) {
-                const float N1 = Nb[1], N2 = Nb[2];
-                if (N1 + e1 != 0.0f) {
-                    red_add4(&g.acc[col + 1].a, N1 * A[0] + e1 * A1[0], N1 * A[1] + e1 * A1[1], N1 * A[2] + e1 * A1[2],
-                             N1 * A[3] + e1 * A1[3]);
-                    red_add4(&g.accw[col + 1].a, N1 * B[0] + e1 * B1[0], N1 * B[1] + e1 * B1[1],
-                             N1 * B[2] + e1 * B1[2], N1 * B[3] + e1 * B1[3]);
-                    red_add4(&g.accd[col + 1], N1 * C[0] + e1 * C1[0], N1 * C[1] + e1 * C1[1], N1 * C[2] + e1 * C1[2],
-                             0.0f);
-                }
-                if (N2 != 0.0f) {
-                    red_add4(&g.acc[col + 2].a, N2 * A[0], N2 * A[1], N2 * A[2], N2 * A[3]);
-                    red_add4(&g.accw[col + 2].a, N2 * B[0], N2 * B[1], N2 * B[2], N2 * B[3]);
-                    red_add4(&g.accd[col + 2], N2 * C[0], N2 * C[1], N2 * C[2], 0.0f);
+                    for (int k = 0; k < 3; ++k) {
+                        fs[k] = dN[0] * t[k][0] + dN[1] * t[k][1] + dN[2] * t[k][2];
+                        fw[k] = k < D ? dN[k] * swv : 0.0f;
+                    }
+                    fs[D - 1] += N * mi * G;
+                    fw[D - 1] += N * mw * G;
+                    red_add4(&g.acc[col + b].b, fs[0], fs[1], fs[2], N * mwn);
+                    red_add4(&g.accw[col + b].b, fw[0], fw[1], fw[2], 0.0f);
                 }
             }
         }
+    }
+    // N-proportional records: acc.a = N·A, accw.a = N·B, accd = N·C
+    {
+        float A[4] = {ms * one_n, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int d = 0; d < D; ++d) A[1 + d] = ms * vs[d] * one_n;
+        chain_nprop<D, 4>(g, w, n0, ch, A, [&](int i) { return &g.acc[i].a; });
+    }
+    {
+        float B[4] = {mw, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int d = 0; d < D; ++d) B[1 + d] = mw * vw[d] * n;
+        chain_nprop<D, 4>(g, w, n0, ch, B, [&](int i) { return &g.accw[i].a; });
+    }
+    {
+        const float tdg = kperm != 0.0f ? (n * mw * G) / kperm : 0.0f;
+        float Cv[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int d = 0; d < D; ++d) Cv[d] = tdg * (vw[d] - vs[d]);
+        chain_nprop<D, 3>(g, w, n0, ch, Cv, [&](int i) { return &g.accd[i]; });
     }
 }
 
 // The fused two-phase pass (FP32) with the lane-merged scatter.
 template <int D, bool MC3 = false>
-__global__ void __launch_bounds__(256, 3) k_g2p_ts_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+__global__ void __launch_bounds__(256, MPM_TS_P_MINB) k_g2p_ts_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool live = i < sp.np;
     double x[3];
