@@ -206,6 +206,14 @@ BP_G2P_2D = 128
 BN_G2P_2D = 28         # Δu read (2 floats) + m, p, f written (5 floats)
 
 
+def advance_time(Ti, dt, n, f32):
+    """Ti after n steps, accumulated as the library does (in FP32 for the
+    reference's FP32 mode), so that the next call continues at the same time."""
+    for _ in range(n):
+        Ti = float(np.float32(np.float32(Ti) + np.float32(dt))) if f32 else Ti + dt
+    return Ti
+
+
 def run_b200(args):
     rank, world, local = dist_env()
     pkg, case = make_case(args.mc3d, args.workload, args.surrogate)
@@ -275,14 +283,12 @@ def run_b200(args):
         sur.set_norm(feat, tgt)
         losses = sur.train(feat, tgt, epochs=6, batch=16384, lr=3e-3, lr_end=1e-4)
         # the plain step on the same state, for comparison
-        dev.step(dt, Ti, 16)
+        Ti = dev.step(dt, Ti, 16)
         plain_ms = dev.stats().last_step_ms / 16
-        Ti += 16 * dt
         dev.set_surrogate(sur, tol=1e-3, sref=1e3)
         surr_info = {"plain_ms_per_step_same_state": plain_ms,"train_samples": int(feat.shape[0]), "epochs": 6, "loss_first_last": [losses[0], losses[-1]],
                      "setup_s": time.perf_counter() - t0, "tol": 1e-3, "sref_pa": 1e3}
-    dev.step(dt, Ti, W)
-    Ti += W * dt
+    Ti = dev.step(dt, Ti, W)
     if use_dist:
         dist.barrier()
     launches0 = dev.stats().launches
@@ -293,7 +299,7 @@ def run_b200(args):
     ms = st.last_step_ms
     launches = st.launches - launches0
     na = st.active_nodes
-    Ti += K * dt
+    Ti = advance_time(Ti, dt, K, dev.desc.time_f32)
     t_max = max_over_ranks(ms, f"cuda:{local}") if use_dist else ms
     value = replica_value(world, npart, K, t_max)
 

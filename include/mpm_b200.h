@@ -353,8 +353,10 @@ int mpm_get_stats(mpm_handle *h, mpm_stats *out);
 const char *mpm_last_error(mpm_handle *h);
 /* Triad bandwidth probe (Tpeak): bytes moved / best time, GB/s. */
 int mpm_peak_bandwidth(int32_t device, double *gbs_out);
-/* Average device time per launch of each kernel over the last timed mpm_step
- * (enabled by mpm_set_profiling): names and ms, up to `cap` entries. */
+/* Profiling mode (mpm_set_profiling): every launch of a mpm_step call is
+ * bracketed by events and waited for (no graph replay).  mpm_get_kernel_times
+ * returns, per kernel name, the average device time per launch (ms) and the
+ * launch count over the last mpm_step call, up to `cap` names. */
 int mpm_set_profiling(mpm_handle *h, int32_t on);
 int mpm_get_kernel_times(mpm_handle *h, const char **names, double *ms, int64_t *launches,
                          int32_t cap, int32_t *count);

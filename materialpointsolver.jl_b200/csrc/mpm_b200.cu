@@ -483,33 +483,41 @@ template <int D, typename R> void do_sort(mpm_handle *h) {
 }
 
 // ---- step --------------------------------------------------------------------------
+// Issues one pass.  In profiling mode each launch is bracketed by events on the
+// library stream and waited for, and its time is added to the per-kernel
+// totals under its name (the launch sequence of a call varies: the standalone
+// P2G, the sorts).
 struct Launcher {
     mpm_handle *h;
-    int idx = 0;
     template <typename F> void run(const char *name, F &&f) {
         if (h->profiling) {
-            if ((int)h->ktimes.size() <= idx) h->ktimes.push_back(KTimer{name});
-            if ((int)h->kev.size() < 2 * (idx + 1)) {
+            KTimer *kt = nullptr;
+            for (KTimer &k : h->ktimes)
+                if (std::strcmp(k.name, name) == 0) { kt = &k; break; }
+            if (!kt) {
+                h->ktimes.push_back(KTimer{name});
+                kt = &h->ktimes.back();
+            }
+            if (h->kev.size() < 2) {
                 cudaEvent_t a, b;
                 CK(cudaEventCreate(&a));
                 CK(cudaEventCreate(&b));
                 h->kev.push_back(a);
                 h->kev.push_back(b);
             }
-            CK(cudaEventRecord(h->kev[2 * idx], h->stream));
+            CK(cudaEventRecord(h->kev[0], h->stream));
             f();
             LAUNCH_CHECK();
-            CK(cudaEventRecord(h->kev[2 * idx + 1], h->stream));
-            CK(cudaEventSynchronize(h->kev[2 * idx + 1]));
+            CK(cudaEventRecord(h->kev[1], h->stream));
+            CK(cudaEventSynchronize(h->kev[1]));
             float ms = 0;
-            CK(cudaEventElapsedTime(&ms, h->kev[2 * idx], h->kev[2 * idx + 1]));
-            h->ktimes[idx].ms += ms;
-            h->ktimes[idx].n += 1;
+            CK(cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]));
+            kt->ms += ms;
+            kt->n += 1;
         } else {
             f();
             LAUNCH_CHECK();
         }
-        ++idx;
         ++h->launches;
     }
 };
@@ -783,8 +791,11 @@ template <int D, typename R> void run_steps(mpm_handle *h, double dt, double Ti0
     auto next_t = [&](double t) {
         return h->d.time_f32 ? (double)((float)t + (float)dt) : t + dt;
     };
-    bool ramp = h->d.Te > 0.0;
-    if (!h->acc_valid || (ramp && h->acc_Ti != Ti0)) {
+    // The nodal mass, momentum and force left by the last fused pass are the
+    // P2G of the current state with the gravity at acc_Ti, the only input of
+    // P2G that depends on time; they are redone when the caller's Ti gives
+    // another gravity (during the ramp Ti < Te).
+    if (!h->acc_valid || gravity_at(h->d, h->acc_Ti) != gravity_at(h->d, Ti0)) {
         if (h->since_sort >= h->sort_every) do_sort<D, R>(h);
         standalone_p2g<D, R>(h, Ti0, L);
     }

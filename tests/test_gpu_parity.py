@@ -221,6 +221,55 @@ def test_gravity_ramp(pkg, orc, gpu_lib):
     check_fields(out, o, case.mp, TOL64)
 
 
+def test_ramp_in_chunks(pkg, orc, gpu_lib):
+    """The P2G a fused pass leaves behind is reused by the next mpm_step call
+    when the caller's Ti gives the same gravity, and redone when it does not
+    (inside the ramp Ti < Te every Ti has its own gravity).  Chunked calls
+    across the ramp match the oracle's single run, and the standalone P2G runs
+    exactly where the rule says."""
+    Te = 0.5 * 1e-3
+    case = small2d(pkg, constitutive="druckerprager", gpu_precision="fp64", Te=Te, Ttol=1.0)
+
+    def stepper(dev):
+        runs = [0]
+
+        def step(Ti, n):
+            Ti = dev.step(case.dt, Ti, n)
+            kt = dev.kernel_times()
+            runs[0] += kt.get("p2g", (0.0, 0))[1]
+            assert kt["g2p_p2g"][1] == n
+            return Ti
+        return step, runs
+
+    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+    try:
+        dev.set_profiling(True)
+        step, runs = stepper(dev)
+        Ti = step(0.0, 5)
+        assert runs[0] == 1
+        for _ in range(3):                      # continuing at the returned Ti
+            Ti = step(Ti, 5)
+        assert runs[0] == 1 and Ti > Te
+        out = fresh_particles(pkg, case.mp)
+        dev.download(pkg._lib.F_REFERENCE | pkg._lib.F_F, out)
+        step(Ti * (1 + 1e-12), 2)               # past the ramp: same gravity, reused
+        assert runs[0] == 1
+    finally:
+        dev.close()
+    o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc)
+    o.run(case.dt, 0.0, 20)
+    check_fields(out, o, case.mp, TOL64)
+    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+    try:
+        dev.set_profiling(True)
+        step, runs = stepper(dev)
+        Ti = step(0.0, 3)
+        step(Ti * (1 + 1e-12), 3)               # inside the ramp: another gravity, redone
+        assert runs[0] == 2
+    finally:
+        dev.close()
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_p2g_stage(pkg, orc, gpu_lib, dim):
     mk = small2d if dim == 2 else small3d
