@@ -150,11 +150,13 @@ def make_case(mc3d, workload="column3d", surrogate=False):
     import __graft_entry__ as g
     pkg = g.load_package()
     if workload == "slope3d":
-        # with the surrogate the run starts in the plastic regime (no gravity
-        # ramp), so that the timed steps exercise the return it replaces
-        case = pkg.workloads.slope_3d(Te=0.0) if surrogate else pkg.workloads.slope_3d()
+        # the run starts in the plastic regime (no gravity ramp: during the
+        # ramp Ti < Te the reference skips the return mapping), so that the
+        # timed steps carry the Drucker-Prager return -- and, with the
+        # surrogate, the return it replaces
+        case = pkg.workloads.slope_3d(Te=0.0)
     elif workload == "batch2d":
-        case = pkg.workloads.slope_batch_2d()
+        case = pkg.workloads.slope_batch_2d(Te=0.0)   # plastic regime, as above
     elif workload == "column2d":
         case = pkg.workloads.column_collapse_2d(gpu_precision="fp64")
     elif workload == "saturated3d":
