@@ -460,6 +460,42 @@ def collapse_2d_validation(*, precision="FP64", gpu_precision="mixed", Ttol=1.0,
     return Case("collapse_2d_validation", args, grid, mp, attr, bc, dt, nsteps, dict(np=npart, h=h, K=K, G=G, seed=0))
 
 
+def cantilever_2d(*, precision="FP64", gpu_precision="fp64", Ttol=3.0, dt=1e-4, constitutive="linearelastic",
+                  project_path="/tmp", **extra):
+    """The reference's 2D cantilever beam (test/c1_accuracy/t1_cantilever_beam/
+    2d_cantilever_beam.jl): a 4 x 1 m beam (E = 1 MPa, ν = 0.3, ρ = 1050) on a
+    0.25 m grid over [-3, 8] x [-8, 4], 3 x 3 particles per cell, clamped where
+    nodes have x <= 0 and y >= -1 (both velocity components fixed), gravity
+    -9.8, Δt = 1e-4, 3 s, MUSL, FLIP 1.  The reference runs it with its
+    Neo-Hookean model and plots the deflection of the bottom corner particle at
+    the free end against FEM and MPM curves it ships; this backend provides the
+    linear elastic model (with the Jaumann rotation of liE!).  meta["tip"] is
+    that particle's index."""
+    h, E, nu, rho = 0.25, 1.0e6, 0.3, 1050.0
+    K, G = elastic_constants(E, nu)
+    lp = h / 3
+    pts = meshbuilder(jl_range(lp / 2, lp, 4.0 - lp / 2), jl_range(lp / 2, lp, 1.0 - lp / 2))
+    npart = pts.shape[0]
+    akw = dict(Ttol=Ttol, Te=0, ΔT=dt, FLIP=1, PIC=0, constitutive=constitutive, basis="uGIMP",
+               device="B200", coupling="OS", scheme="MUSL", va="a", gravity=-9.8, ζs=0,
+               project_name="2d_cantilever_beam", project_path=project_path, ϵ=precision,
+               gpu_precision=gpu_precision, make_project_dir=False)
+    akw.update(extra)
+    args = UserArgs2D(**akw)
+    grid = UserGrid2D(ϵ=precision, x1=-3.0, x2=8.0, y1=-8.0, y2=4.0, dx=h, dy=h, NIC=9)
+    mp = UserParticle2D(ϵ=precision, NIC=9, dx=lp, dy=lp, ξ=pts, ρs=np.full(npart, rho))
+    attr = UserProperty(ϵ=precision, nid=np.ones(npart, np.int64), ν=[nu], Es=[E], Gs=[G], Ks=[K],
+                        σt=[0.0], ϕ=[0.0], ϕr=[0.0], ψ=[0.0], c=[0.0], cr=[0.0], Hp=[0.0])
+    gx, gy = grid.xi[:, 0], grid.xi[:, 1]
+    clamp = ((gx <= 0.0) & (gy >= -1.0)).astype(np.int64)
+    bc = UserVBoundary2D(ϵ=precision, vx_s_idx=clamp, vx_s_val=np.zeros(grid.ni), vy_s_idx=clamp.copy(),
+                         vy_s_val=np.zeros(grid.ni))
+    low = pts[:, 1] == pts[:, 1].min()
+    tip = int(np.nonzero(low & (pts[:, 0] == pts[low, 0].max()))[0][0])
+    nsteps = int(round(Ttol / dt))
+    return Case("cantilever_2d", args, grid, mp, attr, bc, dt, nsteps, dict(np=npart, h=h, K=K, G=G, tip=tip))
+
+
 def free_surface(xi, x_edges):
     """Height of the deposit per x bin: the highest particle in each bin
     (NaN for empty bins)."""

@@ -5,12 +5,20 @@ surface against the laboratory surface MaterialPointSolver.jl ships for that
 case (tests/golden/collapse_2d_experiment.json, made by make_collapse_experiment.py).
 
 Measured on B200: mean |Δh| 1.0 mm over 0 <= x < 0.4 m (heights up to 100 mm),
-max 2.9 mm, in both the FP64 and the mixed mode."""
+max 2.9 mm, in both the FP64 and the mixed mode.
+
+Also: the reference's 2D cantilever beam (test/c1_accuracy/t1_cantilever_beam/
+2d_cantilever_beam.jl) against the FEM and MPM tip-deflection curves it ships
+(tests/golden/cantilever_2d_curves.json, made by make_cantilever_curves.py),
+through the oracle on CPU and the device on GPU; and the two-phase saturated
+column against hydrostatics."""
 import json
 import os
 
 import numpy as np
 import pytest
+
+from helpers import fresh_particles
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "collapse_2d_experiment.json")
 
@@ -96,3 +104,96 @@ def test_saturated_column_consolidates_to_hydrostatic(pkg, gpu_lib, prec, tmp_pa
     assert abs(syy / buoyant - 1) < 0.02, syy
     assert abs(sxx / syy - nu / (1 - nu)) < 0.05, sxx / syy
     assert np.abs(c.mp.vs).max() < 0.02 and np.abs(c.mp.vw).max() < 0.05
+
+
+# ---- the reference's 2D cantilever beam (test/c1_accuracy/t1_cantilever_beam) ----
+
+CANTILEVER = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "cantilever_2d_curves.json")
+
+
+def cantilever_curves():
+    with open(CANTILEVER) as fh:
+        d = json.load(fh)
+    return {k: np.array(d[k]) for k in ("fem", "ugimp", "cpdi")}
+
+
+def tip_track(step_and_read, case, chunks=100):
+    """(time, vertical displacement of the bottom corner particle at the free
+    end) every Ttol/chunks."""
+    n = case.nsteps_full // chunks
+    tip = case.meta["tip"]
+    y0 = case.mp.xi[tip, 1]
+    out, Ti = [], 0.0
+    for _ in range(chunks):
+        Ti, xi = step_and_read(Ti, n)
+        out.append((Ti, xi[tip, 1] - y0))
+    return np.array(out)
+
+
+def deviation(track, curve):
+    m = track[:, 0] <= curve[:, 0].max()
+    ref = np.interp(track[m, 0], curve[:, 0], curve[:, 1])
+    d = np.abs(track[m, 1] - ref)
+    return d.mean(), d.max()
+
+
+@pytest.fixture(scope="module")
+def cantilever_oracle(pkg, orc):
+    """The FP64 oracle's tip track of the cantilever (30 000 steps, ~7 s)."""
+    c = pkg.workloads.cantilever_2d()
+    o = orc.Oracle(c.args, c.grid, c.mp, c.attr, c.bc)
+
+    def step_and_read(Ti, n):
+        for _ in range(n):      # time accumulated step by step, as the library does
+            o.procedure(c.dt, Ti)
+            Ti += c.dt
+        return Ti, o.xi
+
+    return tip_track(step_and_read, c)
+
+
+def check_cantilever_physics(track):
+    curves = cantilever_curves()
+    # the published uGIMP MPM curve: the same method
+    mean, mx = deviation(track, curves["ugimp"])
+    assert mean < 0.12 and mx < 0.35, (mean, mx)
+    # the FEM solution (Neo-Hookean); the hypoelastic beam returns a little later
+    mean, mx = deviation(track, curves["fem"])
+    assert mean < 0.25 and mx < 0.8, (mean, mx)
+    peak = track[:, 1].min()
+    assert abs(peak / curves["fem"][:, 1].min() - 1) < 0.03, peak
+    assert abs(peak / curves["ugimp"][:, 1].min() - 1) < 0.03, peak
+    # the first swing reaches its lowest point between 0.9 and 1.2 s, as in both references
+    t_low = track[np.argmin(track[:track.shape[0] // 2, 1]), 0]
+    assert 0.9 < t_low < 1.2, t_low
+
+
+def test_oracle_cantilever_matches_published_curves(cantilever_oracle):
+    """The oracle (the reference's linear elastic model with its Jaumann
+    rotation, liE!) on the reference's cantilever case against the FEM and MPM
+    curves the reference ships: peak deflection -3.305 m against -3.28 (FEM) and
+    -3.243 (uGIMP); mean deviation from the uGIMP curve 7.7 cm over 3 s."""
+    check_cantilever_physics(cantilever_oracle)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-3)])
+def test_cantilever_device_matches_oracle_and_curves(pkg, gpu_lib, cantilever_oracle, prec, tol):
+    """The same case on the device, stepped in 100 calls with a download each:
+    its tip track against the oracle's (measured on B200: 1e-14 m in FP64,
+    3e-5 m in mixed mode over 30 000 steps) and against the published curves."""
+    c = pkg.workloads.cantilever_2d(gpu_precision=prec)
+    dev = pkg.DeviceModel(c.args, c.grid, c.mp, c.attr, c.bc)
+    try:
+        def step_and_read(Ti, n):
+            Ti = dev.step(c.dt, Ti, n)
+            out = fresh_particles(pkg, c.mp)
+            dev.download(pkg._lib.F_XI, out)
+            return Ti, out.xi
+
+        track = tip_track(step_and_read, c)
+    finally:
+        dev.close()
+    assert np.abs(track[:, 0] - cantilever_oracle[:, 0]).max() < 1e-12
+    assert np.abs(track[:, 1] - cantilever_oracle[:, 1]).max() < tol
+    check_cantilever_physics(track)
