@@ -550,6 +550,9 @@ template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, do
     sp.mvl = h->d.mvl ? 1 : 0;
     sp.ts = h->ts ? 1 : 0;
     sp.zeta_w = h->d.zeta_w;
+    // massless-node cutoff m < eps(T2) of the solves (utils_OS.jl:515, 555, 975): T2
+    // is the reference's float type (the user's ϵ), whatever the device stores
+    sp.meps = h->d.time_f32 ? 1.1920928955078125e-07 : 2.220446049250313e-16;
     sp.surr = h->surr;
     sp.surr.mode = (D == 3 && h->d.constitutive == MPM_DRUCKERPRAGER && !h->ts) ? h->surr_mode : 0;
     sp.surr.salt = (uint32_t)(h->steps_done * 0x9E3779B9ull);

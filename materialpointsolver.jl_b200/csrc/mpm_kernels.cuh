@@ -243,6 +243,7 @@ struct StepParams {
     int prefetch;    // FP32 particle pass: fields staged in dynamic shared memory (PF_N x 256 floats)
     int ts;          // two-phase coupling (TS_MUSL.jl)
     double zeta_w;   // ζw, water damping (two-phase)
+    double meps;     // nodal mass below which a node is massless: eps of the reference's float type
     SurrCtx surr;
     int64_t np;
 };
@@ -410,7 +411,7 @@ __device__ __forceinline__ void solve_node(const GDev<R> &g, const StepParams &s
             return;
         }
     }
-    const R eps = sizeof(R) == 8 ? R(2.220446049250313e-16) : R(1.1920929e-7);
+    const R eps = (R)sp.meps;
     R m = a0.x;
     R md = m < eps ? R(0) : R(1) / m;
     R p[3] = {a0.y, a0.z, a0.w};
@@ -846,7 +847,7 @@ __device__ __forceinline__ void dm3_node(const GDev<R> &g, const StepParams &sp,
         g.gat[i].b = mk4<R>(0, 0, 0, 0);
         return;
     }
-    const R eps = sizeof(R) == 8 ? R(2.220446049250313e-16) : R(1.1920929e-7);
+    const R eps = (R)sp.meps;
     R md = a0.x < eps ? R(0) : R(1) / a0.x;
     R p[3] = {a0.y, a0.z, a0.w};
     R bv[3] = {R(0), R(0), R(0)};

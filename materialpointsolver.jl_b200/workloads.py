@@ -460,6 +460,46 @@ def collapse_2d_validation(*, precision="FP64", gpu_precision="mixed", Ttol=1.0,
     return Case("collapse_2d_validation", args, grid, mp, attr, bc, dt, nsteps, dict(np=npart, h=h, K=K, G=G, seed=0))
 
 
+def collapse_3d_validation(*, precision="FP64", gpu_precision="mixed", Ttol=1.0, project_path="/tmp", **extra):
+    """The reference's 3D granular column validation case (test/validation/3d_case.jl):
+    the 2D case as a 0.05 m thick slab -- a 0.05 x 0.2 x 0.1 m column (x across,
+    y along the flume, z up) of sand (K = 7e5 Pa, ν = 0.3, ρ = 2650,
+    Drucker-Prager φ = 19.8°, c = 0) on a 2.5 mm grid over [-0.02, 0.07] x
+    [-0.02, 0.75] x [-0.02, 0.12], 2 x 2 x 2 particles per cell (512 000
+    particles), USL scheme, free-slip side walls at x <= 0 and x >= 0.05, a wall
+    at y <= 0 (x and y fixed), a rough floor at z <= 0 (all fixed), gravity
+    -9.8, Δt = 0.5 h / sqrt(E/ρ), 1 s."""
+    h = 0.0025
+    K, nu, rho = 7e5, 0.3, 2650.0
+    E = K * (3.0 * (1.0 - 2.0 * nu))
+    G = E / (2.0 * (1.0 + nu))
+    dt = 0.5 * h / math.sqrt(E / rho)
+    lp = h / 2
+    pts = meshbuilder(jl_range(lp / 2, lp, 0.05 - lp / 2), jl_range(lp / 2, lp, 0.2 - lp / 2),
+                      jl_range(lp / 2, lp, 0.1 - lp / 2))
+    npart = pts.shape[0]
+    akw = dict(Ttol=Ttol, Te=0, ΔT=dt, FLIP=1, PIC=0, constitutive="druckerprager", basis="uGIMP",
+               device="B200", coupling="OS", scheme="USL", va="a", gravity=-9.8, ζs=0,
+               project_name="collapse3d_validation", project_path=project_path, ϵ=precision,
+               gpu_precision=gpu_precision, make_project_dir=False)
+    akw.update(extra)
+    args = UserArgs3D(**akw)
+    grid = UserGrid3D(ϵ=precision, x1=-0.02, x2=0.07, y1=-0.02, y2=0.75, z1=-0.02, z2=0.12, dx=h, dy=h, dz=h,
+                      NIC=27)
+    mp = UserParticle3D(ϵ=precision, NIC=27, dx=lp, dy=lp, dz=lp, ξ=pts, ρs=np.full(npart, rho))
+    attr = UserProperty(ϵ=precision, nid=np.ones(npart, np.int64), ν=[nu], Es=[E], Gs=[G], Ks=[K],
+                        σt=[0.0], ϕ=[math.radians(19.8)], ϕr=[0.0], ψ=[0.0], c=[0.0], cr=[0.0], Hp=[0.0])
+    gx, gy, gz = grid.xi[:, 0], grid.xi[:, 1], grid.xi[:, 2]
+    vx = ((gx <= 0.0) | (gx >= 0.05) | (gz <= 0.0) | (gy <= 0.0)).astype(np.int64)
+    vy = ((gy <= 0.0) | (gz <= 0.0)).astype(np.int64)
+    vz = (gz <= 0.0).astype(np.int64)
+    z = np.zeros(grid.ni)
+    bc = UserVBoundary3D(ϵ=precision, vx_s_idx=vx, vx_s_val=z, vy_s_idx=vy, vy_s_val=z.copy(), vz_s_idx=vz,
+                         vz_s_val=z.copy())
+    nsteps = int(math.ceil(Ttol / dt))
+    return Case("collapse_3d_validation", args, grid, mp, attr, bc, dt, nsteps, dict(np=npart, h=h, K=K, G=G, seed=0))
+
+
 def cantilever_2d(*, precision="FP64", gpu_precision="fp64", Ttol=3.0, dt=1e-4, constitutive="linearelastic",
                   project_path="/tmp", **extra):
     """The reference's 2D cantilever beam (test/c1_accuracy/t1_cantilever_beam/

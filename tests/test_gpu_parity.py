@@ -293,6 +293,34 @@ def test_p2g_stage(pkg, orc, gpu_lib, dim):
     assert rel(f_g, o.g_fs) < 1e-12
 
 
+@pytest.mark.parametrize("user_precision,cut", [("FP64", False), ("FP32", True)])
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_massless_cutoff_follows_reference_precision(pkg, gpu_lib, prec, user_precision, cut):
+    """The solve treats a node as massless when m < eps(T2), T2 the reference's
+    float type (utils_OS.jl:515, 555): with FP64 inputs a node of ~1e-9 kg moves
+    with its momentum, with FP32 inputs it is cut (velocity 0) -- whatever the
+    device stores.  (Cutting at FP32's eps in the mixed mode of an FP64 problem
+    froze the light boundary nodes of the reference's 3D validation column,
+    2.5 mm cells, and the USL run blew up.)"""
+    case = small2d(pkg, constitutive="linearelastic", gpu_precision=prec, precision=user_precision, rho=1e-4,
+                   gravity=0.0)
+    case.mp.vs[:, 0] = 1.0
+    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+    try:
+        dev.run_stages(case.dt, 0.0, 1 | 2)          # P2G, solve
+        m = dev.grid_field(0)
+        vT = dev.grid_field(3)
+    finally:
+        dev.close()
+    free = (m > 0) & (case.bc.vx_s_idx == 0) & (case.bc.vy_s_idx == 0)
+    assert free.sum() > 20
+    assert m[free].max() < 1e-7 and m[free].min() > 1e-15
+    if cut:
+        assert not vT[free].any()
+    else:
+        assert np.allclose(vT[free, 0], 1.0, rtol=1e-5) and np.allclose(vT[free, 1], 0.0, atol=1e-6)
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_p2c_bit_exact(pkg, orc, gpu_lib, dim):
     mk = small2d if dim == 2 else small3d
