@@ -27,6 +27,10 @@ namespace {
 
 inline double sgn(double x) { return (x > 0.0) - (x < 0.0); }   // Julia sign()
 
+// eps(T2) of the solves' massless-node cutoff (utils_OS.jl:515, 555, 975), T2
+// the reference's float type
+inline double mass_eps(const orc_model *m) { return m->f32 ? (double)FLT_EPSILON : DBL_EPSILON; }
+
 // Julia `mod(x, y)` for floats (base/float.jl): r = rem(x,y); fix sign to y's.
 inline double jl_mod(double x, double y) {
     double r = std::fmod(x, y);
@@ -282,7 +286,7 @@ void orc_solvegrid(orc_model *m, double dt) {
     const double *val[3] = {m->vx_val, m->vy_val, m->vz_val};
 #pragma omp parallel for if (par(m)) schedule(static)
     for (int64_t i = 0; i < ni; ++i) {
-        double ms_denom = m->g_ms[i] < DBL_EPSILON ? 0.0 : 1.0 / m->g_ms[i];
+        double ms_denom = m->g_ms[i] < mass_eps(m) ? 0.0 : 1.0 / m->g_ms[i];
         if (m->va == ORC_VA_A) {
             for (int d = 0; d < D; ++d)
                 if (idx[d][i] != 0) m->g_ps[i + ni * d] = val[d][i];
@@ -332,7 +336,7 @@ void orc_solvegrid_usl(orc_model *m, double dt) {
     const double *val[3] = {m->vx_val, m->vy_val, m->vz_val};
 #pragma omp parallel for if (par(m)) schedule(static)
     for (int64_t i = 0; i < ni; ++i) {
-        double ms_denom = m->g_ms[i] < DBL_EPSILON ? 0.0 : 1.0 / m->g_ms[i];
+        double ms_denom = m->g_ms[i] < mass_eps(m) ? 0.0 : 1.0 / m->g_ms[i];
         double ss = 0.0;
         for (int d = 0; d < D; ++d) ss += m->g_fs[i + ni * d] * m->g_fs[i + ni * d];
         const double dampvs = -m->zeta_s * std::sqrt(ss);
@@ -431,7 +435,7 @@ void orc_dm3(orc_model *m, double dt) {
     const double *val[3] = {m->vx_val, m->vy_val, m->vz_val};
 #pragma omp parallel for if (par(m)) schedule(static)
     for (int64_t i = 0; i < ni; ++i) {
-        double ms_denom = m->g_ms[i] < DBL_EPSILON ? 0.0 : 1.0 / m->g_ms[i];
+        double ms_denom = m->g_ms[i] < mass_eps(m) ? 0.0 : 1.0 / m->g_ms[i];
         for (int d = 0; d < D; ++d) m->g_vs[i + ni * d] = m->g_ps[i + ni * d] * ms_denom;
         for (int d = 0; d < D; ++d)
             if (idx[d][i] != 0) m->g_vs[i + ni * d] = val[d][i];

@@ -61,7 +61,7 @@ typedef struct {
     int32_t scheme;             /* 0: MUSL (OS_MUSL.jl), 1: USL (OS_USL.jl) */
     /* ---- two-phase coupling (:TS, src/solvers/TS_MUSL.jl, utils_TS.jl) ---- */
     int32_t coupling;           /* 0: :OS, 1: :TS */
-    int32_t pad_ts;
+    int32_t f32;                /* 1: the reference's float type T2 is Float32 (massless-node cutoff eps(T2)) */
     double zeta_w;              /* ζw */
     double *g_mi, *g_mw;        /* ni */
     double *g_pw, *g_fw, *g_fd, *g_vw, *g_vwT, *g_aw, *g_duw; /* ni x dim */

@@ -53,7 +53,7 @@ class OrcModel(C.Structure):
         ("zeta_s", C.c_double),
         ("constitutive", C.c_int32), ("va", C.c_int32), ("mvl", C.c_int32), ("mc3d", C.c_int32),
         ("nthreads", C.c_int32), ("scheme", C.c_int32),
-        ("coupling", C.c_int32), ("pad_ts", C.c_int32), ("zeta_w", C.c_double),
+        ("coupling", C.c_int32), ("f32", C.c_int32), ("zeta_w", C.c_double),
         ("g_mi", _dp), ("g_mw", _dp),
         ("g_pw", _dp), ("g_fw", _dp), ("g_fd", _dp), ("g_vw", _dp), ("g_vwT", _dp), ("g_aw", _dp),
         ("g_duw", _dp),
@@ -218,6 +218,7 @@ class Oracle:
         m.scheme = 1 if getattr(args, "scheme", "MUSL") == "USL" else 0
         m.coupling = 1 if ts else 0
         m.zeta_w = getattr(args, "zeta_w", 0.0)
+        m.f32 = 1 if getattr(args, "precision", "FP64") == "FP32" else 0
         self.m = m
 
     def __getattr__(self, name):

@@ -172,7 +172,8 @@ class PyModel:
                     self.gfs[n, 0] += -vol * (dx * sg[ix, 0] + dy * sg[ix, 3] + dz * sg[ix, 5])
                     self.gfs[n, 1] += -vol * (dy * sg[ix, 1] + dx * sg[ix, 3] + dz * sg[ix, 4])
                     self.gfs[n, 2] += -vol * (dz * sg[ix, 2] + dx * sg[ix, 5] + dy * sg[ix, 4]) + NiM * G
-        eps = np.finfo(np.float64).eps
+        # eps(T2), T2 the reference's float type (utils_OS.jl:515, 555)
+        eps = float(np.finfo(np.float32 if getattr(a, "precision", "FP64") == "FP32" else np.float64).eps)
         if getattr(a, "scheme", "MUSL") == "USL":
             self._usl_a(dt, eps)
         else:
