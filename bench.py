@@ -42,12 +42,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mc3d", default="literal", choices=["literal", "restated"])
     ap.add_argument("--workload", default="column3d",
-                    choices=["column3d", "slope3d", "batch2d", "column2d", "saturated3d"],
+                    choices=["column3d", "slope3d", "batch2d", "column2d", "saturated3d", "example3d"],
                     help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
                          "3D slope with a lognormal cohesion field; batch2d: 256 independent 2D slopes "
                          "(15.5 M particles) advanced together, autotuned during warm-up; column2d: the 3 200-"
                          "particle 2D column in FP64 (launch-bound; CUDA graph replay); saturated3d: the 2.56 M-particle column "
-                         "as a two-phase (solid + water) saturated soil, coupling TS")
+                         "as a two-phase (solid + water) saturated soil, coupling TS; example3d: the reference's "
+                         "own 3D example (512 000 particles, MVL on), against its published 66.3 it/s")
     ap.add_argument("--surrogate", action="store_true",
                     help="slope3d: train the stress-return surrogate on samples logged from plain steps "
                          "(untimed) and time steps with it")
@@ -143,7 +144,13 @@ WORKLOADS = {
                  "constitutive": "druckerprager"},
     "saturated3d": {"workload": "3D saturated soil column collapse, two-phase (coupling TS), uGIMP, MUSL",
                     "constitutive": "druckerprager"},
+    "example3d": {"workload": "the reference's 3D column-collapse example (examples/3d_collapse.ipynb), uGIMP, "
+                              "MUSL va=:a, MVL on", "constitutive": "druckerprager"},
 }
+
+# The reference's published throughput for the example3d case: 66.3 it/s with
+# 512 000 particles, FP64, on an unstated NVIDIA GPU (examples/3d_collapse.ipynb:381).
+EXAMPLE3D_PUBLISHED = 66.3 * 512000
 
 
 def make_case(mc3d, workload="column3d", surrogate=False):
@@ -159,6 +166,8 @@ def make_case(mc3d, workload="column3d", surrogate=False):
         case = pkg.workloads.slope_batch_2d(Te=0.0)   # plastic regime, as above
     elif workload == "column2d":
         case = pkg.workloads.column_collapse_2d(gpu_precision="fp64")
+    elif workload == "example3d":
+        case = pkg.workloads.collapse_3d_example()
     elif workload == "saturated3d":
         case = pkg.workloads.saturated_column(dim=3, h=0.005, size=(0.5, 0.2, 0.4), box=(1.2, 0.4, 0.6),
                                               constitutive="druckerprager", seed=1002)
@@ -214,6 +223,23 @@ def advance_time(Ti, dt, n, f32):
     for _ in range(n):
         Ti = float(np.float32(np.float32(Ti) + np.float32(dt))) if f32 else Ti + dt
     return Ti
+
+
+def fp64_device_rate(pkg, device, K, W):
+    """The example3d case with every device array in FP64 (the precision of
+    the published number): W untimed steps, then K steps timed with CUDA events."""
+    case = pkg.workloads.collapse_3d_example(gpu_precision="fp64")
+    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=device)
+    try:
+        Ti = dev.step(case.dt, 0.0, W)
+        dev.step_async(case.dt, Ti, K)
+        dev.sync()
+        ms = dev.stats().last_step_ms
+    finally:
+        dev.close()
+    value = case.mp.np * K / (ms * 1e-3)
+    return {"value": value, "unit": "particle-updates/s", "ms_per_step": ms / K,
+            "vs_baseline": value / EXAMPLE3D_PUBLISHED}
 
 
 def run_b200(args):
@@ -323,6 +349,10 @@ def run_b200(args):
         # surrogate steps run G2P and P2G as two passes around the MLP
         dom = "g2p+p2g"
         dom_ms = kt["g2p"][0] + kt["p2g"][0]
+    elif dom not in kt and "g2p" in kt and "mvl_p2g" in kt:
+        # MVL: G2P + update + cell sums, then the cell-averaged stress + P2G
+        dom = "g2p+mvl_p2g"
+        dom_ms = kt["g2p"][0] + kt["mvl_p2g"][0]
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -368,6 +398,12 @@ def run_b200(args):
                 "what": "DeviceModel upload from pinned host arrays + K steps + device2host! field set"},
         "clocks": clk.summary(),
     }
+    if args.workload == "example3d":
+        result["vs_baseline"] = value / EXAMPLE3D_PUBLISHED
+        result["baseline"] = {"value": EXAMPLE3D_PUBLISHED, "unit": "particle-updates/s",
+                              "source": "examples/3d_collapse.ipynb:381: 66.3 it/s x 512 000 particles, FP64, "
+                                        "unstated NVIDIA GPU"}
+        result["fp64_device"] = fp64_device_rate(pkg, local, K, W)
     if args.snapshot_every > 0:
         result["snapshots"] = snapshot_cost(pkg, case, dt, K, args.snapshot_every, local)
     if rank == 0 and not args.no_cpu_baseline:
