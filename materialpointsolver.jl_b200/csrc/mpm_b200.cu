@@ -665,7 +665,15 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
                 if (mc3) k_g2p<D, R, false, D == 3, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
                 else k_g2p<D, R, false, false, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
             });
-            L.run("mvl_p2g", [&] { k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+            L.run("mvl_p2g", [&] {
+                if constexpr (std::is_same<R, float>::value) {
+                    if (h->chain) {
+                        k_mvl_p2g_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                        return;
+                    }
+                }
+                k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            });
         } else {
             L.run("g2p_p2g", [&] {
                 if constexpr (std::is_same<R, float>::value) {
@@ -681,7 +689,17 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         }
     } else if (sp.mvl && np) {
         // MVL: update + cell sums, then the cell-averaged mean stress + P2G
-        L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        // (FP32: the scatters of chained lanes merged, as in the default passes)
+        const bool chain = h->chain && std::is_same<R, float>::value;
+        L.run("dmap", [&] {
+            if constexpr (std::is_same<R, float>::value) {
+                if (chain) {
+                    k_dmap_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    return;
+                }
+            }
+            k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+        });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         CK(cudaMemsetAsync(h->csigm, 0, (size_t)h->nc * sizeof(R), h->stream));
@@ -690,7 +708,15 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
             if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
             else k_g2p<D, R, false><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
         });
-        L.run("mvl_p2g", [&] { k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("mvl_p2g", [&] {
+            if constexpr (std::is_same<R, float>::value) {
+                if (chain) {
+                    k_mvl_p2g_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    return;
+                }
+            }
+            k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+        });
     } else if (sp.surr.mode == 2 && sp.plastic && np) {
         // surrogate: G2P + update with the yielding particles' returns deferred,
         // the MLP over the deferred rows, accept-or-fallback, then the scatter

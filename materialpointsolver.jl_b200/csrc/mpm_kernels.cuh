@@ -1296,6 +1296,55 @@ __global__ void __launch_bounds__(256) k_mvl_p2g(PDev<D, R> P, GDev<R> g, StepPa
     p2g_scatter<D, R>(g, w, P.m[i], P.vol[i], v, s, (R)sp.G);
 }
 
+// The same pass (FP32) with the scatters of chained lanes merged (p2g_scatter_chain).
+template <int D>
+__global__ void __launch_bounds__(256) k_mvl_p2g_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool live = i < sp.np;
+    constexpr int NV = PDev<D, float>::NV;
+    float s[6] = {0, 0, 0, 0, 0, 0}, v[3] = {0, 0, 0}, m = 0.0f, vol = 0.0f;
+    AxisW<float> w[3];
+    if (live) {
+        const uint32_t c = g.pcell[i];
+        const float cm = g.csigm[c] / g.comega[c];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s[k] = P.sig[k][i];
+        const float sm = (s[0] + s[1] + s[2]) * 0.333333f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            s[k] = (s[k] - sm) + cm;
+            P.sig[k][i] = s[k];
+        }
+        double x[3];
+        load_x<D, float>(P, i, x);
+        if (!particle_weights<D, float>(x, g, w)) {
+            atomicOr(g.err, ERR_OOG);
+            live = false;
+        } else {
+            v[0] = P.v[0][i]; v[1] = P.v[1][i];
+            if (D == 3) v[2] = P.v[2][i];
+            m = P.m[i];
+            vol = P.vol[i];
+        }
+    }
+    int n0 = 0, key = dead_key();
+    if (live) {
+        n0 = key = window_n0<D, float>(g, w);
+    } else {
+        m = vol = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            w[a].base = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+        }
+    }
+    MarkState mk;
+    if (live) mk = mark_begin<D, float>(g, w);
+    p2g_scatter_chain<D>(g, w, n0, key, m, vol, v, s, (float)sp.G);
+    if (live) mark_end<float>(g, mk);
+}
+
 // Finish the deferred returns: accept the surrogate's stress when its yield
 // residual |f(s_hat)| / max(kphi, |qphi s_hat_m|, s_ref) is within tol (f of the
 // branch the trial stress takes: the shear cone, or the tension cut-off

@@ -464,19 +464,20 @@ def test_graph_replay_matches_direct_launches(pkg, orc, gpu_lib, dim, monkeypatc
     check_fields(outs[0], o, case.mp, TOL64)
 
 
+@pytest.mark.parametrize("mvl", [False, True])
 @pytest.mark.parametrize("scheme", ["MUSL", "USL"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_lane_merged_scatter_matches_plain(pkg, orc, gpu_lib, dim, scheme, monkeypatch):
+def test_lane_merged_scatter_matches_plain(pkg, orc, gpu_lib, dim, scheme, mvl, monkeypatch):
     """The FP32 particle passes merge the scatters of warp lanes whose windows
-    are consecutive in y (k_g2p_chain / k_dmap_chain); with the merging off
-    (MPM_B200_CHAIN=0) the plain per-lane reductions run.  Both are the same
-    sums in another order: they agree to FP32 rounding, and both match the
-    oracle to the mixed-mode tolerance."""
+    are consecutive in y (k_g2p_chain / k_dmap_chain, and k_mvl_p2g_chain with
+    MVL); with the merging off (MPM_B200_CHAIN=0) the plain per-lane
+    reductions run.  Both are the same sums in another order: they agree to
+    FP32 rounding, and both match the oracle to the mixed-mode tolerance."""
     mk = small2d if dim == 2 else small3d
     outs = []
     for chain in ("1", "0"):
         monkeypatch.setenv("MPM_B200_CHAIN", chain)
-        case = mk(pkg, constitutive="druckerprager", gpu_precision="mixed", scheme=scheme)
+        case = mk(pkg, constitutive="druckerprager", gpu_precision="mixed", scheme=scheme, MVL=mvl)
         dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
         dev.step(case.dt, 0.0, 24)
         out = fresh_particles(pkg, case.mp)
