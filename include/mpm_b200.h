@@ -192,6 +192,11 @@ typedef struct {
 
 /* ---- lifecycle (host2device / clean_device!) ---- */
 int mpm_create(const mpm_desc *desc, mpm_handle **out);
+/* mpm_upload / mpm_download: the host arrays may be pageable or page-locked;
+ * both calls return once every copy into or out of them has completed (with
+ * page-locked arrays the copies run asynchronously inside the call and the
+ * host-side conversions overlap them).  Staging uses the model's own particle
+ * buffers, no device allocation. */
 int mpm_upload(mpm_handle *h, const mpm_host_views *v);
 int mpm_destroy(mpm_handle *h);
 
