@@ -666,22 +666,15 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
                 else k_g2p<D, R, false, false, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
             });
             L.run("mvl_p2g", [&] {
-                if constexpr (std::is_same<R, float>::value) {
-                    if (h->chain) {
-                        k_mvl_p2g_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                        return;
-                    }
-                }
-                k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                if (h->chain) k_mvl_p2g_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                else k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
             });
         } else {
             L.run("g2p_p2g", [&] {
-                if constexpr (std::is_same<R, float>::value) {
-                    if (h->chain) {
-                        if (mc3) k_g2p_chain<D, D == 3, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                        else k_g2p_chain<D, false, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                        return;
-                    }
+                if (h->chain) {
+                    if (mc3) k_g2p_chain<D, D == 3, true, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    else k_g2p_chain<D, false, true, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    return;
                 }
                 if (mc3) k_g2p<D, R, true, D == 3, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
                 else k_g2p<D, R, true, false, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
@@ -689,16 +682,11 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         }
     } else if (sp.mvl && np) {
         // MVL: update + cell sums, then the cell-averaged mean stress + P2G
-        // (FP32: the scatters of chained lanes merged, as in the default passes)
-        const bool chain = h->chain && std::is_same<R, float>::value;
+        // (the scatters of chained lanes merged, as in the default passes)
+        const bool chain = h->chain;
         L.run("dmap", [&] {
-            if constexpr (std::is_same<R, float>::value) {
-                if (chain) {
-                    k_dmap_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    return;
-                }
-            }
-            k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (chain) k_dmap_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
         });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
@@ -709,13 +697,8 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
             else k_g2p<D, R, false><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
         });
         L.run("mvl_p2g", [&] {
-            if constexpr (std::is_same<R, float>::value) {
-                if (chain) {
-                    k_mvl_p2g_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    return;
-                }
-            }
-            k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (chain) k_mvl_p2g_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_mvl_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
         });
     } else if (sp.surr.mode == 2 && sp.plastic && np) {
         // surrogate: G2P + update with the yielding particles' returns deferred,
@@ -737,25 +720,18 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         }
         L.run("p2g", [&] { k_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
     } else {
-        const bool chain = h->chain && std::is_same<R, float>::value;
+        const bool chain = h->chain;
         if (np) L.run("dmap", [&] {
-            if constexpr (std::is_same<R, float>::value) {
-                if (chain) {
-                    k_dmap_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    return;
-                }
-            }
-            k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (chain) k_dmap_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
         });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         if (np) L.run("g2p_p2g", [&] {
-            if constexpr (std::is_same<R, float>::value) {
-                if (chain) {
-                    if (mc3) k_g2p_chain<D, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    else k_g2p_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    return;
-                }
+            if (chain) {
+                if (mc3) k_g2p_chain<D, D == 3, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                else k_g2p_chain<D, false, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                return;
             }
             if (mc3) k_g2p<D, R, true, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
             else k_g2p<D, R, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);

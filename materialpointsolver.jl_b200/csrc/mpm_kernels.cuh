@@ -44,6 +44,11 @@
 // two-phase chain kernels (both phases' records): the fused pass measured
 // 1.26 / 1.23 ms at 3 / 4 CTAs per SM on the 2.56 M saturated column, the
 // double mapping 0.447 / 0.448 / 0.476 ms at 4 / 5 / 6
+// the chain kernels in the all-FP64 mode: twice the registers per value; 3 CTAs
+// (85 registers) measured 2.56 ms per step on the 2.56 M column against 2.63 at 2
+#ifndef MPM_CHAIN_MINB_F64
+#define MPM_CHAIN_MINB_F64 3
+#endif
 #ifndef MPM_TS_P_MINB
 #define MPM_TS_P_MINB 4
 #endif
@@ -518,15 +523,15 @@ __device__ __forceinline__ Chain chain_of(int n0, int nny) {
 // 0 takes the two shuffled contributions; only the last lane of an x chain also
 // emits columns 1 and 2.  v[a][k]: k-th component of column a; returns whether
 // column a is emitted by this lane.
-template <int K>
-__device__ __forceinline__ void xmerge_row0(const Chain &ch, float (*v)[K], bool *emit) {
+template <typename R, int K>
+__device__ __forceinline__ void xmerge_row0(const Chain &ch, R (*v)[K], bool *emit) {
     const unsigned F = 0xffffffffu;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        const float a1 = __shfl_up_sync(F, v[1][k], 8), a2 = __shfl_up_sync(F, v[2][k], 16);
-        const float b2 = __shfl_up_sync(F, v[2][k], 8);
-        v[0][k] += (ch.x1 ? a1 : 0.0f) + (ch.x2 ? a2 : 0.0f);
-        v[1][k] += ch.x1 ? b2 : 0.0f;
+        const R a1 = __shfl_up_sync(F, v[1][k], 8), a2 = __shfl_up_sync(F, v[2][k], 16);
+        const R b2 = __shfl_up_sync(F, v[2][k], 8);
+        v[0][k] += (ch.x1 ? a1 : R(0.0)) + (ch.x2 ? a2 : R(0.0));
+        v[1][k] += ch.x1 ? b2 : R(0.0);
     }
     emit[0] = true;
     emit[1] = emit[2] = ch.xend;
@@ -534,12 +539,12 @@ __device__ __forceinline__ void xmerge_row0(const Chain &ch, float (*v)[K], bool
 
 // doublemapping2 (momentum N·p) with chained lanes merged; n0 = window corner,
 // key = n0 for a live lane, a value no other lane's key follows for a dead one
-template <int D>
-__device__ __forceinline__ void dm2_scatter_chain(const GDev<float> &g, const AxisW<float> *w, int n0, int key,
-                                                  const float *p) {
+template <int D, typename R = float>
+__device__ __forceinline__ void dm2_scatter_chain(const GDev<R> &g, const AxisW<R> *w, int n0, int key,
+                                                  const R *p) {
     const Chain ch = chain_of(key, g.nny);
     const unsigned F = 0xffffffffu;
-    float p1[3], p2[3];
+    R p1[3], p2[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         p1[k] = __shfl_up_sync(F, p[k], 1);
@@ -549,29 +554,29 @@ __device__ __forceinline__ void dm2_scatter_chain(const GDev<float> &g, const Ax
     constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-        const float wz = D == 3 ? w[2].N[c] : 1.0f;
-        float r0[3][3];   // row 0 of columns a = 0..2 (merged along y)
+        const R wz = D == 3 ? w[2].N[c] : R(1.0);
+        R r0[3][3];   // row 0 of columns a = 0..2 (merged along y)
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float wxz = w[0].N[a] * wz;
-            const float N0 = wxz * w[1].N[0], N1 = wxz * w[1].N[1], N2 = wxz * w[1].N[2];
-            const float u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2), v2 = __shfl_up_sync(F, N2, 1);
-            const float a1 = ch.c1 ? u1 : 0.0f, a2 = ch.c2 ? u2 : 0.0f, b2 = ch.c1 ? v2 : 0.0f;
+            const R wxz = w[0].N[a] * wz;
+            const R N0 = wxz * w[1].N[0], N1 = wxz * w[1].N[1], N2 = wxz * w[1].N[2];
+            const R u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2), v2 = __shfl_up_sync(F, N2, 1);
+            const R a1 = ch.c1 ? u1 : R(0.0), a2 = ch.c2 ? u2 : R(0.0), b2 = ch.c1 ? v2 : R(0.0);
 #pragma unroll
             for (int k = 0; k < 3; ++k) r0[a][k] = N0 * p[k] + a1 * p1[k] + a2 * p2[k];
             if (ch.end) {
-                Node8<float> *col = g.acc + (n0 + a * g.nny + c * plane);
-                if (N1 + b2 != 0.0f)
-                    red_add4(&col[1].a, 0.0f, N1 * p[0] + b2 * p1[0], N1 * p[1] + b2 * p1[1], N1 * p[2] + b2 * p1[2]);
-                if (N2 != 0.0f) red_add4(&col[2].a, 0.0f, N2 * p[0], N2 * p[1], N2 * p[2]);
+                Node8<R> *col = g.acc + (n0 + a * g.nny + c * plane);
+                if (N1 + b2 != R(0.0))
+                    red_add4(&col[1].a, R(0.0), N1 * p[0] + b2 * p1[0], N1 * p[1] + b2 * p1[1], N1 * p[2] + b2 * p1[2]);
+                if (N2 != R(0.0)) red_add4(&col[2].a, R(0.0), N2 * p[0], N2 * p[1], N2 * p[2]);
             }
         }
         bool emit[3];
-        xmerge_row0<3>(ch, r0, emit);
+        xmerge_row0<R, 3>(ch, r0, emit);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            if (!emit[a] || (r0[a][0] == 0.0f && r0[a][1] == 0.0f && r0[a][2] == 0.0f)) continue;
-            red_add4(&g.acc[n0 + a * g.nny + c * plane].a, 0.0f, r0[a][0], r0[a][1], r0[a][2]);
+            if (!emit[a] || (r0[a][0] == R(0.0) && r0[a][1] == R(0.0) && r0[a][2] == R(0.0))) continue;
+            red_add4(&g.acc[n0 + a * g.nny + c * plane].a, R(0.0), r0[a][0], r0[a][1], r0[a][2]);
         }
     }
 }
@@ -625,81 +630,146 @@ __device__ __forceinline__ void chain_nprop(const GDev<float> &g, const AxisW<fl
 
 // P2G_OS! of one particle with chained lanes merged (the arithmetic of
 // p2g_scatter; 7 components per node: m, p, f)
-template <int D>
-__device__ __forceinline__ void p2g_scatter_chain(const GDev<float> &g, const AxisW<float> *w, int n0, int key,
-                                                  float m, float vol, const float *v, const float *s, float G) {
-    const Chain ch = chain_of(key, g.nny);
-    const unsigned F = 0xffffffffu;
-    const float p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : 0.0f};
-    const int plane = g.nnx * g.nny;
-    constexpr int NC = D == 3 ? 3 : 1;
-    float sv[6];
-    if (D == 2) {
-        sv[0] = -vol * s[0]; sv[1] = -vol * s[1]; sv[3] = -vol * s[3];
-        sv[2] = sv[4] = sv[5] = 0.0f;
-    } else {
+template <int D, typename R = float>
+__device__ __forceinline__ void p2g_scatter_chain(const GDev<R> &g, const AxisW<R> *w, int n0, int key,
+                                                  R m, R vol, const R *v, const R *s, R G) {
+    if constexpr (std::is_same<R, float>::value) {
+        const Chain ch = chain_of(key, g.nny);
+        const unsigned F = 0xffffffffu;
+        const float p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : 0.0f};
+        const int plane = g.nnx * g.nny;
+        constexpr int NC = D == 3 ? 3 : 1;
+        float sv[6];
+        if (D == 2) {
+            sv[0] = -vol * s[0]; sv[1] = -vol * s[1]; sv[3] = -vol * s[3];
+            sv[2] = sv[4] = sv[5] = 0.0f;
+        } else {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) sv[k] = -vol * s[k];
-    }
+            for (int k = 0; k < 6; ++k) sv[k] = -vol * s[k];
+        }
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        const float wz = D == 3 ? w[2].N[c] : 1.0f, gz = D == 3 ? w[2].dN[c] : 0.0f;
+        for (int c = 0; c < NC; ++c) {
+            const float wz = D == 3 ? w[2].N[c] : 1.0f, gz = D == 3 ? w[2].dN[c] : 0.0f;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float wx = w[0].N[a];
-            const float wxz = wx * wz, gxz = w[0].dN[a] * wz, xdz = wx * gz;
-            // per column: node value = Ny·(M, P, X) + dNy·(0, 0, Y)
-            float U[7], Y[3];
-            U[0] = m * wxz;
-            U[1] = p[0] * wxz; U[2] = p[1] * wxz; U[3] = p[2] * wxz;
-            if (D == 2) {
-                U[4] = sv[0] * gxz; U[5] = sv[3] * gxz + U[0] * G; U[6] = 0.0f;
-                Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = 0.0f;
-            } else {
-                U[4] = sv[0] * gxz + sv[5] * xdz;
-                U[5] = sv[3] * gxz + sv[4] * xdz;
-                U[6] = sv[5] * gxz + sv[2] * xdz + U[0] * G;
-                Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = sv[4] * wxz;
-            }
-            // this lane's rows b = 0, 1, 2 as component pairs (packed FP32 arithmetic):
-            // (m, px), (py, pz), (fx, fy), (fz, 0)
-            float2 r0[4], r1[4], r2[4];
-            const float2 U01 = make_float2(U[0], U[1]), U23 = make_float2(U[2], U[3]);
-            const float2 U45 = make_float2(U[4], U[5]), Y01 = make_float2(Y[0], Y[1]);
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const float wy = w[1].N[b], gy = w[1].dN[b];
-                const float2 w2 = make_float2(wy, wy), g2 = make_float2(gy, gy);
-                float2 *r = b == 0 ? r0 : (b == 1 ? r1 : r2);
-                r[0] = __fmul2_rn(w2, U01);
-                r[1] = __fmul2_rn(w2, U23);
-                r[2] = __ffma2_rn(w2, U45, __fmul2_rn(g2, Y01));
-                r[3] = make_float2(wy * U[6] + gy * Y[2], 0.0f);
-            }
-            // row 0 += lane L-1's row 1 + lane L-2's row 2; chain ends: row 1 += lane L-1's row 2
-            const float f1 = ch.c1 ? 1.0f : 0.0f, f2 = ch.c2 ? 1.0f : 0.0f;
-            const float2 c1 = make_float2(f1, f1), c2 = make_float2(f2, f2);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float2 x1 = make_float2(__shfl_up_sync(F, r1[j].x, 1), __shfl_up_sync(F, r1[j].y, 1));
-                const float2 x2 = make_float2(__shfl_up_sync(F, r2[j].x, 2), __shfl_up_sync(F, r2[j].y, 2));
-                const float2 y2 = make_float2(__shfl_up_sync(F, r2[j].x, 1), __shfl_up_sync(F, r2[j].y, 1));
-                r0[j] = __ffma2_rn(c2, x2, __ffma2_rn(c1, x1, r0[j]));
-                r1[j] = __ffma2_rn(c1, y2, r1[j]);
-            }
-            Node8<float> *col = g.acc + (n0 + a * g.nny + c * plane);
-            if (r0[0].x != 0.0f) {
-                red_add4(&col[0].a, r0[0].x, r0[0].y, r0[1].x, r0[1].y);
-                red_add4(&col[0].b, r0[2].x, r0[2].y, r0[3].x, 0.0f);
-            }
-            if (ch.end) {
-                if (r1[0].x != 0.0f) {
-                    red_add4(&col[1].a, r1[0].x, r1[0].y, r1[1].x, r1[1].y);
-                    red_add4(&col[1].b, r1[2].x, r1[2].y, r1[3].x, 0.0f);
+            for (int a = 0; a < 3; ++a) {
+                const float wx = w[0].N[a];
+                const float wxz = wx * wz, gxz = w[0].dN[a] * wz, xdz = wx * gz;
+                // per column: node value = Ny·(M, P, X) + dNy·(0, 0, Y)
+                float U[7], Y[3];
+                U[0] = m * wxz;
+                U[1] = p[0] * wxz; U[2] = p[1] * wxz; U[3] = p[2] * wxz;
+                if (D == 2) {
+                    U[4] = sv[0] * gxz; U[5] = sv[3] * gxz + U[0] * G; U[6] = 0.0f;
+                    Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = 0.0f;
+                } else {
+                    U[4] = sv[0] * gxz + sv[5] * xdz;
+                    U[5] = sv[3] * gxz + sv[4] * xdz;
+                    U[6] = sv[5] * gxz + sv[2] * xdz + U[0] * G;
+                    Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = sv[4] * wxz;
                 }
-                if (r2[0].x != 0.0f) {
-                    red_add4(&col[2].a, r2[0].x, r2[0].y, r2[1].x, r2[1].y);
-                    red_add4(&col[2].b, r2[2].x, r2[2].y, r2[3].x, 0.0f);
+                // this lane's rows b = 0, 1, 2 as component pairs (packed FP32 arithmetic):
+                // (m, px), (py, pz), (fx, fy), (fz, 0)
+                float2 r0[4], r1[4], r2[4];
+                const float2 U01 = make_float2(U[0], U[1]), U23 = make_float2(U[2], U[3]);
+                const float2 U45 = make_float2(U[4], U[5]), Y01 = make_float2(Y[0], Y[1]);
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const float wy = w[1].N[b], gy = w[1].dN[b];
+                    const float2 w2 = make_float2(wy, wy), g2 = make_float2(gy, gy);
+                    float2 *r = b == 0 ? r0 : (b == 1 ? r1 : r2);
+                    r[0] = __fmul2_rn(w2, U01);
+                    r[1] = __fmul2_rn(w2, U23);
+                    r[2] = __ffma2_rn(w2, U45, __fmul2_rn(g2, Y01));
+                    r[3] = make_float2(wy * U[6] + gy * Y[2], 0.0f);
+                }
+                // row 0 += lane L-1's row 1 + lane L-2's row 2; chain ends: row 1 += lane L-1's row 2
+                const float f1 = ch.c1 ? 1.0f : 0.0f, f2 = ch.c2 ? 1.0f : 0.0f;
+                const float2 c1 = make_float2(f1, f1), c2 = make_float2(f2, f2);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float2 x1 = make_float2(__shfl_up_sync(F, r1[j].x, 1), __shfl_up_sync(F, r1[j].y, 1));
+                    const float2 x2 = make_float2(__shfl_up_sync(F, r2[j].x, 2), __shfl_up_sync(F, r2[j].y, 2));
+                    const float2 y2 = make_float2(__shfl_up_sync(F, r2[j].x, 1), __shfl_up_sync(F, r2[j].y, 1));
+                    r0[j] = __ffma2_rn(c2, x2, __ffma2_rn(c1, x1, r0[j]));
+                    r1[j] = __ffma2_rn(c1, y2, r1[j]);
+                }
+                Node8<float> *col = g.acc + (n0 + a * g.nny + c * plane);
+                if (r0[0].x != 0.0f) {
+                    red_add4(&col[0].a, r0[0].x, r0[0].y, r0[1].x, r0[1].y);
+                    red_add4(&col[0].b, r0[2].x, r0[2].y, r0[3].x, 0.0f);
+                }
+                if (ch.end) {
+                    if (r1[0].x != 0.0f) {
+                        red_add4(&col[1].a, r1[0].x, r1[0].y, r1[1].x, r1[1].y);
+                        red_add4(&col[1].b, r1[2].x, r1[2].y, r1[3].x, 0.0f);
+                    }
+                    if (r2[0].x != 0.0f) {
+                        red_add4(&col[2].a, r2[0].x, r2[0].y, r2[1].x, r2[1].y);
+                        red_add4(&col[2].b, r2[2].x, r2[2].y, r2[3].x, 0.0f);
+                    }
+                }
+            }
+        }
+
+    } else {
+        // FP64: the same rows and merging, component by component
+        const Chain ch = chain_of(key, g.nny);
+        const unsigned F = 0xffffffffu;
+        const R p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : R(0)};
+        const int plane = g.nnx * g.nny;
+        constexpr int NC = D == 3 ? 3 : 1;
+        R sv[6];
+        if (D == 2) {
+            sv[0] = -vol * s[0]; sv[1] = -vol * s[1]; sv[3] = -vol * s[3];
+            sv[2] = sv[4] = sv[5] = R(0);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) sv[k] = -vol * s[k];
+        }
+        const R f1 = ch.c1 ? R(1) : R(0), f2 = ch.c2 ? R(1) : R(0);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const R wz = D == 3 ? w[2].N[c] : R(1), gz = D == 3 ? w[2].dN[c] : R(0);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const R wx = w[0].N[a];
+                const R wxz = wx * wz, gxz = w[0].dN[a] * wz, xdz = wx * gz;
+                R U[7], Y[3];
+                U[0] = m * wxz;
+                U[1] = p[0] * wxz; U[2] = p[1] * wxz; U[3] = p[2] * wxz;
+                if (D == 2) {
+                    U[4] = sv[0] * gxz; U[5] = sv[3] * gxz + U[0] * G; U[6] = R(0);
+                    Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = R(0);
+                } else {
+                    U[4] = sv[0] * gxz + sv[5] * xdz;
+                    U[5] = sv[3] * gxz + sv[4] * xdz;
+                    U[6] = sv[5] * gxz + sv[2] * xdz + U[0] * G;
+                    Y[0] = sv[3] * wxz; Y[1] = sv[1] * wxz; Y[2] = sv[4] * wxz;
+                }
+                // rows b = 0, 1, 2: (m, px, py, pz, fx, fy, fz)
+                R r[3][7];
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const R wy = w[1].N[b], gy = w[1].dN[b];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) r[b][k] = wy * U[k];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) r[b][4 + k] = wy * U[4 + k] + gy * Y[k];
+                }
+#pragma unroll
+                for (int j = 0; j < 7; ++j) {
+                    const R x1 = __shfl_up_sync(F, r[1][j], 1), x2 = __shfl_up_sync(F, r[2][j], 2);
+                    const R y2 = __shfl_up_sync(F, r[2][j], 1);
+                    r[0][j] += f1 * x1 + f2 * x2;
+                    r[1][j] += f1 * y2;
+                }
+                Node8<R> *col = g.acc + (n0 + a * g.nny + c * plane);
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    if (b > 0 && !ch.end) break;
+                    if (r[b][0] == R(0)) continue;
+                    red_add4(&col[b].a, r[b][0], r[b][1], r[b][2], r[b][3]);
+                    red_add4(&col[b].b, r[b][4], r[b][5], r[b][6], R(0));
                 }
             }
         }
@@ -812,26 +882,26 @@ __global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<
     dm2_scatter<D, R>(g, w, p);
 }
 
-// The same pass (FP32) with the re-scatter of chained lanes merged.
-template <int D>
-__global__ void __launch_bounds__(256, MPM_DMAP_CHAIN_MINB) k_dmap_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+// The same pass with the re-scatter of chained lanes merged (FP32 and FP64).
+template <int D, typename R = float>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM_DMAP_CHAIN_MINB) k_dmap_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < sp.np;
-    AxisW<float> w[3];
-    float p[3] = {0, 0, 0};
+    AxisW<R> w[3];
+    R p[3] = {0, 0, 0};
     int n0 = 0, key = dead_key();
     if (live) {
-        dmap_core<D, float>(P, g, sp, i, w, p);
-        n0 = key = window_n0<D, float>(g, w);
+        dmap_core<D, R>(P, g, sp, i, w, p);
+        n0 = key = window_n0<D, R>(g, w);
     } else {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             w[a].base = 0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = R(0.0); w[a].dN[k] = R(0.0); }
         }
     }
-    dm2_scatter_chain<D>(g, w, n0, key, p);
+    dm2_scatter_chain<D, R>(g, w, n0, key, p);
 }
 
 // doublemapping3_OS!, utils_OS.jl:968-1016: grid velocity from the re-mapped
@@ -1232,17 +1302,17 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
     }
 }
 
-// The same pass (FP32, FUSE) with the scatter of chained lanes merged.
-template <int D, bool MC3 = false, bool USL = false>
-__global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+// The same pass (FUSE) with the scatter of chained lanes merged (FP32 and FP64).
+template <int D, bool MC3 = false, bool USL = false, typename R = float>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM_P_MINB) k_g2p_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool live = i < sp.np;
     double x[3];
-    AxisW<float> w[3];
-    float s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, v[3] = {0, 0, 0}, m = 0;
+    AxisW<R> w[3];
+    R s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, v[3] = {0, 0, 0}, m = 0;
     if (live) {
-        g2p_core<D, float, true, MC3, USL>(P, g, sp, i, nullptr, x, w, s, vol);
-        if (!particle_weights<D, float>(x, g, w)) {
+        g2p_core<D, R, true, MC3, USL>(P, g, sp, i, nullptr, x, w, s, vol);
+        if (!particle_weights<D, R>(x, g, w)) {
             atomicOr(g.err, ERR_OOG);
             live = false;
         } else {
@@ -1253,20 +1323,20 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p_chain(PDev<D, float> P,
     }
     int n0 = 0, key = dead_key();
     if (live) {
-        n0 = key = window_n0<D, float>(g, w);
+        n0 = key = window_n0<D, R>(g, w);
     } else {
-        m = 0.0f;
+        m = R(0.0);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             w[a].base = 0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = R(0.0); w[a].dN[k] = R(0.0); }
         }
     }
     MarkState mk;
-    if (live) mk = mark_begin<D, float>(g, w);
-    p2g_scatter_chain<D>(g, w, n0, key, m, vol, v, s, (float)sp.G);
-    if (live) mark_end<float>(g, mk);
+    if (live) mk = mark_begin<D, R>(g, w);
+    p2g_scatter_chain<D, R>(g, w, n0, key, m, vol, v, s, (R)sp.G);
+    if (live) mark_end<R>(g, mk);
 }
 
 // vollock2_OS! + the next step's P2G: the particle's mean stress is replaced by
@@ -1296,28 +1366,28 @@ __global__ void __launch_bounds__(256) k_mvl_p2g(PDev<D, R> P, GDev<R> g, StepPa
     p2g_scatter<D, R>(g, w, P.m[i], P.vol[i], v, s, (R)sp.G);
 }
 
-// The same pass (FP32) with the scatters of chained lanes merged (p2g_scatter_chain).
-template <int D>
-__global__ void __launch_bounds__(256) k_mvl_p2g_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+// The same pass with the scatters of chained lanes merged (p2g_scatter_chain).
+template <int D, typename R = float>
+__global__ void __launch_bounds__(256) k_mvl_p2g_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool live = i < sp.np;
-    constexpr int NV = PDev<D, float>::NV;
-    float s[6] = {0, 0, 0, 0, 0, 0}, v[3] = {0, 0, 0}, m = 0.0f, vol = 0.0f;
-    AxisW<float> w[3];
+    constexpr int NV = PDev<D, R>::NV;
+    R s[6] = {0, 0, 0, 0, 0, 0}, v[3] = {0, 0, 0}, m = R(0.0), vol = R(0.0);
+    AxisW<R> w[3];
     if (live) {
         const uint32_t c = g.pcell[i];
-        const float cm = g.csigm[c] / g.comega[c];
+        const R cm = g.csigm[c] / g.comega[c];
 #pragma unroll
         for (int k = 0; k < NV; ++k) s[k] = P.sig[k][i];
-        const float sm = (s[0] + s[1] + s[2]) * 0.333333f;
+        const R sm = (s[0] + s[1] + s[2]) * R(0.333333);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             s[k] = (s[k] - sm) + cm;
             P.sig[k][i] = s[k];
         }
         double x[3];
-        load_x<D, float>(P, i, x);
-        if (!particle_weights<D, float>(x, g, w)) {
+        load_x<D, R>(P, i, x);
+        if (!particle_weights<D, R>(x, g, w)) {
             atomicOr(g.err, ERR_OOG);
             live = false;
         } else {
@@ -1329,20 +1399,20 @@ __global__ void __launch_bounds__(256) k_mvl_p2g_chain(PDev<D, float> P, GDev<fl
     }
     int n0 = 0, key = dead_key();
     if (live) {
-        n0 = key = window_n0<D, float>(g, w);
+        n0 = key = window_n0<D, R>(g, w);
     } else {
-        m = vol = 0.0f;
+        m = vol = R(0.0);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             w[a].base = 0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = R(0.0); w[a].dN[k] = R(0.0); }
         }
     }
     MarkState mk;
-    if (live) mk = mark_begin<D, float>(g, w);
-    p2g_scatter_chain<D>(g, w, n0, key, m, vol, v, s, (float)sp.G);
-    if (live) mark_end<float>(g, mk);
+    if (live) mk = mark_begin<D, R>(g, w);
+    p2g_scatter_chain<D, R>(g, w, n0, key, m, vol, v, s, (R)sp.G);
+    if (live) mark_end<R>(g, mk);
 }
 
 // Finish the deferred returns: accept the surrogate's stress when its yield

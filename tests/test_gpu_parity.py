@@ -464,33 +464,38 @@ def test_graph_replay_matches_direct_launches(pkg, orc, gpu_lib, dim, monkeypatc
     check_fields(outs[0], o, case.mp, TOL64)
 
 
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
 @pytest.mark.parametrize("mvl", [False, True])
 @pytest.mark.parametrize("scheme", ["MUSL", "USL"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_lane_merged_scatter_matches_plain(pkg, orc, gpu_lib, dim, scheme, mvl, monkeypatch):
-    """The FP32 particle passes merge the scatters of warp lanes whose windows
+def test_lane_merged_scatter_matches_plain(pkg, orc, gpu_lib, dim, scheme, mvl, prec, monkeypatch):
+    """The particle passes merge the scatters of warp lanes whose windows
     are consecutive in y (k_g2p_chain / k_dmap_chain, and k_mvl_p2g_chain with
     MVL); with the merging off (MPM_B200_CHAIN=0) the plain per-lane
     reductions run.  Both are the same sums in another order: they agree to
-    FP32 rounding, and both match the oracle to the mixed-mode tolerance."""
+    rounding (FP32 or FP64), and both match the oracle to that mode's tolerance."""
     mk = small2d if dim == 2 else small3d
     outs = []
     for chain in ("1", "0"):
         monkeypatch.setenv("MPM_B200_CHAIN", chain)
-        case = mk(pkg, constitutive="druckerprager", gpu_precision="mixed", scheme=scheme, MVL=mvl)
+        case = mk(pkg, constitutive="druckerprager", gpu_precision=prec, scheme=scheme, MVL=mvl)
         dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
         dev.step(case.dt, 0.0, 24)
         out = fresh_particles(pkg, case.mp)
         dev.download(pkg._lib.F_REFERENCE | pkg._lib.F_F, out)
         dev.close()
         outs.append(out)
-    assert rel(outs[0].xi - case.mp.xi, outs[1].xi - case.mp.xi) < 1e-5
+    agree = 1e-5 if prec == "mixed" else 1e-10
+    assert rel(outs[0].xi - case.mp.xi, outs[1].xi - case.mp.xi) < agree
     for f in ("vs", "F", "Omega"):
-        assert rel(getattr(outs[0], f), getattr(outs[1], f)) < 1e-5, f
+        assert rel(getattr(outs[0], f), getattr(outs[1], f)) < agree, f
     o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc)
     o.run(case.dt, 0.0, 24)
     for out in outs:
-        check_fields(out, o, case.mp, TOL32, TOL32_STRESS)
+        if prec == "mixed":
+            check_fields(out, o, case.mp, TOL32, TOL32_STRESS)
+        else:
+            check_fields(out, o, case.mp, TOL64)
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", TOL32)])
