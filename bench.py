@@ -42,13 +42,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mc3d", default="literal", choices=["literal", "restated"])
     ap.add_argument("--workload", default="column3d",
-                    choices=["column3d", "slope3d", "batch2d", "column2d", "saturated3d", "example3d"],
+                    choices=["column3d", "slope3d", "batch2d", "column2d", "saturated3d", "example3d", "example2d"],
                     help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
                          "3D slope with a lognormal cohesion field; batch2d: 256 independent 2D slopes "
                          "(15.5 M particles) advanced together, autotuned during warm-up; column2d: the 3 200-"
                          "particle 2D column in FP64 (launch-bound; CUDA graph replay); saturated3d: the 2.56 M-particle column "
                          "as a two-phase (solid + water) saturated soil, coupling TS; example3d: the reference's "
-                         "own 3D example (512 000 particles, MVL on), against its published 66.3 it/s")
+                         "own 3D example (512 000 particles, MVL on), against its published 66.3 it/s; example2d: its "
+                         "2D example (20 000 particles), against its published 2.11e3 it/s")
     ap.add_argument("--surrogate", action="store_true",
                     help="slope3d: train the stress-return surrogate on samples logged from plain steps "
                          "(untimed) and time steps with it")
@@ -146,11 +147,20 @@ WORKLOADS = {
                     "constitutive": "druckerprager"},
     "example3d": {"workload": "the reference's 3D column-collapse example (examples/3d_collapse.ipynb), uGIMP, "
                               "MUSL va=:a, MVL on", "constitutive": "druckerprager"},
+    "example2d": {"workload": "the reference's 2D column-collapse example (examples/2d_collapse.ipynb), uGIMP, "
+                              "MUSL va=:a", "constitutive": "druckerprager"},
 }
 
 # The reference's published throughput for the example3d case: 66.3 it/s with
 # 512 000 particles, FP64, on an unstated NVIDIA GPU (examples/3d_collapse.ipynb:381).
 EXAMPLE3D_PUBLISHED = 66.3 * 512000
+# ... and for the example2d case: 2.11e3 it/s with 20 000 particles, FP64, on an
+# unstated NVIDIA GPU (examples/2d_collapse.ipynb:385).
+EXAMPLE2D_PUBLISHED = 2.11e3 * 20000
+EXAMPLES = {"example3d": ("collapse_3d_example", EXAMPLE3D_PUBLISHED,
+                          "examples/3d_collapse.ipynb:381: 66.3 it/s x 512 000 particles, FP64, unstated NVIDIA GPU"),
+            "example2d": ("collapse_2d_example", EXAMPLE2D_PUBLISHED,
+                          "examples/2d_collapse.ipynb:385: 2.11e3 it/s x 20 000 particles, FP64, unstated NVIDIA GPU")}
 
 
 def make_case(mc3d, workload="column3d", surrogate=False):
@@ -166,8 +176,8 @@ def make_case(mc3d, workload="column3d", surrogate=False):
         case = pkg.workloads.slope_batch_2d(Te=0.0)   # plastic regime, as above
     elif workload == "column2d":
         case = pkg.workloads.column_collapse_2d(gpu_precision="fp64")
-    elif workload == "example3d":
-        case = pkg.workloads.collapse_3d_example()
+    elif workload in EXAMPLES:
+        case = getattr(pkg.workloads, EXAMPLES[workload][0])()
     elif workload == "saturated3d":
         case = pkg.workloads.saturated_column(dim=3, h=0.005, size=(0.5, 0.2, 0.4), box=(1.2, 0.4, 0.6),
                                               constitutive="druckerprager", seed=1002)
@@ -225,10 +235,10 @@ def advance_time(Ti, dt, n, f32):
     return Ti
 
 
-def fp64_device_rate(pkg, device, K, W):
-    """The example3d case with every device array in FP64 (the precision of
-    the published number): W untimed steps, then K steps timed with CUDA events."""
-    case = pkg.workloads.collapse_3d_example(gpu_precision="fp64")
+def fp64_device_rate(pkg, builder, published, device, K, W):
+    """A reference example with every device array in FP64 (the precision of
+    its published number): W untimed steps, then K steps timed with CUDA events."""
+    case = getattr(pkg.workloads, builder)(gpu_precision="fp64")
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=device)
     try:
         Ti = dev.step(case.dt, 0.0, W)
@@ -239,7 +249,7 @@ def fp64_device_rate(pkg, device, K, W):
         dev.close()
     value = case.mp.np * K / (ms * 1e-3)
     return {"value": value, "unit": "particle-updates/s", "ms_per_step": ms / K,
-            "vs_baseline": value / EXAMPLE3D_PUBLISHED}
+            "vs_baseline": value / published}
 
 
 def run_b200(args):
@@ -383,7 +393,10 @@ def run_b200(args):
                        mc3d=args.mc3d, precision=("all FP64" if args.workload == "column2d"
                                                    else "FP32 bulk, FP64 positions and det(F)"), sort_every=sort_used,
                        particle_passes="tiled" if tiled_used else "per-particle",
-                       l2=f"particle state {npart * bp_step / 1e9:.2f} GB > 126 MB L2 (no flush needed)",
+                       l2=(f"particle state {npart * bp_step / 1e9:.2f} GB > 126 MB L2 (no flush needed)"
+                           if npart * bp_step > 126e6 else
+                           f"particle state {npart * bp_step / 1e6:.1f} MB < 126 MB L2: L2-resident, not "
+                           "flushed (a model of this size runs from L2; launch-bound)"),
                        parallelism=f"replicas x{world}",
                        **({"slopes": len(case.meta["slopes"]), "tuning": tuning} if tuning else {}),
                        **({"surrogate": surr_info} if surr_info else {})),
@@ -398,12 +411,11 @@ def run_b200(args):
                 "what": "DeviceModel upload from pinned host arrays + K steps + device2host! field set"},
         "clocks": clk.summary(),
     }
-    if args.workload == "example3d":
-        result["vs_baseline"] = value / EXAMPLE3D_PUBLISHED
-        result["baseline"] = {"value": EXAMPLE3D_PUBLISHED, "unit": "particle-updates/s",
-                              "source": "examples/3d_collapse.ipynb:381: 66.3 it/s x 512 000 particles, FP64, "
-                                        "unstated NVIDIA GPU"}
-        result["fp64_device"] = fp64_device_rate(pkg, local, K, W)
+    if args.workload in EXAMPLES:
+        builder, published, source = EXAMPLES[args.workload]
+        result["vs_baseline"] = value / published
+        result["baseline"] = {"value": published, "unit": "particle-updates/s", "source": source}
+        result["fp64_device"] = fp64_device_rate(pkg, builder, published, local, K, W)
     if args.snapshot_every > 0:
         result["snapshots"] = snapshot_cost(pkg, case, dt, K, args.snapshot_every, local)
     if rank == 0 and not args.no_cpu_baseline:

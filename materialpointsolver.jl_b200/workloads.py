@@ -500,6 +500,41 @@ def collapse_3d_validation(*, precision="FP64", gpu_precision="mixed", Ttol=1.0,
     return Case("collapse_3d_validation", args, grid, mp, attr, bc, dt, nsteps, dict(np=npart, h=h, K=K, G=G, seed=0))
 
 
+def collapse_2d_example(*, precision="FP64", gpu_precision="mixed", Ttol=1.0, project_path="/tmp", **extra):
+    """The reference's 2D column-collapse example (examples/2d_collapse.ipynb),
+    the case behind its published 2D throughput (2.11e3 it/s, FP64, on an
+    unstated NVIDIA GPU): a 0.2 x 0.1 m column, 2 x 2 particles per 2 mm cell
+    (20 000 particles) on [-0.1, 0.82] x [-0.1, 0.12] (51 171 nodes),
+    Drucker-Prager φ = 19.8°, c = 0, ψ = 0, K = 7e5 Pa, ν = 0.3, ρ = 2650,
+    MUSL va = :a, gravity -9.8, Δt = 0.5 h / sqrt(E/ρ), 1 s; walls at x <= 0 and
+    x >= 0.8 and a rough floor (both components fixed at y <= 0)."""
+    h = 0.002
+    K, nu, rho = 7e5, 0.3, 2650.0
+    E = K * (3.0 * (1.0 - 2.0 * nu))
+    G = E / (2.0 * (1.0 + nu))
+    dt = 0.5 * h / math.sqrt(E / rho)
+    lp = h / 2
+    pts = meshbuilder(jl_range(lp / 2, lp, 0.2 - lp / 2), jl_range(lp / 2, lp, 0.1 - lp / 2))
+    npart = pts.shape[0]
+    akw = dict(Ttol=Ttol, Te=0, ΔT=dt, FLIP=1, PIC=0, constitutive="druckerprager", basis="uGIMP",
+               device="B200", coupling="OS", scheme="MUSL", va="a", gravity=-9.8, ζs=0,
+               project_name="2d_collapse", project_path=project_path, ϵ=precision,
+               gpu_precision=gpu_precision, make_project_dir=False)
+    akw.update(extra)
+    args = UserArgs2D(**akw)
+    grid = UserGrid2D(ϵ=precision, x1=-0.1, x2=0.82, y1=-0.1, y2=0.12, dx=h, dy=h, NIC=9)
+    mp = UserParticle2D(ϵ=precision, NIC=9, dx=lp, dy=lp, ξ=pts, ρs=np.full(npart, rho))
+    attr = UserProperty(ϵ=precision, nid=np.ones(npart, np.int64), ν=[nu], Es=[E], Gs=[G], Ks=[K],
+                        σt=[0.0], ϕ=[math.radians(19.8)], ϕr=[0.0], ψ=[0.0], c=[0.0], cr=[0.0], Hp=[0.0])
+    gx, gy = grid.xi[:, 0], grid.xi[:, 1]
+    vx = ((gx <= 0.0) | (gx >= 0.8) | (gy <= 0.0)).astype(np.int64)
+    vy = (gy <= 0.0).astype(np.int64)
+    bc = UserVBoundary2D(ϵ=precision, vx_s_idx=vx, vx_s_val=np.zeros(grid.ni), vy_s_idx=vy,
+                         vy_s_val=np.zeros(grid.ni))
+    nsteps = int(math.ceil(Ttol / dt))
+    return Case("collapse_2d_example", args, grid, mp, attr, bc, dt, nsteps, dict(np=npart, h=h, K=K, G=G, seed=0))
+
+
 def collapse_3d_example(*, precision="FP64", gpu_precision="mixed", Ttol=1.0, mvl=True, project_path="/tmp",
                         **extra):
     """The reference's 3D column-collapse example (examples/3d_collapse.ipynb),
