@@ -5,7 +5,7 @@ Workload (per GPU): 3D column collapse, domain 1.2 x 0.4 x 0.6 m, h = 5 mm,
 column 0.5 x 0.2 x 0.4 m at 2x2x2 particles per cell = 2 560 000 particles,
 Mohr-Coulomb (phi = 30 deg, c = 0, psi = 0), rho = 2650, E = 1 MPa, nu = 0.3,
 free-slip walls, CFL 0.2, FP32 bulk with FP64 positions and det(F).  A bench
-step is one MPM time step over all particles (cell re-sort every 8 steps
+step is one MPM time step over all particles (cell re-sort every 16 steps
 included).  The particle state (~0.5 GB) exceeds the 126 MB L2, so no flush is
 needed between steps.
 
