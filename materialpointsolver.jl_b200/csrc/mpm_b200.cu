@@ -619,23 +619,16 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         // two-phase MUSL (TS_MUSL.jl): solve, DM1+DM2, DM3, G2P_TS! + next P2G_TS!
         L.run("solve", [&] { k_solve_ts<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         if (np) L.run("dmap", [&] {
-            if constexpr (std::is_same<R, float>::value) {
-                if (h->chain) {
-                    k_dmap_ts_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    return;
-                }
-            }
-            k_dmap_ts<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (h->chain) k_dmap_ts_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_dmap_ts<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
         });
         L.run("dm3", [&] { k_dm3_ts<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         if (np) L.run("g2p_p2g", [&] {
-            if constexpr (std::is_same<R, float>::value) {
-                if (h->chain) {
-                    if (mc3) k_g2p_ts_chain<D, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    else k_g2p_ts_chain<D><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    return;
-                }
+            if (h->chain) {
+                if (mc3) k_g2p_ts_chain<D, D == 3, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                else k_g2p_ts_chain<D, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                return;
             }
             if (mc3) k_g2p_ts<D, R, true, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
             else k_g2p_ts<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);

@@ -52,6 +52,9 @@
 #ifndef MPM_TS_P_MINB
 #define MPM_TS_P_MINB 4
 #endif
+#ifndef MPM_TS_P_MINB_F64
+#define MPM_TS_P_MINB_F64 2
+#endif
 #ifndef MPM_TS_DMAP_CHAIN_MINB
 #define MPM_TS_DMAP_CHAIN_MINB 4
 #endif
@@ -586,39 +589,39 @@ __device__ __forceinline__ void dm2_scatter_chain(const GDev<R> &g, const AxisW<
 // takes lane L-1's row 1 and lane L-2's row 2 (V and the weights shuffled);
 // rows 1 and 2 are reduced by the chain's last lane.  rec(i) is the record of
 // node i.  All lanes call it.
-template <int D, int K, typename Rec>
-__device__ __forceinline__ void chain_nprop(const GDev<float> &g, const AxisW<float> *w, int n0, const Chain &ch,
-                                               const float *V, Rec rec) {
+template <int D, int K, typename R, typename Rec>
+__device__ __forceinline__ void chain_nprop(const GDev<R> &g, const AxisW<R> *w, int n0, const Chain &ch,
+                                               const R *V, Rec rec) {
     const unsigned F = 0xffffffffu;
-    float V1[K], V2[K];
+    R V1[K], V2[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) { V1[k] = __shfl_up_sync(F, V[k], 1); V2[k] = __shfl_up_sync(F, V[k], 2); }
     const int plane = g.nnx * g.nny;
     constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-        const float wz = D == 3 ? w[2].N[c] : 1.0f;
+        const R wz = D == 3 ? w[2].N[c] : R(1.0);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float wx = w[0].N[a];
+            const R wx = w[0].N[a];
             const int col = n0 + a * g.nny + c * plane;
-            const float N0 = wx * w[1].N[0] * wz, N1 = wx * w[1].N[1] * wz, N2 = wx * w[1].N[2] * wz;
-            const float u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2);
-            const float v2 = __shfl_up_sync(F, N2, 1);
-            const float f1 = ch.c1 ? u1 : 0.0f, f2 = ch.c2 ? u2 : 0.0f, e1 = ch.c1 ? v2 : 0.0f;
-            float r[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            if (N0 + f1 + f2 != 0.0f) {
+            const R N0 = wx * w[1].N[0] * wz, N1 = wx * w[1].N[1] * wz, N2 = wx * w[1].N[2] * wz;
+            const R u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2);
+            const R v2 = __shfl_up_sync(F, N2, 1);
+            const R f1 = ch.c1 ? u1 : R(0.0), f2 = ch.c2 ? u2 : R(0.0), e1 = ch.c1 ? v2 : R(0.0);
+            R r[4] = {R(0.0), R(0.0), R(0.0), R(0.0)};
+            if (N0 + f1 + f2 != R(0.0)) {
 #pragma unroll
                 for (int k = 0; k < K; ++k) r[k] = N0 * V[k] + f1 * V1[k] + f2 * V2[k];
                 red_add4(rec(col), r[0], r[1], r[2], r[3]);
             }
             if (ch.end) {
-                if (N1 + e1 != 0.0f) {
+                if (N1 + e1 != R(0.0)) {
 #pragma unroll
                     for (int k = 0; k < K; ++k) r[k] = N1 * V[k] + e1 * V1[k];
                     red_add4(rec(col + 1), r[0], r[1], r[2], r[3]);
                 }
-                if (N2 != 0.0f) {
+                if (N2 != R(0.0)) {
 #pragma unroll
                     for (int k = 0; k < K; ++k) r[k] = N2 * V[k];
                     red_add4(rec(col + 2), r[0], r[1], r[2], r[3]);

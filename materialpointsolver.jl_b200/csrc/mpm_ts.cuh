@@ -278,27 +278,27 @@ __global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepPa
 // The same pass (FP32) with the re-scatter of chained warp lanes merged (the
 // momenta are lane constants, so only the weights are shuffled; see
 // dm2_scatter_chain).
-template <int D>
-__global__ void __launch_bounds__(256, MPM_TS_DMAP_CHAIN_MINB) k_dmap_ts_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+template <int D, typename R = float>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM_TS_DMAP_CHAIN_MINB) k_dmap_ts_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < sp.np;
-    AxisW<float> w[3];
-    float ps[3] = {0, 0, 0}, pw[3] = {0, 0, 0};
+    AxisW<R> w[3];
+    R ps[3] = {0, 0, 0}, pw[3] = {0, 0, 0};
     int n0 = 0, key = dead_key();
     if (live) {
-        dmap_ts_core<D, float>(P, g, sp, i, w, ps, pw);
-        n0 = key = window_n0<D, float>(g, w);
+        dmap_ts_core<D, R>(P, g, sp, i, w, ps, pw);
+        n0 = key = window_n0<D, R>(g, w);
     } else {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             w[a].base = 0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = R(0.0); w[a].dN[k] = R(0.0); }
         }
     }
     const Chain ch = chain_of(key, g.nny);
     const unsigned F = 0xffffffffu;
-    float s1[3], s2[3], q1[3], q2[3];
+    R s1[3], s2[3], q1[3], q2[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         s1[k] = __shfl_up_sync(F, ps[k], 1); s2[k] = __shfl_up_sync(F, ps[k], 2);
@@ -308,30 +308,30 @@ __global__ void __launch_bounds__(256, MPM_TS_DMAP_CHAIN_MINB) k_dmap_ts_chain(P
     constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-        const float wz = D == 3 ? w[2].N[c] : 1.0f;
+        const R wz = D == 3 ? w[2].N[c] : R(1.0);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float wxz = w[0].N[a] * wz;
-            const float N0 = wxz * w[1].N[0], N1 = wxz * w[1].N[1], N2 = wxz * w[1].N[2];
-            const float u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2), v2 = __shfl_up_sync(F, N2, 1);
-            const float a1 = ch.c1 ? u1 : 0.0f, a2 = ch.c2 ? u2 : 0.0f, b2 = ch.c1 ? v2 : 0.0f;
+            const R wxz = w[0].N[a] * wz;
+            const R N0 = wxz * w[1].N[0], N1 = wxz * w[1].N[1], N2 = wxz * w[1].N[2];
+            const R u1 = __shfl_up_sync(F, N1, 1), u2 = __shfl_up_sync(F, N2, 2), v2 = __shfl_up_sync(F, N2, 1);
+            const R a1 = ch.c1 ? u1 : R(0.0), a2 = ch.c2 ? u2 : R(0.0), b2 = ch.c1 ? v2 : R(0.0);
             const int col = n0 + a * g.nny + c * plane;
-            if (N0 + a1 + a2 != 0.0f) {
-                red_add4(&g.acc[col].a, 0.0f, N0 * ps[0] + a1 * s1[0] + a2 * s2[0], N0 * ps[1] + a1 * s1[1] + a2 * s2[1],
+            if (N0 + a1 + a2 != R(0.0)) {
+                red_add4(&g.acc[col].a, R(0.0), N0 * ps[0] + a1 * s1[0] + a2 * s2[0], N0 * ps[1] + a1 * s1[1] + a2 * s2[1],
                          N0 * ps[2] + a1 * s1[2] + a2 * s2[2]);
-                red_add4(&g.accw[col].a, 0.0f, N0 * pw[0] + a1 * q1[0] + a2 * q2[0],
+                red_add4(&g.accw[col].a, R(0.0), N0 * pw[0] + a1 * q1[0] + a2 * q2[0],
                          N0 * pw[1] + a1 * q1[1] + a2 * q2[1], N0 * pw[2] + a1 * q1[2] + a2 * q2[2]);
             }
             if (ch.end) {
-                if (N1 + b2 != 0.0f) {
-                    red_add4(&g.acc[col + 1].a, 0.0f, N1 * ps[0] + b2 * s1[0], N1 * ps[1] + b2 * s1[1],
+                if (N1 + b2 != R(0.0)) {
+                    red_add4(&g.acc[col + 1].a, R(0.0), N1 * ps[0] + b2 * s1[0], N1 * ps[1] + b2 * s1[1],
                              N1 * ps[2] + b2 * s1[2]);
-                    red_add4(&g.accw[col + 1].a, 0.0f, N1 * pw[0] + b2 * q1[0], N1 * pw[1] + b2 * q1[1],
+                    red_add4(&g.accw[col + 1].a, R(0.0), N1 * pw[0] + b2 * q1[0], N1 * pw[1] + b2 * q1[1],
                              N1 * pw[2] + b2 * q1[2]);
                 }
-                if (N2 != 0.0f) {
-                    red_add4(&g.acc[col + 2].a, 0.0f, N2 * ps[0], N2 * ps[1], N2 * ps[2]);
-                    red_add4(&g.accw[col + 2].a, 0.0f, N2 * pw[0], N2 * pw[1], N2 * pw[2]);
+                if (N2 != R(0.0)) {
+                    red_add4(&g.acc[col + 2].a, R(0.0), N2 * ps[0], N2 * ps[1], N2 * ps[2]);
+                    red_add4(&g.accw[col + 2].a, R(0.0), N2 * pw[0], N2 * pw[1], N2 * pw[2]);
                 }
             }
         }
@@ -488,22 +488,22 @@ __global__ void __launch_bounds__(256) k_g2p_ts(PDev<D, R> P, GDev<R> g, StepPar
 // are reduced per node as in p2g_scatter_ts.  The record groups are scattered
 // in separate sweeps over the window, so only one group's factors are live at
 // a time.  All lanes call it.
-template <int D>
-__device__ __forceinline__ void p2g_scatter_ts_chain(const GDev<float> &g, const AxisW<float> *w, int n0, int key,
-                                                     float ms, float mw, float n, float vol, const float *vs,
-                                                     const float *vw, const float *s, float sw, float G, float kperm) {
+template <int D, typename R = float>
+__device__ __forceinline__ void p2g_scatter_ts_chain(const GDev<R> &g, const AxisW<R> *w, int n0, int key,
+                                                     R ms, R mw, R n, R vol, const R *vs,
+                                                     const R *vw, const R *s, R sw, R G, R kperm) {
     const Chain ch = chain_of(key, g.nny);
-    const float one_n = 1.0f - n;
-    const float mi = one_n * ms + n * mw;
-    const float mwn = mw * n;
+    const R one_n = R(1.0) - n;
+    const R mi = one_n * ms + n * mw;
+    const R mwn = mw * n;
     // force records, per node: σ̃ = -Ω (σ + σw I) by rows, σ̃w = -Ω σw
     {
-        const float swv = -vol * sw;
-        float t[3][3];
+        const R swv = -vol * sw;
+        R t[3][3];
         if (D == 2) {
-            t[0][0] = -vol * s[0] + swv; t[0][1] = -vol * s[3]; t[0][2] = 0.0f;
-            t[1][0] = -vol * s[3]; t[1][1] = -vol * s[1] + swv; t[1][2] = 0.0f;
-            t[2][0] = t[2][1] = t[2][2] = 0.0f;
+            t[0][0] = -vol * s[0] + swv; t[0][1] = -vol * s[3]; t[0][2] = R(0.0);
+            t[1][0] = -vol * s[3]; t[1][1] = -vol * s[1] + swv; t[1][2] = R(0.0);
+            t[2][0] = t[2][1] = t[2][2] = R(0.0);
         } else {
             t[0][0] = -vol * s[0] + swv; t[0][1] = -vol * s[3]; t[0][2] = -vol * s[5];
             t[1][0] = -vol * s[3]; t[1][1] = -vol * s[1] + swv; t[1][2] = -vol * s[4];
@@ -513,47 +513,47 @@ __device__ __forceinline__ void p2g_scatter_ts_chain(const GDev<float> &g, const
         constexpr int NC = D == 3 ? 3 : 1;
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-            const float wz = D == 3 ? w[2].N[c] : 1.0f, gz = D == 3 ? w[2].dN[c] : 0.0f;
+            const R wz = D == 3 ? w[2].N[c] : R(1.0), gz = D == 3 ? w[2].dN[c] : R(0.0);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                const float wx = w[0].N[a], gx = w[0].dN[a];
+                const R wx = w[0].N[a], gx = w[0].dN[a];
                 const int col = n0 + a * g.nny + c * plane;
 #pragma unroll
                 for (int b = 0; b < 3; ++b) {
-                    const float wy = w[1].N[b], gy = w[1].dN[b];
-                    const float N = wx * wy * wz;
-                    if (N == 0.0f) continue;
-                    const float dN[3] = {gx * wy * wz, wx * gy * wz, wx * wy * gz};
-                    float fs[3], fw[3];
+                    const R wy = w[1].N[b], gy = w[1].dN[b];
+                    const R N = wx * wy * wz;
+                    if (N == R(0.0)) continue;
+                    const R dN[3] = {gx * wy * wz, wx * gy * wz, wx * wy * gz};
+                    R fs[3], fw[3];
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         fs[k] = dN[0] * t[k][0] + dN[1] * t[k][1] + dN[2] * t[k][2];
-                        fw[k] = k < D ? dN[k] * swv : 0.0f;
+                        fw[k] = k < D ? dN[k] * swv : R(0.0);
                     }
                     fs[D - 1] += N * mi * G;
                     fw[D - 1] += N * mw * G;
                     red_add4(&g.acc[col + b].b, fs[0], fs[1], fs[2], N * mwn);
-                    red_add4(&g.accw[col + b].b, fw[0], fw[1], fw[2], 0.0f);
+                    red_add4(&g.accw[col + b].b, fw[0], fw[1], fw[2], R(0.0));
                 }
             }
         }
     }
     // N-proportional records: acc.a = N·A, accw.a = N·B, accd = N·C
     {
-        float A[4] = {ms * one_n, 0.0f, 0.0f, 0.0f};
+        R A[4] = {ms * one_n, R(0.0), R(0.0), R(0.0)};
 #pragma unroll
         for (int d = 0; d < D; ++d) A[1 + d] = ms * vs[d] * one_n;
         chain_nprop<D, 4>(g, w, n0, ch, A, [&](int i) { return &g.acc[i].a; });
     }
     {
-        float B[4] = {mw, 0.0f, 0.0f, 0.0f};
+        R B[4] = {mw, R(0.0), R(0.0), R(0.0)};
 #pragma unroll
         for (int d = 0; d < D; ++d) B[1 + d] = mw * vw[d] * n;
         chain_nprop<D, 4>(g, w, n0, ch, B, [&](int i) { return &g.accw[i].a; });
     }
     {
-        const float tdg = kperm != 0.0f ? (n * mw * G) / kperm : 0.0f;
-        float Cv[3] = {0.0f, 0.0f, 0.0f};
+        const R tdg = kperm != R(0.0) ? (n * mw * G) / kperm : R(0.0);
+        R Cv[3] = {R(0.0), R(0.0), R(0.0)};
 #pragma unroll
         for (int d = 0; d < D; ++d) Cv[d] = tdg * (vw[d] - vs[d]);
         chain_nprop<D, 3>(g, w, n0, ch, Cv, [&](int i) { return &g.accd[i]; });
@@ -561,42 +561,42 @@ __device__ __forceinline__ void p2g_scatter_ts_chain(const GDev<float> &g, const
 }
 
 // The fused two-phase pass (FP32) with the lane-merged scatter.
-template <int D, bool MC3 = false>
-__global__ void __launch_bounds__(256, MPM_TS_P_MINB) k_g2p_ts_chain(PDev<D, float> P, GDev<float> g, StepParams sp) {
+template <int D, bool MC3 = false, typename R = float>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_TS_P_MINB_F64 : MPM_TS_P_MINB) k_g2p_ts_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool live = i < sp.np;
     double x[3];
-    AxisW<float> w[3];
-    float s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, nn = 0, sw = 0, kperm = 0;
-    float vs[3] = {0, 0, 0}, vw[3] = {0, 0, 0}, ms = 0, mw = 0;
+    AxisW<R> w[3];
+    R s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, nn = 0, sw = 0, kperm = 0;
+    R vs[3] = {0, 0, 0}, vw[3] = {0, 0, 0}, ms = 0, mw = 0;
     if (live) {
-        g2p_ts_core<D, float, MC3>(P, g, sp, i, x, w, s, vol, nn, sw, kperm);
-        if (!particle_weights<D, float>(x, g, w)) {
+        g2p_ts_core<D, R, MC3>(P, g, sp, i, x, w, s, vol, nn, sw, kperm);
+        if (!particle_weights<D, R>(x, g, w)) {
             atomicOr(g.err, ERR_OOG);
             live = false;
         } else {
-            load_vel<D, float>(P.v, i, vs);
-            load_vel<D, float>(P.vw, i, vw);
+            load_vel<D, R>(P.v, i, vs);
+            load_vel<D, R>(P.vw, i, vw);
             ms = P.m[i];
             mw = P.mw[i];
         }
     }
     int n0 = 0, key = dead_key();
     if (live) {
-        n0 = key = window_n0<D, float>(g, w);
+        n0 = key = window_n0<D, R>(g, w);
     } else {
-        ms = mw = vol = 0.0f;
+        ms = mw = vol = R(0.0);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             w[a].base = 0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { w[a].N[k] = 0.0f; w[a].dN[k] = 0.0f; }
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = R(0.0); w[a].dN[k] = R(0.0); }
         }
     }
     MarkState mk;
-    if (live) mk = mark_begin<D, float>(g, w);
-    p2g_scatter_ts_chain<D>(g, w, n0, key, ms, mw, nn, vol, vs, vw, s, sw, (float)sp.G, kperm);
-    if (live) mark_end<float>(g, mk);
+    if (live) mk = mark_begin<D, R>(g, w);
+    p2g_scatter_ts_chain<D, R>(g, w, n0, key, ms, mw, nn, vol, vs, vw, s, sw, (R)sp.G, kperm);
+    if (live) mark_end<R>(g, mk);
 }
 
 }  // namespace mpm
