@@ -52,6 +52,8 @@
 #ifndef MPM_TS_P_MINB
 #define MPM_TS_P_MINB 4
 #endif
+// the two-phase fused pass in FP64: 2 CTAs (128 registers) ran 5.86 ms per step
+// on the 2.56 M saturated column against 5.96 at 3
 #ifndef MPM_TS_P_MINB_F64
 #define MPM_TS_P_MINB_F64 2
 #endif
