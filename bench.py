@@ -5,7 +5,7 @@ Workload (per GPU): 3D column collapse, domain 1.2 x 0.4 x 0.6 m, h = 5 mm,
 column 0.5 x 0.2 x 0.4 m at 2x2x2 particles per cell = 2 560 000 particles,
 Mohr-Coulomb (phi = 30 deg, c = 0, psi = 0), rho = 2650, E = 1 MPa, nu = 0.3,
 free-slip walls, CFL 0.2, FP32 bulk with FP64 positions and det(F).  A bench
-step is one MPM time step over all particles (cell re-sort every 16 steps
+step is one MPM time step over all particles (cell re-sort every 32 steps
 included).  The particle state (~0.5 GB) exceeds the 126 MB L2, so no flush is
 needed between steps.
 
@@ -287,7 +287,7 @@ def run_b200(args):
         return t1 - t0
 
     # warm: context, module load, first allocations, and the first CUDA-graph
-    # capture/instantiation (a block of two sort periods is replayed after 16 steps)
+    # capture/instantiation (a block of two sort periods is replayed once a period has passed)
     e2e_once(max(W, 40))
     e2e_t = e2e_once(K)
     D = case.grid.dim
