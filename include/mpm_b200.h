@@ -243,16 +243,18 @@ int mpm_download_grid(mpm_handle *h, int32_t field, double *out);
 /* ---- cell ordering without allocation ----
  * No counterpart in the reference (which never reorders particles).  For
  * callers that cannot allocate device memory -- a host runtime that owns all
- * device memory through its own pool, code running while a CUDA graph is
- * being captured, a real-time loop that must not hit the allocator's implicit
- * synchronisation -- this computes what mpm_compute_p2c() and mpm_sort() +
+ * device memory through its own pool, a real-time loop that must not hit the
+ * allocator's implicit synchronisation -- this computes what mpm_compute_p2c() and mpm_sort() +
  * mpm_download_order() compute for particles in their original order:
  * p2c_out[i] (1-based, the reference's formula) and order_out[k] (0-based
  * index of the k-th particle in the library's cell-sorted order).  All five
  * pointers are caller-owned DEVICE buffers (x, y, z: np FP64 coordinates; z is
  * unused in 2D; order_out, p2c_out: np int64).  The grid and np come from
  * `d` (the other descriptor fields are ignored).  The work runs on `stream`
- * (a cudaStream_t; NULL = default stream) and the call returns after it.
+ * (a cudaStream_t; NULL = the legacy default stream) and the call is
+ * synchronous: it copies an error word back and waits for the stream before
+ * returning, so it must not be called on a stream that is being captured, and
+ * should get a non-blocking stream while another thread captures a graph.
  *
  * The scratch is a fixed static device array of MPM_NOALLOC_SCRATCH_BYTES
  * that every GPU loading the library holds until process exit; np above
@@ -264,7 +266,7 @@ int mpm_download_grid(mpm_handle *h, int32_t field, double *out);
  * them on one stream or serialise them.  Errors: mpm_last_error(NULL). */
 #define MPM_NOALLOC_MAX_PARTICLES (1 << 19)
 #define MPM_NOALLOC_MAX_KEYS (1 << 19)
-#define MPM_NOALLOC_SCRATCH_BYTES 14731264
+#define MPM_NOALLOC_SCRATCH_BYTES 14780416
 int mpm_cell_order_noalloc(const mpm_desc *d, const double *x, const double *y, const double *z,
                            int64_t *order_out, int64_t *p2c_out, void *stream);
 
@@ -291,6 +293,10 @@ int mpm_grf_eval(int32_t device, const double *x, const double *y, const double 
  * gets bit 0 set if a tensor-core completion wait timed out. */
 int mpm_mlp_nparams(void);
 #define MPM_MLP_RESIDUAL 1   /* flags: the network predicts out - feat[0..5] (the correction) */
+/* flags, test hook of the tensor-core completion wait: issue no MMA and wait
+ * with a short limit, so the wait times out, *err gets bit 0 and no output is
+ * written; the context stays usable (nothing is in flight when the CTA leaves) */
+#define MPM_MLP_TEST_STALL 2
 int mpm_mlp_forward(const float *params, const float *norm, const float *feat, float *out, int64_t n,
                     int32_t flags, int *err, void *stream);
 /* Adds the gradient of 1/2 * inv_btot * sum (MLP(x) - y)^2 (normalised units)

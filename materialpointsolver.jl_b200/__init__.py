@@ -10,7 +10,6 @@ from .types import (Args2D, Args3D, Grid2D, Grid3D, Particle2D, Particle3D, Prop
 from . import workloads
 from . import randomfield
 from . import surrogate
-from . import precision
 from . import hdf5
 from . import _lib
 from .solver import (DeviceModel, host2device, device2host, clean_device, procedure,

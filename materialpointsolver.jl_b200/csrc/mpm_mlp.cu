@@ -128,8 +128,8 @@ __device__ __forceinline__ void issue_layer(uint32_t tmem_d, uint32_t a_saddr, u
 // Wait for the MMAs committed to `bar` (phase parity flips per use).  The
 // outcome is made CTA-uniform, so a timed-out wait takes every thread out of
 // the tile loop together.
-__device__ __forceinline__ bool layer_done(uint32_t bar, uint32_t &parity, int *err) {
-    const bool mine = mbar_wait(bar, parity);
+__device__ __forceinline__ bool layer_done(uint32_t bar, uint32_t &parity, int *err, int limit = 1 << 20) {
+    const bool mine = mbar_wait(bar, parity, limit);
     parity ^= 1u;
     const bool ok = __syncthreads_and(mine) != 0;
     if (!ok && threadIdx.x == 0) atomicOr(err, 1);
@@ -157,10 +157,16 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t trow, const float *bias
 
 // ---------------------------------------------------------------------------
 // Inference: out[i, 0..5] = MLP(feat[i, 0..15]) in physical units.
+// flags bit 0: residual (the network predicts out - feat[0..5]); bit 1: the
+// timeout test of mpm_mlp_forward (MPM_MLP_TEST_STALL) -- no MMA and no commit
+// is issued, so nothing is in flight when the short wait gives up.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(TILE) k_mlp_forward(const float *__restrict__ P, const float *__restrict__ norm,
                                                       const float *__restrict__ feat, float *__restrict__ out,
-                                                      int64_t n, const uint32_t *n_dev, int residual, int *err) {
+                                                      int64_t n, const uint32_t *n_dev, int flags, int *err) {
+    const int residual = flags & 1;
+    const bool stall = (flags & 2) != 0;
+    const int limit = stall ? (1 << 10) : (1 << 20);
     if (n_dev) n = min(n, (int64_t)*n_dev);   // rows counted on the device, capped by the buffers
     extern __shared__ __align__(128) uint8_t smem_raw[];
     uint8_t *p = smem_raw;
@@ -203,11 +209,11 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const float *__restrict__ 
         fence_proxy_async();
         __syncthreads();
         // layer 0
-        if (t == 0) {
+        if (t == 0 && !stall) {
             fence_after_sync();
             issue_layer(tmem, smem_u32(S.x), smem_u32(S.wT[0]), 16, 64, bar);
         }
-        ok = layer_done(bar, parity, err);
+        ok = layer_done(bar, parity, err, limit);
         if (!ok) break;
         hidden_epilogue(trow, S.bias, S.a, nullptr);
         fence_before_sync();
@@ -295,7 +301,7 @@ extern "C" int mpm_mlp_forward(const float *params, const float *norm, const flo
         const int64_t ntiles = (n + TILE - 1) / TILE;
         const int grid = (int)(ntiles < mpm_detail::MLP_FWD_CTAS_PER_SM * nsm ? ntiles
                                                                               : mpm_detail::MLP_FWD_CTAS_PER_SM * nsm);
-        k_mlp_forward<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, out, n, nullptr, flags & 1, err);
+        k_mlp_forward<<<grid, TILE, smem, (cudaStream_t)stream>>>(params, norm, feat, out, n, nullptr, flags & 3, err);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {

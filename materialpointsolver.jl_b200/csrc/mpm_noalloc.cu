@@ -3,9 +3,8 @@
 //
 // Some host environments call into this library from places where
 // cudaMalloc is not available or not allowed: a host runtime that owns all
-// device memory through its own pool and forbids foreign allocations, code
-// that runs while a CUDA graph is being captured elsewhere on the device, or
-// a real-time loop that must not trigger the allocator's implicit
+// device memory through its own pool and forbids foreign allocations, or a
+// real-time loop that must not trigger the allocator's implicit
 // synchronisation.  For them, mpm_cell_order_noalloc() computes the same
 // particle-to-cell indices and the same cell-sorted particle order as
 // mpm_sort() + mpm_download_order(), using only the caller's input and output
@@ -14,6 +13,9 @@
 // library, held until the process exits).
 //
 // Nothing here calls cudaMalloc, cudaFree or an allocating library routine.
+// The call is synchronous: it reads the sort's error word back and waits for
+// its stream before returning, so it must not be issued on a stream that is
+// being captured into a graph.
 #include "../../include/mpm_b200.h"
 #include "mpm_sort.cuh"
 
@@ -34,7 +36,11 @@ namespace {
 
 constexpr int64_t NA_NP = MPM_NOALLOC_MAX_PARTICLES;
 constexpr int64_t NA_NK = MPM_NOALLOC_MAX_KEYS;
-constexpr uint32_t NA_BIG_CAP = 4096;
+// cells holding more than BUCKET_SMALL particles are queued for the CTA sort;
+// np <= NA_NP particles fill at most NA_NP / (BUCKET_SMALL + 1) such cells, so
+// the queue (rounded up to a power of two) can never overflow
+constexpr uint32_t NA_BIG_CAP = 16384;
+static_assert((int64_t)NA_BIG_CAP >= NA_NP / (BUCKET_SMALL + 1) + 1, "big-bucket queue smaller than the worst case");
 
 // scratch layout (byte offsets, each 256-byte aligned)
 constexpr size_t al(size_t b) { return (b + 255) / 256 * 256; }
@@ -57,8 +63,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[MPM_NOALLOC_SCR
 
 constexpr int MAX_DEV = 64;
 unsigned char *g_scratch_ptr[MAX_DEV] = {};
-std::once_flag g_once[MAX_DEV];
-cudaError_t g_setup_err[MAX_DEV] = {};
+std::mutex g_setup_mu;
 
 template <int D>
 __global__ void k_na_keys(const double *x, const double *y, const double *z, int64_t np, AxisC<float> ax,
@@ -182,15 +187,21 @@ extern "C" int mpm_cell_order_noalloc(const mpm_desc *d, const double *x, const 
     int dev = 0;
     NA_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= MAX_DEV) return na_fail(MPM_E_ARG, "mpm_cell_order_noalloc: device ordinal out of range");
-    // one-time set-up per device, with that device current: the scratch's device address
-    std::call_once(g_once[dev], [dev] {
-        void *p = nullptr;
-        g_setup_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (g_setup_err[dev] == cudaSuccess) g_scratch_ptr[dev] = (unsigned char *)p;
-    });
-    if (g_setup_err[dev] != cudaSuccess || !g_scratch_ptr[dev])
-        return na_fail(MPM_E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(g_setup_err[dev]));
+    // set-up per device, with that device current: the scratch's device
+    // address.  A failed lookup is not remembered, so a later call retries it.
+    unsigned char *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_setup_mu);
+        if (!g_scratch_ptr[dev]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p)
+                return na_fail(MPM_E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+            g_scratch_ptr[dev] = (unsigned char *)p;
+        }
+        scratch = g_scratch_ptr[dev];
+    }
     cudaStream_t st = (cudaStream_t)stream;
-    return d->dim == 2 ? run<2>(d, x, y, z, order_out, p2c_out, st, g_scratch_ptr[dev])
-                       : run<3>(d, x, y, z, order_out, p2c_out, st, g_scratch_ptr[dev]);
+    return d->dim == 2 ? run<2>(d, x, y, z, order_out, p2c_out, st, scratch)
+                       : run<3>(d, x, y, z, order_out, p2c_out, st, scratch);
 }

@@ -91,8 +91,9 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 }
 
 // bounded wait for the given phase parity; false if it never completed
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int it = 0; it < (1 << 20); ++it) {
+// within `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit = 1 << 20) {
+    for (int it = 0; it < limit; ++it) {
         uint32_t ok;
         asm volatile(
             "{\n\t"

@@ -198,41 +198,3 @@ def collect_samples(dev, dt, Ti, nsteps, cap, every=1, device=0):
 
 
 FLOP_FORWARD = 2 * (NF * 64 + 64 * 64 + 64 * 64 + 64 * NO)   # 19 072 per sample (unpadded)
-
-
-def benchmark(n=2_000_000, reps=20, device=0):
-    """Time the tensor-core forward and gradient kernels on n random samples;
-    prints and returns samples/s and TFLOP/s (unpadded FLOP count; the
-    backward counts twice the forward)."""
-    import json
-    import torch
-    d = torch.device("cuda", device)
-    g = torch.Generator(device=d)
-    g.manual_seed(0)
-    feat = torch.randn((n, NFP), generator=g, device=d)
-    feat[:, NF] = 0
-    tgt = torch.randn((n, NO), generator=g, device=d)
-    sur = Surrogate(seed=0, device=device, residual=False)
-    sur.set_norm(feat[:4096].cpu().numpy(), tgt[:4096].cpu().numpy())
-    for _ in range(3):
-        sur.forward(feat)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        sur.forward(feat)
-    e1.record()
-    torch.cuda.synchronize()
-    fwd_ms = e0.elapsed_time(e1) / reps
-    sur._grad(feat, tgt, 1.0 / n)
-    e0.record()
-    for _ in range(reps):
-        sur._grad(feat, tgt, 1.0 / n)
-    e1.record()
-    torch.cuda.synchronize()
-    grad_ms = e0.elapsed_time(e1) / reps
-    sur._check_err()
-    out = {"samples": n, "forward_ms": fwd_ms, "forward_samples_per_s": n / (fwd_ms * 1e-3),
-           "forward_tflops": n * FLOP_FORWARD / (fwd_ms * 1e-3) / 1e12,
-           "grad_ms": grad_ms, "grad_tflops": 3 * n * FLOP_FORWARD / (grad_ms * 1e-3) / 1e12}
-    print(json.dumps(out))
-    return out

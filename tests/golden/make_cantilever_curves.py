@@ -5,14 +5,16 @@ docs/assets/data/2d_cantileverbeam_data/ of the reference repository: the FEM
 solution (FEM_cantilever_beam.csv) and the published uGIMP and CPDI MPM curves
 (MPM_uGIMP.csv, MPM_CPDI.csv); time in s, vertical displacement of the bottom
 corner particle at the free end in m, each curve sorted by time.  Run from the
-repository root with the reference checked out at REFERENCE (default
-/root/reference)."""
+repository root with the reference checked out at the directory that the
+environment variable REFERENCE names (required)."""
 import csv
 import json
 import os
 import sys
 
-REF = os.environ.get("REFERENCE", "/root/reference")
+REF = os.environ.get("REFERENCE")
+if not REF:
+    sys.exit("set REFERENCE to the MaterialPointSolver.jl checkout to read its data files from")
 SRC = os.path.join(REF, "docs", "assets", "data", "2d_cantileverbeam_data")
 
 

@@ -2,14 +2,16 @@
 line of the 2D granular column collapse that MaterialPointSolver.jl ships with
 its validation case (docs/assets/data/2d_collapse_experiments/surface.csv and
 failure.csv of the reference repository; x, y in metres).  Run from the
-repository root with the reference checked out at REFERENCE (default
-/root/reference)."""
+repository root with the reference checked out at the directory that the
+environment variable REFERENCE names (required)."""
 import csv
 import json
 import os
 import sys
 
-REF = os.environ.get("REFERENCE", "/root/reference")
+REF = os.environ.get("REFERENCE")
+if not REF:
+    sys.exit("set REFERENCE to the MaterialPointSolver.jl checkout to read its data files from")
 SRC = os.path.join(REF, "docs", "assets", "data", "2d_collapse_experiments")
 
 

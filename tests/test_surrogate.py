@@ -112,3 +112,34 @@ def test_residual_mode_adds_the_trial_stress(pkg, gpu_lib):
     oa = a.forward(x).cpu().numpy()
     ob = b.forward(x).cpu().numpy()
     assert np.allclose(ob, oa + feat[:, :6], rtol=1e-6, atol=1e-5 * np.abs(oa).max())
+
+
+@pytest.mark.gpu
+def test_completion_wait_timeout_is_reported(pkg, gpu_lib):
+    """The bounded wait on the tensor-core completion barrier: with the test
+    flag no MMA (and no commit) is issued, so the first wait runs out after
+    its short limit; the kernel sets the error word and leaves with nothing in
+    flight.  The host sees the error, and a normal call on the same context
+    afterwards still succeeds and matches a fresh one."""
+    import ctypes as C
+    import torch
+    feat, target, P, norm = rand_case(pkg, 300, seed=8)
+    sur = gpu_surrogate(pkg, P, norm)
+    x = torch.tensor(feat, device="cuda")
+    good = sur.forward(x).cpu().numpy()
+    out = torch.full((x.shape[0], 6), 7.0, device="cuda")
+    sur.err.zero_()
+    rc = gpu_lib.mpm_mlp_forward(sur.P.data_ptr(), sur.norm.data_ptr(), x.data_ptr(), out.data_ptr(),
+                                 x.shape[0], sur.flags | 2, sur.err.data_ptr(),
+                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(sur.err.item()) & 1, "the timed-out wait was not reported"
+    assert torch.all(out == 7.0), "a timed-out tile wrote output"
+    with pytest.raises(pkg._lib.MPMError):
+        sur._check_err()
+    sur.err.zero_()
+    again = sur.forward(x).cpu().numpy()
+    torch.cuda.synchronize()
+    assert int(sur.err.item()) == 0
+    assert np.array_equal(again, good)
