@@ -259,7 +259,7 @@ int mpm_download_grid(mpm_handle *h, int32_t field, double *out);
  * The scratch is a fixed static device array of MPM_NOALLOC_SCRATCH_BYTES
  * that every GPU loading the library holds until process exit; np above
  * MPM_NOALLOC_MAX_PARTICLES or a grid above MPM_NOALLOC_MAX_KEYS cell keys
- * (cells rounded up to whole 4x8x4 / 8x8 tiles) is rejected with MPM_E_ARG.
+ * (cells rounded up to whole 2x8x2 / 4x8 tiles) is rejected with MPM_E_ARG.
  * The first call on each device looks up the scratch's device address (with
  * that device current); make it before any stream capture.  All calls share
  * the one scratch array, so calls whose work overlaps on the GPU race: issue

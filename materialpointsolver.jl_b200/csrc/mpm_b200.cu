@@ -5,6 +5,7 @@
 // cell sort.  Kernels live in mpm_kernels.cuh / mpm_sort.cuh.
 #include "../../include/mpm_b200.h"
 #include "mpm_tiled.cuh"
+#include "mpm_box.cuh"
 #include "mpm_ts.cuh"
 
 #include <cuda_runtime.h>
@@ -115,6 +116,8 @@ struct mpm_handle {
     bool prefetch = true;    // FP32 particle pass stages fields by cp.async (MPM_B200_PREFETCH=0 turns it off)
     bool cell_major = false; // order inside a tile: rank-major (default) or cell-major (MPM_B200_ORDER=cell)
     bool chain = true;       // FP32 scatters merge chained warp lanes (MPM_B200_CHAIN=0 turns it off)
+    bool box = true;         // FP32 MUSL passes with the tile's nodes in shared memory (MPM_B200_BOX=0: off)
+    uint32_t *work = nullptr;   // tile counters of the box passes
     GraphCache graph;
     int64_t graph_launches = 0;
     // stress-return surrogate: 1 = log samples into caller buffers, 2 = infer
@@ -466,13 +469,18 @@ template <int D, typename R> void do_sort(mpm_handle *h) {
     k_sort_buckets<<<cdiv(h->nk, 256), 256, 0, st>>>(h->off, h->nk, h->pairs, h->big, h->nbig, h->big_cap, h->err);
     k_sort_big<<<64, 512, 0, st>>>(h->off, h->big, h->nbig, h->big_cap, h->pairs);
     CK(cudaMemsetAsync(h->ntiles, 0, 4, st));
-    k_tile_list<<<cdiv(h->ntile_total, 256), 256, 0, st>>>(h->off, h->ntile_total, Tile<D>::CPT, h->tiles, h->ntiles);
+    const int cpt = h->sg.cpt;
+    k_tile_list<<<cdiv(h->ntile_total, 256), 256, 0, st>>>(h->off, h->ntile_total, (uint32_t)cpt, h->tiles, h->ntiles);
     if (h->cell_major) {
-        // particles of a cell stay consecutive (tile-major, then cell, then original index)
+        // particles of a cell stay consecutive (tile-major, then cell, then (octant, original index))
         k_permute<D, R><<<cdiv(np, 256), 256, 0, st>>>(A, B, h->pairs, np);
     } else {
-        k_tile_transpose<Tile<D>::CPT><<<h->nsm * 8, Tile<D>::CPT, 0, st>>>(h->off, h->tiles, h->ntiles, h->pairs,
-                                                                             h->pairs2);
+        if (cpt == 32)
+            k_tile_transpose<32><<<h->nsm * 16, 32, 0, st>>>(h->off, h->tiles, h->ntiles, h->pairs, h->pairs2);
+        else if (cpt == 64)
+            k_tile_transpose<64><<<h->nsm * 16, 64, 0, st>>>(h->off, h->tiles, h->ntiles, h->pairs, h->pairs2);
+        else
+            k_tile_transpose<128><<<h->nsm * 8, 128, 0, st>>>(h->off, h->tiles, h->ntiles, h->pairs, h->pairs2);
         k_permute<D, R><<<cdiv(np, 256), 256, 0, st>>>(A, B, h->pairs2, np);
     }
     LAUNCH_CHECK();
@@ -605,6 +613,81 @@ template <int D, typename R> const TiledCfg &tiled_cfg(mpm_handle *h, int need_v
     return cc;
 }
 
+// ---- box passes (mpm_box.cuh) ---------------------------------------------------------
+// Tile shapes with compiled box passes (32 cells each).
+#define MPM_BOX_SHAPES_3D(X) X(3, 2, 8, 2) X(3, 4, 8, 1) X(3, 4, 4, 2)
+#define MPM_BOX_SHAPES_2D(X) X(2, 4, 8, 1) X(2, 2, 16, 1)
+
+template <int D, int TX, int TY, int TZ> struct BoxPass {
+    using G = BoxGeo<D, TX, TY, TZ>;
+    static constexpr size_t G2P_SMEM = (size_t)MPM_BOX_WARPS * G::G2P_BYTES;
+    static constexpr size_t DM_SMEM = (size_t)MPM_BOX_WARPS * G::DM_BYTES;
+    static void prepare() {
+        CK(cudaFuncSetAttribute(k_g2p_box<D, TX, TY, TZ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)G2P_SMEM));
+        if (D == 3)
+            CK(cudaFuncSetAttribute(k_g2p_box<D, TX, TY, TZ, D == 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)G2P_SMEM));
+        CK(cudaFuncSetAttribute(k_dmap_box<D, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)DM_SMEM));
+    }
+    static void dmap(mpm_handle *h, const PDev<D, float> &P, const GDev<float> &g, const StepParams &sp,
+                     const BoxTiles &bt) {
+        k_dmap_box<D, TX, TY, TZ><<<h->nsm * MPM_BOX_DMAP_MINB, MPM_BOX_WARPS * 32, DM_SMEM, h->stream>>>(P, g, sp,
+                                                                                                        bt);
+    }
+    static void g2p(mpm_handle *h, const PDev<D, float> &P, const GDev<float> &g, const StepParams &sp,
+                    const BoxTiles &bt, bool mc3) {
+        if (mc3 && D == 3)
+            k_g2p_box<D, TX, TY, TZ, D == 3><<<h->nsm * MPM_BOX_G2P_MINB, MPM_BOX_WARPS * 32, G2P_SMEM, h->stream>>>(
+                P, g, sp, bt);
+        else
+            k_g2p_box<D, TX, TY, TZ, false><<<h->nsm * MPM_BOX_G2P_MINB, MPM_BOX_WARPS * 32, G2P_SMEM, h->stream>>>(
+                P, g, sp, bt);
+    }
+};
+
+// Shared-memory limits of the box passes (outside any stream capture).
+void box_prepare(mpm_handle *h) {
+#define MPM_BOX_PREP(D, A, B, C) \
+    if (h->d.dim == D) BoxPass<D, A, B, C>::prepare();
+    MPM_BOX_SHAPES_3D(MPM_BOX_PREP)
+    MPM_BOX_SHAPES_2D(MPM_BOX_PREP)
+#undef MPM_BOX_PREP
+}
+
+// Does the handle's tile shape have box passes?
+bool box_shape_ok(const mpm_handle *h) {
+    const SortGeom &sg = h->sg;
+#define MPM_BOX_HAS(D, A, B, C) \
+    if (h->d.dim == D && sg.tx == A && sg.ty == B && (D == 2 || sg.tz == C)) return true;
+    MPM_BOX_SHAPES_3D(MPM_BOX_HAS)
+    MPM_BOX_SHAPES_2D(MPM_BOX_HAS)
+#undef MPM_BOX_HAS
+    return false;
+}
+
+// One box pass (which = 0: double mapping, 1: fused G2P + next P2G) with the
+// handle's tile shape.
+template <int D> void box_launch(mpm_handle *h, int which, const PDev<D, float> &P, const GDev<float> &g,
+                                 const StepParams &sp, bool mc3) {
+    BoxTiles bt{h->tiles, h->ntiles, h->off, h->work + which, h->sg};
+    CK(cudaMemsetAsync(h->work + which, 0, 4, h->stream));
+    const SortGeom &sg = h->sg;
+#define MPM_BOX_GO(DD, A, B, C)                                                                 \
+    if constexpr (D == DD) {                                                                    \
+        if (sg.tx == A && sg.ty == B && (DD == 2 || sg.tz == C)) {                              \
+            if (which == 0) BoxPass<DD, A, B, C>::dmap(h, P, g, sp, bt);                        \
+            else BoxPass<DD, A, B, C>::g2p(h, P, g, sp, bt, mc3);                               \
+            return;                                                                             \
+        }                                                                                       \
+    }
+    MPM_BOX_SHAPES_3D(MPM_BOX_GO)
+    MPM_BOX_SHAPES_2D(MPM_BOX_GO)
+#undef MPM_BOX_GO
+    throw Err{MPM_E_STATE, "no box pass for this tile shape"};
+}
+
 // The launches of one step (solve, double mapping, DM3, fused G2P + next P2G).
 template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double dt, double Ti, double Tn) {
     const int64_t np = h->d.np;
@@ -712,6 +795,14 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
             });
         }
         L.run("p2g", [&] { k_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+    } else if (std::is_same<R, float>::value && h->box && sp.va == MPM_VA_A && !sp.need_vs && box_shape_ok(h)) {
+        // FP32 MUSL :a: the box passes (node data of a tile in shared memory)
+        if constexpr (std::is_same<R, float>::value) {
+            if (np) L.run("dmap", [&] { box_launch<D>(h, 0, P, g, sp, mc3); });
+            L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
+            CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
+            if (np) L.run("g2p_p2g", [&] { box_launch<D>(h, 1, P, g, sp, mc3); });
+        }
     } else {
         const bool chain = h->chain;
         if (np) L.run("dmap", [&] {
@@ -1457,19 +1548,22 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         h->mat = dalloc(h, d->nmat * msz);
         h->err = (int *)dalloc(h, 4);
         CK(cudaMemset(h->err, 0, 4));
-        // sort geometry
+        // sort geometry: tiles of 32 cells by default (MPM_B200_TILE=AxBxC picks
+        // another shape: 32, 64 or 128 cells)
         SortGeom &sg = h->sg;
-        sg.ncx = (int)(d->nnx - 1);
-        sg.ncy = (int)(d->nny - 1);
-        sg.ncz = d->dim == 3 ? (int)(nnz - 1) : 1;
-        if (d->dim == 3) {
-            sg.ntx = (int)cdiv(sg.ncx, Tile<3>::TX); sg.nty = (int)cdiv(sg.ncy, Tile<3>::TY); sg.ntz = (int)cdiv(sg.ncz, Tile<3>::TZ);
-            h->nk = (uint32_t)((int64_t)sg.ntx * sg.nty * sg.ntz * Tile<3>::CPT);
-        } else {
-            sg.ntx = (int)cdiv(sg.ncx, Tile<2>::TX); sg.nty = (int)cdiv(sg.ncy, Tile<2>::TY); sg.ntz = 1;
-            h->nk = (uint32_t)((int64_t)sg.ntx * sg.nty * Tile<2>::CPT);
+        int tsh[3] = {d->dim == 3 ? Tile<3>::TX : Tile<2>::TX, d->dim == 3 ? Tile<3>::TY : Tile<2>::TY,
+                      d->dim == 3 ? Tile<3>::TZ : 1};
+        if (const char *e = getenv("MPM_B200_TILE")) {
+            int a = 0, b = 0, c = 1;
+            if (std::sscanf(e, "%dx%dx%d", &a, &b, &c) >= 2) { tsh[0] = a; tsh[1] = b; tsh[2] = d->dim == 3 ? c : 1; }
         }
-        sg.nk = h->nk;
+        const int cpt = tsh[0] * tsh[1] * tsh[2];
+        if (tsh[0] < 1 || tsh[1] < 1 || tsh[2] < 1 || (cpt != 32 && cpt != 64 && cpt != 128))
+            throw Err{MPM_E_ARG, "tile shape must hold 32, 64 or 128 cells"};
+        const int64_t nk = sort_geom(sg, d->dim, d->nnx, d->nny, nnz, tsh[0], tsh[1], tsh[2]);
+        if (nk >= (int64_t)LOW29 || d->np >= (int64_t)LOW29)
+            throw Err{MPM_E_ARG, "grid or particle count beyond the sort's 2^29 limit"};
+        h->nk = (uint32_t)nk;
         int64_t npa = std::max<int64_t>(d->np, 1);
         h->keys = (uint32_t *)dalloc(h, npa * 4);
         h->cnt = (uint32_t *)dalloc(h, (size_t)h->nk * 4);
@@ -1480,7 +1574,7 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         h->nbig = (uint32_t *)dalloc(h, 4);
         h->pairs = (uint2 *)dalloc(h, npa * 8);
         h->pairs2 = (uint2 *)dalloc(h, npa * 8);
-        h->ntile_total = h->nk / (d->dim == 3 ? Tile<3>::CPT : Tile<2>::CPT);
+        h->ntile_total = h->nk / (uint32_t)sg.cpt;
         h->tiles = (uint32_t *)dalloc(h, (size_t)h->ntile_total * 4);
         h->ntiles = (uint32_t *)dalloc(h, 4);
         CK(cudaMemset(h->ntiles, 0, 4));
@@ -1496,6 +1590,9 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         if (const char *e = getenv("MPM_B200_PREFETCH")) h->prefetch = (e[0] != '0');
         if (const char *e = getenv("MPM_B200_ORDER")) h->cell_major = (std::string(e) == "cell");
         if (const char *e = getenv("MPM_B200_CHAIN")) h->chain = std::atoi(e) != 0;
+        if (const char *e = getenv("MPM_B200_BOX")) h->box = std::atoi(e) != 0;
+        h->work = (uint32_t *)dalloc(h, 16);
+        if (!h->fp64) box_prepare(h);
         *out = h;
         return MPM_OK;
     } catch (const Err &e) {

@@ -109,9 +109,22 @@ template <typename R> __device__ __forceinline__ void ugimp1(R d, const AxisC<R>
 }
 
 // The three window nodes of one axis.  With lp <= h at most three nodes lie in
-// the support |Δ| < h + lp/2 and they are consecutive: base = ci - 1 when node
-// ci - 1 is in the support, else ci.  Nodes outside the grid get weight 0 and
-// raise the out-of-grid flag when they would have carried weight.
+// the support |Δ| < h + lp/2 and they are consecutive: node ci - 1 can only be
+// in it when the particle sits in the lower half of its cell (offset below
+// h/2, as lp/2 <= h/2), node ci + 2 only in the upper half.  The window is
+// ci - 1 .. ci + 1 for the lower half and ci .. ci + 2 for the upper one; the
+// node it adds beyond the support carries weight 0.  Splitting at the cell
+// centre (rather than at the support edge h - lp/2 from the node) keeps the
+// window of a particle on the regular lattice positions (h/4, 3h/4 for two per
+// cell) fixed under small motions, so particles of one sub-cell octant share
+// a window shape.  Nodes outside the grid get weight 0 and raise the
+// out-of-grid flag when they would have carried weight.
+// offset of a particle from node ci of its cell, in FP64 without contraction
+// (the cell sort classifies sub-cell octants with the same expression)
+template <typename R> __device__ __forceinline__ double cell_offset(double xp, int ci, const AxisC<R> &c) {
+    return __dsub_rn(xp, __dadd_rn(c.x1, __dmul_rn((double)ci, c.h)));
+}
+
 template <typename R> struct AxisW {
     int base;
     R N[3], dN[3];
@@ -120,8 +133,8 @@ template <typename R> struct AxisW {
 template <typename R>
 __device__ __forceinline__ bool axis_weights(double xp, int ci, const AxisC<R> &c, AxisW<R> &w) {
     // distances to nodes ci-1 .. ci+1 (or ci .. ci+2) from the offset to node ci
-    const double s = xp - (c.x1 + (double)ci * c.h);
-    const int lo = (fabs(s + c.h) < c.supp) ? 1 : 0;
+    const double s = cell_offset(xp, ci, c);
+    const int lo = s < 0.5 * c.h ? 1 : 0;
     const int base = ci - lo;
     bool oob = false;
 #pragma unroll

@@ -77,7 +77,12 @@ __global__ void k_na_keys(const double *x, const double *y, const double *z, int
     int cy = clampi(cell_cld_m1<float>(yp, ay), 0, sg.ncy - 1);
     int cz = D == 3 ? clampi(cell_fld<float>(zp, az), 0, sg.ncz - 1) : 0;
     uint32_t k = cell_key<D>(cx, cy, cz, sg);
-    keys[i] = k;
+    // sub-cell octant, the rank order inside a cell (mpm_sort.cuh)
+    uint32_t o = 0;
+    if (cell_offset<float>(xp, cx, ax) >= 0.5 * ax.h) o |= 1u;
+    if (cell_offset<float>(yp, cy, ay) >= 0.5 * ay.h) o |= 2u;
+    if (D == 3 && cell_offset<float>(zp, cz, az) >= 0.5 * az.h) o |= 4u;
+    keys[i] = k | (o << OCT_SHIFT);
     atomicAdd(&cnt[k], 1u);
     // p2c, 1-based, the reference's float formula (utils_OS.jl:247-249, 380-383)
     double qy = jl_cld(yp - ay.x1, ay.h), qx = jl_fld(xp - ax.x1, ax.h);
@@ -89,14 +94,14 @@ __global__ void k_na_keys(const double *x, const double *y, const double *z, int
 __global__ void k_na_scatter(int64_t np, const uint32_t *keys, const uint32_t *off, uint32_t *cur, uint2 *pairs) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
-    uint32_t k = keys[i];
+    const uint32_t kk = keys[i], k = kk & LOW29;
     uint32_t pos = off[k] + atomicAdd(&cur[k], 1u);
-    pairs[pos] = make_uint2((uint32_t)i, (uint32_t)i);
+    pairs[pos] = make_uint2((uint32_t)i | (kk & ~LOW29), (uint32_t)i);
 }
 
 __global__ void k_na_out(int64_t np, const uint2 *pairs2, int64_t *order_out) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < np) order_out[k] = (int64_t)pairs2[k].x;
+    if (k < np) order_out[k] = (int64_t)(pairs2[k].x & LOW29);
 }
 
 inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
@@ -128,17 +133,10 @@ int run(const mpm_desc *d, const double *x, const double *y, const double *z, in
     using T = Tile<D>;
     const int64_t np = d->np;
     SortGeom sg{};
-    sg.ncx = (int)(d->nnx - 1);
-    sg.ncy = (int)(d->nny - 1);
-    sg.ncz = D == 3 ? (int)(d->nnz - 1) : 1;
-    sg.ntx = (int)cdiv(sg.ncx, T::TX);
-    sg.nty = (int)cdiv(sg.ncy, T::TY);
-    sg.ntz = D == 3 ? (int)cdiv(sg.ncz, T::TZ) : 1;
-    const int64_t nk = (int64_t)sg.ntx * sg.nty * sg.ntz * T::CPT;
+    const int64_t nk = sort_geom(sg, D, d->nnx, d->nny, d->nnz, T::TX, T::TY, T::TZ);
     if (nk > NA_NK)
         return na_fail(MPM_E_ARG, "mpm_cell_order_noalloc: the grid needs " + std::to_string(nk) +
                                       " cell keys, more than MPM_NOALLOC_MAX_KEYS (" + std::to_string(NA_NK) + ")");
-    sg.nk = (uint32_t)nk;
     const uint32_t ntile = (uint32_t)(nk / T::CPT);
     uint32_t *keys = (uint32_t *)(S + OFF_KEYS), *cnt = (uint32_t *)(S + OFF_CNT), *off = (uint32_t *)(S + OFF_OFF);
     uint32_t *bsum = (uint32_t *)(S + OFF_BSUM), *tiles = (uint32_t *)(S + OFF_TILES), *big = (uint32_t *)(S + OFF_BIG);

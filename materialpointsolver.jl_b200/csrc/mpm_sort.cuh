@@ -2,37 +2,78 @@
 // which never reorders particles).
 //
 // Key: the particle's cell (the reference's p2c cell, Julia fld/cld rule)
-// renumbered tile-major: tiles of TX x TY x TZ cells, key = tile * CPT +
-// cell-in-tile.  Order: ascending tile; inside a tile ascending rank of the
-// particle within its cell (rank = position by original index), then
-// ascending cell-in-tile -- a CPU stable sort by (tile, rank, cell-in-tile).
+// renumbered tile-major: tiles of tx x ty x tz cells (a run-time shape, 32
+// cells by default so that one warp lane stands for one cell), key = tile *
+// cpt + cell-in-tile.  Order: ascending tile; inside a tile ascending rank of
+// the particle within its cell, then ascending cell-in-tile -- a CPU stable
+// sort by (tile, rank, cell-in-tile).  The rank orders a cell's particles by
+// their sub-cell octant (which half of the cell they sit in along each axis:
+// bit 0 x, bit 1 y, bit 2 z), then by original index; on a regular lattice
+// with two particles per cell and axis, rank r then holds the particles of
+// one octant in every cell, whose uGIMP windows have the same shape.
 //
 // Counting sort: count per key, exclusive scan, scatter (atomic slot within
-// the bucket), then each bucket is ordered by original index (buckets hold the
-// few particles of one cell), then every particle array is gathered through
-// the permutation.
+// the bucket), then each bucket is ordered by (octant, original index) (buckets
+// hold the few particles of one cell), then every particle array is gathered
+// through the permutation.
 #pragma once
 #include "mpm_kernels.cuh"
 
 namespace mpm {
 
+// default tile shapes (cells): one warp lane per cell
 template <int D> struct Tile {
-    static constexpr int TX = D == 3 ? 4 : 8, TY = 8, TZ = D == 3 ? 4 : 1;
+    static constexpr int TX = D == 3 ? 2 : 4, TY = 8, TZ = D == 3 ? 2 : 1;
     static constexpr int CPT = TX * TY * TZ;
 };
 
 struct SortGeom {
     int ncx, ncy, ncz;      // cells per axis
     int ntx, nty, ntz;      // tiles per axis
-    uint32_t nk;            // number of keys = tiles * CPT
+    int tx, ty, tz, cpt;    // tile shape (cells) and cells per tile
+    uint32_t nk;            // number of keys = tiles * cpt
 };
 
+inline int64_t sort_cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// sort geometry of a grid of nnx x nny (x nnz) nodes in tiles of tx x ty (x tz)
+// cells; returns the number of keys (tiles x cells per tile)
+inline int64_t sort_geom(SortGeom &sg, int dim, int64_t nnx, int64_t nny, int64_t nnz, int tx, int ty, int tz) {
+    sg.ncx = (int)(nnx - 1);
+    sg.ncy = (int)(nny - 1);
+    sg.ncz = dim == 3 ? (int)(nnz - 1) : 1;
+    sg.tx = tx;
+    sg.ty = ty;
+    sg.tz = dim == 3 ? tz : 1;
+    sg.cpt = sg.tx * sg.ty * sg.tz;
+    sg.ntx = (int)sort_cdiv(sg.ncx, sg.tx);
+    sg.nty = (int)sort_cdiv(sg.ncy, sg.ty);
+    sg.ntz = dim == 3 ? (int)sort_cdiv(sg.ncz, sg.tz) : 1;
+    const int64_t nk = (int64_t)sg.ntx * sg.nty * sg.ntz * sg.cpt;
+    sg.nk = (uint32_t)nk;
+    return nk;
+}
+
+// sort keys and original indices carry the octant in their top bits
+constexpr int OCT_SHIFT = 29;
+constexpr uint32_t LOW29 = (1u << OCT_SHIFT) - 1u;
+
 template <int D> __device__ __forceinline__ uint32_t cell_key(int cx, int cy, int cz, const SortGeom &s) {
-    using T = Tile<D>;
-    int tx = cx / T::TX, ty = cy / T::TY, tz = D == 3 ? cz / T::TZ : 0;
-    int lx = cx - tx * T::TX, ly = cy - ty * T::TY, lz = D == 3 ? cz - tz * T::TZ : 0;
+    int tx = cx / s.tx, ty = cy / s.ty, tz = D == 3 ? cz / s.tz : 0;
+    int lx = cx - tx * s.tx, ly = cy - ty * s.ty, lz = D == 3 ? cz - tz * s.tz : 0;
     uint32_t t = (uint32_t)((tz * s.ntx + tx) * s.nty + ty);
-    return t * T::CPT + (uint32_t)((lz * T::TX + lx) * T::TY + ly);
+    return t * (uint32_t)s.cpt + (uint32_t)((lz * s.tx + lx) * s.ty + ly);
+}
+
+// sub-cell octant of a particle in cell (cx, cy, cz): bit a set when its offset
+// from the cell's first node is at least half a cell along axis a
+template <int D, typename R>
+__device__ __forceinline__ uint32_t cell_octant(const double *x, int cx, int cy, int cz, const GDev<R> &g) {
+    uint32_t o = 0;
+    if (cell_offset<R>(x[0], cx, g.ax[0]) >= 0.5 * g.ax[0].h) o |= 1u;
+    if (cell_offset<R>(x[1], cy, g.ax[1]) >= 0.5 * g.ax[1].h) o |= 2u;
+    if (D == 3 && cell_offset<R>(x[2], cz, g.ax[2]) >= 0.5 * g.ax[2].h) o |= 4u;
+    return o;
 }
 
 template <int D, typename R>
@@ -47,7 +88,7 @@ __global__ void k_sort_keys(PDev<D, R> P, GDev<R> g, SortGeom sg, int64_t np, ui
     int cx = clampi(ci[0], 0, sg.ncx - 1), cy = clampi(ci[1], 0, sg.ncy - 1);
     int cz = D == 3 ? clampi(ci[2], 0, sg.ncz - 1) : 0;
     uint32_t k = cell_key<D>(cx, cy, cz, sg);
-    keys[i] = k;
+    keys[i] = k | (cell_octant<D, R>(x, cx, cy, cz, g) << OCT_SHIFT);
     atomicAdd(&cnt[k], 1u);
 }
 
@@ -135,12 +176,13 @@ __global__ void k_sort_scatter(PDev<D, R> P, int64_t np, const uint32_t *keys, c
                                uint32_t *cur, uint2 *pairs) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
-    uint32_t k = keys[i];
+    const uint32_t kk = keys[i], k = kk & LOW29;
     uint32_t pos = off[k] + atomicAdd(&cur[k], 1u);
-    pairs[pos] = make_uint2(P.orig[i], (uint32_t)i);
+    pairs[pos] = make_uint2(P.orig[i] | (kk & ~LOW29), (uint32_t)i);
 }
 
-// order each bucket by original index; buckets above SMALL are queued for the CTA sort
+// order each bucket by (octant, original index) (the pair's first word);
+// buckets above SMALL are queued for the CTA sort
 constexpr int BUCKET_SMALL = 32;
 constexpr int BUCKET_MAX = 4096;
 
@@ -274,7 +316,7 @@ __global__ void k_permute(PDev<D, R> src, PDev<D, R> dst, const uint2 *pairs, in
 #pragma unroll
         for (int c = 0; c < NV; ++c) dst.epsw[c][k] = src.epsw[c][o];
     }
-    dst.orig[k] = pr.x;
+    dst.orig[k] = pr.x & LOW29;
 }
 
 }  // namespace mpm

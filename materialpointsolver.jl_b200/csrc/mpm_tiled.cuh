@@ -43,14 +43,15 @@ template <int D> struct TileGeo {
     int w0[3];   // first node of the window
 };
 
+// (the window is sized for the default tile shape; with a larger run-time
+// shape the particles beyond it take the global path)
 template <int D> __device__ __forceinline__ TileGeo<D> tile_geo(uint32_t t, const SortGeom &sg) {
-    using T = Tile<D>;
     TileGeo<D> g;
     int ty = (int)(t % (uint32_t)sg.nty);
     uint32_t r = t / (uint32_t)sg.nty;
     int tx = (int)(r % (uint32_t)sg.ntx);
     int tz = (int)(r / (uint32_t)sg.ntx);
-    g.c0[0] = tx * T::TX; g.c0[1] = ty * T::TY; g.c0[2] = D == 3 ? tz * T::TZ : 0;
+    g.c0[0] = tx * sg.tx; g.c0[1] = ty * sg.ty; g.c0[2] = D == 3 ? tz * sg.tz : 0;
     for (int a = 0; a < 3; ++a) g.w0[a] = g.c0[a] - MARGIN - 1;
     if (D == 2) g.w0[2] = 0;
     return g;
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_dmap_tile(PDev<D, R> P, GDe
     for (uint32_t q = blockIdx.x; q < nt; q += gridDim.x) {
         const uint32_t t = tl.tiles[q];
         const TileGeo<D> tg = tile_geo<D>(t, tl.sg);
-        const uint32_t p0 = tl.off[t * Tile<D>::CPT], p1 = tl.off[(t + 1) * Tile<D>::CPT];
+        const uint32_t p0 = tl.off[t * (uint32_t)tl.sg.cpt], p1 = tl.off[(t + 1) * (uint32_t)tl.sg.cpt];
         for (int n = threadIdx.x; n < W::WN; n += blockDim.x) {
             int gn = window_global<D, R>(g, tg, n);
             Node8<R> r;
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p_tile(PDev<D, R> P, GDev
     for (uint32_t q = blockIdx.x; q < nt; q += gridDim.x) {
         const uint32_t t = tl.tiles[q];
         const TileGeo<D> tg = tile_geo<D>(t, tl.sg);
-        const uint32_t p0 = tl.off[t * Tile<D>::CPT], p1 = tl.off[(t + 1) * Tile<D>::CPT];
+        const uint32_t p0 = tl.off[t * (uint32_t)tl.sg.cpt], p1 = tl.off[(t + 1) * (uint32_t)tl.sg.cpt];
         for (int n = threadIdx.x; n < W::WN; n += blockDim.x) {
             int gn = window_global<D, R>(g, tg, n);
             Node8<R> r;

@@ -9,7 +9,7 @@ configuration's horizon:
            in FP64 and in the mixed mode against the CPU oracle over the whole
            run, beside the oracle's own sensitivity to its summation order
            (sequential against OpenMP atomics).
-  config2  3D column, 2 560 000 particles, 1 s (22 500 steps): both device
+  config2  3D column, 2 560 000 particles, 1 s (22 539 steps): both device
            modes against the oracle over a 20-step prefix, then the mixed mode
            against the all-FP64 device mode over the whole second (the oracle
            would need hours), beside the run-to-run spread of each mode (the
@@ -85,8 +85,10 @@ def run_device(pkg, case, nsteps, chunk=2000, surrogate=None, log=None):
             Ti = dev.step(case.dt, Ti, n)
         done += n
     secs = time.perf_counter() - t0
-    out = pkg.types.Particle3D(dx=case.mp.dx, dy=case.mp.dy, dz=case.mp.dz, xi=case.mp.xi, rho=case.mp.rho) \
-        if case.grid.dim == 3 else pkg.types.Particle2D(dx=case.mp.dx, dy=case.mp.dy, xi=case.mp.xi, rho=case.mp.rho)
+    if case.grid.dim == 3:
+        out = pkg.types.Particle3D(dx=case.mp.dx, dy=case.mp.dy, dz=case.mp.dz, xi=case.mp.xi, rho=case.mp.rho)
+    else:
+        out = pkg.types.Particle2D(dx=case.mp.dx, dy=case.mp.dy, xi=case.mp.xi, rho=case.mp.rho)
     dev.download(pkg._lib.F_REFERENCE, out)
     st = dev.stats()
     dev.close()

@@ -24,18 +24,20 @@ def tol_stress(tol):
     return TOL32_STRESS if tol == TOL32 else tol
 
 
-def run_both(pkg, orc, case, nsteps, tiled=False):
+def run_both(pkg, orc, case, nsteps, tiled=False, box=True):
     import os
     lib = pkg._lib
-    old = os.environ.get("MPM_B200_TILED")
-    os.environ["MPM_B200_TILED"] = "1" if tiled else "0"
+    env = {"MPM_B200_TILED": "1" if tiled else "0", "MPM_B200_BOX": "1" if box else "0"}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
     finally:
-        if old is None:
-            del os.environ["MPM_B200_TILED"]
-        else:
-            os.environ["MPM_B200_TILED"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
     dev.step(case.dt, 0.0, nsteps)
     out = fresh_particles(pkg, case.mp)
     dev.download(lib.F_REFERENCE | lib.F_F, out)
@@ -166,10 +168,25 @@ def test_tiled_path(pkg, orc, gpu_lib, dim, prec, tol):
     check_fields(out, o, case.mp, tol, tol_stress(tol))
 
 
+@pytest.mark.parametrize("box", [False, True])
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("model", ["linearelastic", "druckerprager"])
+def test_box_and_chain_passes(pkg, orc, gpu_lib, dim, model, box):
+    """The mixed-mode step through the shared-memory box passes (one warp per
+    tile) and through the per-particle lane-merged passes, each against the
+    oracle."""
+    mk = small2d if dim == 2 else small3d
+    case = mk(pkg, constitutive=model, gpu_precision="mixed", sort_every=8)
+    out, o = run_both(pkg, orc, case, 24, box=box)
+    check_fields(out, o, case.mp, TOL32, TOL32_STRESS)
+
+
+@pytest.mark.parametrize("tiled", [False, True])
 @pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("mixed", 1e-3)])
-def test_drift_beyond_tile_margin(pkg, orc, gpu_lib, prec, tol):
+def test_drift_beyond_tile_margin(pkg, orc, gpu_lib, prec, tol, tiled):
     """No re-sort for 120 steps while the column translates by > 2 cells: the
-    particles leaving their tile's window take the global path.  Mixed mode is
+    particles leaving their tile's window (tiled passes) or their tile's node
+    box (box passes, the mixed-mode default) take the global path.  Mixed mode is
     checked on the kinematics only: the elastic velocities (~1e-3 m/s) ride on
     a 3 m/s translation, and FP32 nodal velocities resolve them to ~1e-3, so
     the stresses they integrate differ from FP64 by up to ~10 % -- the same
@@ -178,7 +195,7 @@ def test_drift_beyond_tile_margin(pkg, orc, gpu_lib, prec, tol):
                    domain=(0.4, 0.12, 0.16))
     case.mp.xi[:, 0] += 0.05          # away from the fixed wall
     case.mp.vs[:, 0] = 3.0
-    out, o = run_both(pkg, orc, case, 120, tiled=True)
+    out, o = run_both(pkg, orc, case, 120, tiled=tiled)
     moved = np.abs(o.xi[:, 0] - case.mp.xi[:, 0]).max() / case.grid.dx
     assert moved > 2.0
     if prec == "fp64":
@@ -344,22 +361,40 @@ def test_p2c_bit_exact(pkg, orc, gpu_lib, dim):
     assert np.array_equal(p_gpu, p_ref)
 
 
-def host_key(p2c, g, dim):
-    """Tile-major cell key (tiles of 4x8x4 cells in 3D, 8x8 in 2D) from the 1-based p2c."""
+TILE = {3: (2, 8, 2), 2: (4, 8, 1)}   # the library's default sort tiles (32 cells)
+
+
+def host_cells(p2c, g, dim):
     q = p2c - 1
     cy = q % g.ncy
     cx = (q // g.ncy) % g.ncx
-    TX, TY, TZ = (4, 8, 4) if dim == 3 else (8, 8, 1)
+    cz = q // (g.ncy * g.ncx) if dim == 3 else np.zeros_like(q)
+    return cx, cy, cz
+
+
+def host_key(p2c, g, dim):
+    """Tile-major cell key (the default tiles) from the 1-based p2c."""
+    cx, cy, cz = host_cells(p2c, g, dim)
+    TX, TY, TZ = TILE[dim]
     ntx = -(-g.ncx // TX)
     nty = -(-g.ncy // TY)
-    if dim == 3:
-        cz = q // (g.ncy * g.ncx)
-    else:
-        cz = np.zeros_like(q)
     tx, ty, tz = cx // TX, cy // TY, cz // TZ
     lx, ly, lz = cx - tx * TX, cy - ty * TY, cz - tz * TZ
     t = (tz * ntx + tx) * nty + ty
     return t * (TX * TY * TZ) + (lz * TX + lx) * TY + ly
+
+
+def host_octant(xi, p2c, g, dim):
+    """Sub-cell octant: bit a set when the offset from the cell's first node is
+    at least half a cell (the same FP64 operations as the device)."""
+    cells = host_cells(p2c, g, dim)
+    x1 = (g.x1, g.y1, g.z1 if dim == 3 else 0.0)
+    h = (g.dx, g.dy, g.dz if dim == 3 else 1.0)
+    o = np.zeros(len(p2c), np.int64)
+    for a in range(dim):
+        s = xi[:, a] - (x1[a] + cells[a].astype(np.float64) * h[a])
+        o |= (s >= 0.5 * h[a]).astype(np.int64) << a
+    return o
 
 
 @pytest.mark.parametrize("dim", [2, 3])
@@ -375,10 +410,12 @@ def test_sort_bit_exact(pkg, orc, gpu_lib, dim):
     order = dev.order()
     dev.close()
     o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc)
-    key = host_key(o.p2c(case.mp.xi), case.grid, dim)
-    cpt = 128 if dim == 3 else 64
-    # rank of each particle within its cell, by original index
-    by_cell = np.lexsort((np.arange(case.mp.np), key))
+    p2c = o.p2c(case.mp.xi)
+    key = host_key(p2c, case.grid, dim)
+    octant = host_octant(case.mp.xi, p2c, case.grid, dim)
+    cpt = 32
+    # rank of each particle within its cell, by (octant, original index)
+    by_cell = np.lexsort((np.arange(case.mp.np), octant, key))
     rank = np.empty(case.mp.np, np.int64)
     ks = key[by_cell]
     start = np.r_[0, np.flatnonzero(np.diff(ks)) + 1]
