@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="column3d: skip the batched (batch2d) and learned (slope3d surrogate) forms")
     ap.add_argument("--mc3d", default="literal", choices=["literal", "restated"])
     ap.add_argument("--workload", default="column3d",
                     choices=["column3d", "slope3d", "batch2d", "column2d", "saturated3d", "example3d", "example2d"],
@@ -69,34 +71,87 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """SM clocks and clock-event (throttle) reasons sampled through NVML
+    (read-only queries) every 5 ms while the timed region runs, plus one
+    sample right before and one right after it, so that even a region of a
+    few milliseconds has a record.  Falls back to nvidia-smi polling when
+    NVML is not available."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []          # (sm_mhz, max_mhz, set of reasons)
         self.proc = None
+        self.nv = None
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml as nv
+        nv.nvmlInit()
+        self.nv = nv
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _sample(self):
+        nv = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        masks = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        self.rows.append((float(sm), float(mx), {n for n, m in zip(self.NAMES, masks) if bits & m}))
+
+    def _poll(self):
+        while not self.stop.wait(0.005):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.h = self._nvml_handle()
+            self._sample()
+            self.t = threading.Thread(target=self._poll, daemon=True)
             self.t.start()
-        except OSError:
-            self.proc = None
+        except Exception:
+            self.nv = None
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                     "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.t = threading.Thread(target=self._read, daemon=True)
+                self.t.start()
+            except OSError:
+                self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            try:
+                reasons = {n for k, n in enumerate(self.NAMES) if len(r) > 5 + k and r[5 + k].lower() == "active"}
+                self.rows.append((float(r[1]), float(r[2]), reasons))
+            except ValueError:
+                pass
 
     def __exit__(self, *a):
-        if self.proc:
+        if self.nv is not None:
+            self.stop.set()
+            self.t.join(timeout=2)
+            try:
+                self._sample()
+            except Exception:
+                pass
+        elif self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -107,17 +162,13 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
         for r in self.rows:
-            for k, n in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+            reasons |= r[2]
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows),
+                "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted(reasons), "samples": len(self.rows),
+                "source": "nvml" if self.nv is not None else "nvidia-smi"}
 
 
 def max_over_ranks(x, device):
@@ -329,29 +380,38 @@ def run_b200(args):
     Ti = dev.step(dt, Ti, W)
     if use_dist:
         dist.barrier()
-    launches0 = dev.stats().launches
+    st0 = dev.stats()
+    launches0, sorts0 = st0.launches, st0.sorts_done
     with ClockSampler(local) as clk:
         dev.step_async(dt, Ti, K)
         dev.sync()
     st = dev.stats()
-    ms = st.last_step_ms
+    ms_window = st.last_step_ms
     launches = st.launches - launches0
+    sorts_window = st.sorts_done - sorts0
     na = st.active_nodes
     Ti = advance_time(Ti, dt, K, dev.desc.time_f32)
-    t_max = max_over_ranks(ms, f"cuda:{local}") if use_dist else ms
-    value = replica_value(world, npart, K, t_max)
-
     sort_used, tiled_used = dev.tuning()
     if surr_info is not None:
         st_s = dev.stats()
         surr_info["rows"] = int(st_s.surr_rows)
         surr_info["accepted_fraction"] = 1.0 - st_s.surr_fallbacks / max(st_s.surr_rows, 1)
 
-    # ---- per-kernel device times (events on the library stream) ----
+    # ---- per-kernel device times (events on the library stream), and the
+    # cell re-sort, which runs every sort_used steps: the K-step window holds
+    # whole sorts or none, so the reported time replaces the sorts it holds by
+    # the amortised share sort_ms * K / sort_used ----
     dev.set_profiling(True)
     dev.step(dt, Ti, 16)
+    for _ in range(3):
+        dev.sort()
     kt = dev.kernel_times()
     dev.set_profiling(False)
+    sort_ms = kt.get("sort", (0.0, 0))[0]
+    ms = ms_window - sorts_window * sort_ms + sort_ms * K / sort_used
+    t_max = max_over_ranks(ms, f"cuda:{local}") if use_dist else ms
+    value = replica_value(world, npart, K, t_max)
+
     dev.close()
     dom = "g2p_p2g"
     dom_ms = kt.get(dom, (float("nan"), 0))[0]
@@ -401,6 +461,9 @@ def run_b200(args):
                        **({"slopes": len(case.meta["slopes"]), "tuning": tuning} if tuning else {}),
                        **({"surrogate": surr_info} if surr_info else {})),
         "gpu_launches": launches,
+        "timed_window": {"ms_per_step": ms_window / K, "sorts": sorts_window, "sort_ms": sort_ms,
+                         "sort_every": sort_used,
+                         "note": "value and ms_per_step count the re-sort as sort_ms / sort_every per step"},
         "kernel_ms": {k: v[0] for k, v in kt.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
@@ -418,6 +481,8 @@ def run_b200(args):
         result["fp64_device"] = fp64_device_rate(pkg, builder, published, local, K, W)
     if args.snapshot_every > 0:
         result["snapshots"] = snapshot_cost(pkg, case, dt, K, args.snapshot_every, local)
+    if args.workload == "column3d" and not args.no_extra:
+        result["forms"] = extra_forms(pkg, local, K, W)
     if rank == 0 and not args.no_cpu_baseline:
         if args.workload in ("column3d", "column2d"):
             result["cpu_baseline"] = cpu_baseline(args.mc3d, args.workload)
@@ -426,6 +491,104 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result))
+
+
+def _timed_steps(dev, dt, Ti, K):
+    """K steps timed on the device (CUDA events inside the library); returns
+    (ms for the K steps, end time)."""
+    dev.step_async(dt, Ti, K)
+    dev.sync()
+    ms = dev.stats().last_step_ms
+    return ms, advance_time(Ti, dt, K, dev.desc.time_f32)
+
+
+def extra_forms(pkg, local, K, W):
+    """The batched and learned forms of the metric, beside the plain column:
+    batch2d -- 256 independent 2D slopes in one grid (15.5 M particles),
+    autotuned during untimed steps, K timed steps, and the run-out of two of
+    its slopes against the same slopes stepped alone; slope3d -- the 8.0 M-
+    particle 3D slope (lognormal cohesion field, Drucker-Prager) stepped
+    plainly and with the trained stress-return surrogate from the same state
+    (samples logged from 60 plain steps, 6 epochs of training on the device),
+    with the surrogate's accepted fraction and its run-out / displacement
+    error against the plain step after the same K steps."""
+    out = {}
+    # ---- batch2d ----
+    case = pkg.workloads.slope_batch_2d(Te=0.0)
+    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
+    try:
+        Ti, S, tiled, trial_ms = dev.autotune(case.dt, 0.0, 16)
+        n_pre = 8 * 16
+        Ti = dev.step(case.dt, Ti, W)
+        ms, Ti = _timed_steps(dev, case.dt, Ti, K)
+        xb = pkg.types.Particle2D(dx=case.mp.dx, dy=case.mp.dy, xi=case.mp.xi, rho=case.mp.rho)
+        dev.download(pkg._lib.F_XI, xb)
+    finally:
+        dev.close()
+    n_total = n_pre + W + K
+    ro_b = pkg.workloads.slope_runouts(case, xb.xi)
+    errs = []
+    for k in (0, len(case.meta["slopes"]) // 2):
+        single = pkg.workloads.slope_2d_single(case, k)
+        d1 = pkg.DeviceModel(single.args, single.grid, single.mp, single.attr, single.bc, device=local)
+        try:
+            d1.step(single.dt, 0.0, n_total)
+            x1 = pkg.types.Particle2D(dx=single.mp.dx, dy=single.mp.dy, xi=single.mp.xi, rho=single.mp.rho)
+            d1.download(pkg._lib.F_XI, x1)
+        finally:
+            d1.close()
+        ro_1 = pkg.workloads.slope_runouts(single, x1.xi)[0]
+        errs.append(abs(ro_b[k] - ro_1) / max(abs(ro_1), case.meta["h"]))
+    out["batch2d"] = {"workload": "256 independent 2D slopes in one grid (Drucker-Prager, FP32)",
+                      "particles": int(case.mp.np), "ms_per_step": ms / K,
+                      "particle_updates_per_s": case.mp.np * K / (ms * 1e-3),
+                      "tuning": {"sort_every": S, "tiled": tiled, "trial_ms_per_step": trial_ms},
+                      "runout_err_vs_alone": {"slopes": 2, "steps": n_total, "max": max(errs)}}
+    del case
+    # ---- slope3d, plain and surrogate from the same state ----
+    S_ = pkg.surrogate
+    runs = {}
+    for mode in ("plain", "surrogate"):
+        case = pkg.workloads.slope_3d(Te=0.0)
+        dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
+        try:
+            info = {}
+            if mode == "surrogate":
+                t0 = time.perf_counter()
+                feat, tgt, Ti = S_.collect_samples(dev, case.dt, 0.0, 60, 6_000_000, every=8, device=local)
+                sur = S_.Surrogate(seed=1, device=local)
+                sur.set_norm(feat, tgt)
+                losses = sur.train(feat, tgt, epochs=6, batch=16384, lr=3e-3, lr_end=1e-4)
+                dev.set_surrogate(sur, tol=1e-3, sref=1e3)
+                info = {"train_samples": int(feat.shape[0]), "epochs": 6,
+                        "loss_first_last": [losses[0], losses[-1]], "setup_s": time.perf_counter() - t0}
+                del feat, tgt
+            else:
+                Ti = dev.step(case.dt, 0.0, 60)
+            Ti = dev.step(case.dt, Ti, W)
+            ms, Ti = _timed_steps(dev, case.dt, Ti, K)
+            st = dev.stats()
+            x = pkg.types.Particle3D(dx=case.mp.dx, dy=case.mp.dy, dz=case.mp.dz, xi=case.mp.xi, rho=case.mp.rho)
+            dev.download(pkg._lib.F_XI, x)
+            if mode == "surrogate":
+                info.update(rows=int(st.surr_rows),
+                            accepted_fraction=1.0 - st.surr_fallbacks / max(st.surr_rows, 1))
+            runs[mode] = (ms, x.xi.copy(), info, case.mp.xi.copy(), case.mp.np, case.meta["h"])
+        finally:
+            dev.close()
+        del case
+    ms_p, x_p, _, x0, npart, h = runs["plain"]
+    ms_s, x_s, info, _, _, _ = runs["surrogate"]
+    ro = lambda x: float(x[:, 0].max() - x0[:, 0].max())
+    du_p, du_s = x_p - x0, x_s - x0
+    info.update(ms_per_step=ms_s / K, particle_updates_per_s=npart * K / (ms_s * 1e-3),
+                runout_err_vs_plain=abs(ro(x_s) - ro(x_p)) / max(abs(ro(x_p)), h),
+                disp_rel_vs_plain=float(np.linalg.norm(du_s - du_p) / max(np.linalg.norm(du_p), 1e-300)))
+    out["slope3d"] = {"workload": "3D slope, lognormal cohesion field, Drucker-Prager (plastic from the start)",
+                      "particles": int(npart), "steps_compared": 60 + W + K,
+                      "plain": {"ms_per_step": ms_p / K, "particle_updates_per_s": npart * K / (ms_p * 1e-3)},
+                      "surrogate": info}
+    return out
 
 
 def snapshot_cost(pkg, case, dt, K, every, local):

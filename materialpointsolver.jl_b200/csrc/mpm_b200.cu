@@ -448,10 +448,38 @@ template <typename R> void build_materials(mpm_handle *h, const mpm_host_views *
     CK(cudaMemcpyAsync(h->mat, M.data(), nm * sizeof(Mat<R>), cudaMemcpyHostToDevice, h->stream));
 }
 
+// ---- profiling mode: device time of a span of the library stream, by name ---------
+void prof_begin(mpm_handle *h) {
+    if (h->kev.size() < 2) {
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        h->kev.push_back(a);
+        h->kev.push_back(b);
+    }
+    CK(cudaEventRecord(h->kev[0], h->stream));
+}
+void prof_end(mpm_handle *h, const char *name) {
+    KTimer *kt = nullptr;
+    for (KTimer &k : h->ktimes)
+        if (std::strcmp(k.name, name) == 0) { kt = &k; break; }
+    if (!kt) {
+        h->ktimes.push_back(KTimer{name});
+        kt = &h->ktimes.back();
+    }
+    CK(cudaEventRecord(h->kev[1], h->stream));
+    CK(cudaEventSynchronize(h->kev[1]));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]));
+    kt->ms += ms;
+    kt->n += 1;
+}
+
 // ---- the sort ----------------------------------------------------------------------
 template <int D, typename R> void do_sort(mpm_handle *h) {
     const int64_t np = h->d.np;
     if (np == 0) return;
+    if (h->profiling) prof_begin(h);
     cudaStream_t st = h->stream;
     PDev<D, R> A = pdev_from<D, R>(h, 0), B = pdev_from<D, R>(h, 1);
     GDev<R> g = gdev_from<R>(h);
@@ -488,6 +516,7 @@ template <int D, typename R> void do_sort(mpm_handle *h) {
     h->since_sort = 0;
     h->sorts_done++;
     h->launches += 10;
+    if (h->profiling) prof_end(h, "sort");
 }
 
 // ---- step --------------------------------------------------------------------------
@@ -499,29 +528,10 @@ struct Launcher {
     mpm_handle *h;
     template <typename F> void run(const char *name, F &&f) {
         if (h->profiling) {
-            KTimer *kt = nullptr;
-            for (KTimer &k : h->ktimes)
-                if (std::strcmp(k.name, name) == 0) { kt = &k; break; }
-            if (!kt) {
-                h->ktimes.push_back(KTimer{name});
-                kt = &h->ktimes.back();
-            }
-            if (h->kev.size() < 2) {
-                cudaEvent_t a, b;
-                CK(cudaEventCreate(&a));
-                CK(cudaEventCreate(&b));
-                h->kev.push_back(a);
-                h->kev.push_back(b);
-            }
-            CK(cudaEventRecord(h->kev[0], h->stream));
+            prof_begin(h);
             f();
             LAUNCH_CHECK();
-            CK(cudaEventRecord(h->kev[1], h->stream));
-            CK(cudaEventSynchronize(h->kev[1]));
-            float ms = 0;
-            CK(cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]));
-            kt->ms += ms;
-            kt->n += 1;
+            prof_end(h, name);
         } else {
             f();
             LAUNCH_CHECK();

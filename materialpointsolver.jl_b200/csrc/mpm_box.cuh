@@ -26,7 +26,12 @@
 // sort, particles of one octant, whose windows start at distinct nodes; a
 // particle that has since crossed a cell centre can meet another lane's
 // window.  Such lanes are detected per rank (__match_any_sync on the window
-// corner) and scatter in successive rounds.  A particle whose window reaches
+// corner) and scatter in successive rounds.  Windows of neighbouring lanes do
+// overlap (lane L's row 1 is lane L+1's row 0), so one node is updated by
+// different lanes at different window offsets: every node update is followed
+// by __syncwarp over the scattering lanes, which orders it before the next
+// offset's loads of the other lanes (without it the compiler may hoist those
+// loads above the stores).  A particle whose window reaches
 // outside the box (it drifted more than half a cell out of its tile since the
 // sort) gathers from and reduces into the global node records directly, like
 // the per-particle kernels.
@@ -239,7 +244,8 @@ __device__ __forceinline__ void gather_global(const GDev<float> &g, const AxisW<
 // Y_k = σv_ky·Nx·Nz (the separable form of p2g_scatter).
 template <typename G, int D>
 __device__ __forceinline__ void scatter_box(float4 *sa, float4 *sb, const AxisW<float> *w, const int *lb, float m,
-                                            float vol, const float *v, const float *s, float grav) {
+                                            float vol, const float *v, const float *s, float grav,
+                                            unsigned lanes) {
     constexpr int NC = D == 3 ? 3 : 1;
     const float p[3] = {m * v[0], m * v[1], D == 3 ? m * v[2] : 0.0f};
     float sv[6];
@@ -284,6 +290,7 @@ __device__ __forceinline__ void scatter_box(float4 *sa, float4 *sb, const AxisW<
                 const float2 b01 = __ffma2_rn(g2, Y01, __ffma2_rn(w2, U45, make_float2(B.x, B.y)));
                 const float b2 = fmaf(gy, Y[2], fmaf(wy, U[6], B.z));
                 sb[col + b] = make_float4(b01.x, b01.y, b2, 0.0f);
+                __syncwarp(lanes);
             }
         }
     }
@@ -368,7 +375,9 @@ __global__ void __launch_bounds__(MPM_BOX_WARPS * 32, MPM_BOX_G2P_MINB)
             const int grank = __popc(same & lt);
             const int rounds = __reduce_max_sync(FULL, (live && inside) ? grank : 0);
             for (int rr = 0; rr <= rounds; ++rr) {
-                if (live && inside && grank == rr) scatter_box<G, D>(sa, sb, w, lb, m, vol, v, s, grav);
+                const bool mine = live && inside && grank == rr;
+                const unsigned lanes = __ballot_sync(FULL, mine);
+                if (mine) scatter_box<G, D>(sa, sb, w, lb, m, vol, v, s, grav, lanes);
                 __syncwarp();
             }
             if (live && !inside) p2g_scatter<D, float>(g, w, m, vol, v, s, grav);
@@ -499,7 +508,9 @@ __global__ void __launch_bounds__(MPM_BOX_WARPS * 32, MPM_BOX_DMAP_MINB)
             const int grank = __popc(same & lt);
             const int rounds = __reduce_max_sync(FULL, (act && inside) ? grank : 0);
             for (int rr = 0; rr <= rounds; ++rr) {
-                if (act && inside && grank == rr) {
+                const bool mine = act && inside && grank == rr;
+                const unsigned lanes = __ballot_sync(FULL, mine);
+                if (mine) {
 #pragma unroll
                     for (int c = 0; c < NC; ++c) {
                         const float wz = D == 3 ? w[2].N[c] : 1.0f;
@@ -515,6 +526,7 @@ __global__ void __launch_bounds__(MPM_BOX_WARPS * 32, MPM_BOX_DMAP_MINB)
                                 const float4 A = sp4[col + b];
                                 const float2 a01 = __ffma2_rn(make_float2(wy, wy), P01, make_float2(A.x, A.y));
                                 sp4[col + b] = make_float4(a01.x, a01.y, fmaf(wy, P2, A.z), 0.f);
+                                __syncwarp(lanes);
                             }
                         }
                     }
