@@ -358,8 +358,8 @@ def run_b200(args):
     if args.workload == "batch2d":
         # untimed: the autotuner's trials are real steps of the model
         Ti, S, tiled, trial_ms = dev.autotune(dt, Ti, 16)
-        tuning = {"sort_every": S, "tiled": tiled, "trial_ms_per_step": trial_ms,
-                  "candidates": "sort period 4/8/16/32 x per-particle/tiled passes, 16 steps each"}
+        tuning = {"sort_every": S, "tiled": tiled, "tile": dev.tile(), "trial_ms_per_step": trial_ms,
+                  "candidates": "tile shapes x sort periods 8/16/32/64 (box passes), tiled passes at 16/32; max(16, period) steps each"}
     surr_info = None
     if args.surrogate:
         if args.workload != "slope3d":
@@ -518,7 +518,8 @@ def extra_forms(pkg, local, K, W):
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
     try:
         Ti, S, tiled, trial_ms = dev.autotune(case.dt, 0.0, 16)
-        n_pre = 8 * 16
+        n_pre = dev.stats().steps_done
+        tile = dev.tile()
         Ti = dev.step(case.dt, Ti, W)
         ms, Ti = _timed_steps(dev, case.dt, Ti, K)
         xb = pkg.types.Particle2D(dx=case.mp.dx, dy=case.mp.dy, xi=case.mp.xi, rho=case.mp.rho)
@@ -542,7 +543,7 @@ def extra_forms(pkg, local, K, W):
     out["batch2d"] = {"workload": "256 independent 2D slopes in one grid (Drucker-Prager, FP32)",
                       "particles": int(case.mp.np), "ms_per_step": ms / K,
                       "particle_updates_per_s": case.mp.np * K / (ms * 1e-3),
-                      "tuning": {"sort_every": S, "tiled": tiled, "trial_ms_per_step": trial_ms},
+                      "tuning": {"sort_every": S, "tiled": tiled, "tile": tile, "trial_ms_per_step": trial_ms},
                       "runout_err_vs_alone": {"slopes": 2, "steps": n_total, "max": max(errs)}}
     del case
     # ---- slope3d, plain and surrogate from the same state ----

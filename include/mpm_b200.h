@@ -210,16 +210,23 @@ int mpm_step_async(mpm_handle *h, double dt, double Ti0, int64_t nsteps);
 int mpm_sync(mpm_handle *h);
 
 /* ---- tuning (no counterpart in the reference) ----
- * Run-time choices of the step: the cell re-sort period (steps) and the
- * particle-pass variant (0 = per-particle kernels with vector reductions into
- * L2, 1 = shared-memory tiled kernels).  mpm_autotune times each of the sort
- * periods 4, 8, 16, 32 with each variant on `steps_per_trial` REAL steps of
- * the model (8 trials; they advance the simulation exactly like mpm_step, from
- * Ti0, and *Ti_out receives the end time), keeps the fastest and reports it;
- * trial_ms (optional, trial_cap entries) receives each trial's ms per step in
- * the order variant-major, period-minor. */
+ * Run-time choices of the step: the cell re-sort period (steps), the
+ * particle-pass variant (0 = the default passes: in FP32 with va = :a and no
+ * PIC/MVL/USL/two-phase the shared-memory box passes, one warp per tile of 32
+ * cells, else per-particle kernels with vector reductions into L2; 1 =
+ * shared-memory tiled kernels) and the sort's tile shape (cells; 3D 2x8x2
+ * (default), 4x8x1, 4x4x2; 2D 4x8 (default), 2x16; mpm_set_tile re-sorts at
+ * the next step).  mpm_autotune times, on REAL steps of the model (they advance
+ * the simulation exactly like mpm_step, from Ti0, and *Ti_out receives the end
+ * time), every tile shape with the re-sort periods 8, 16, 32, 64 (default
+ * passes), then the tiled passes at periods 16 and 32; each trial runs
+ * max(steps_per_trial, period) steps starting with a sort.  It keeps the
+ * fastest (mpm_get_tile reports its shape) and writes each trial's ms per step
+ * to trial_ms (optional, trial_cap entries) in that order. */
 int mpm_set_tuning(mpm_handle *h, int32_t sort_every, int32_t tiled);
 int mpm_get_tuning(mpm_handle *h, int32_t *sort_every, int32_t *tiled);
+int mpm_set_tile(mpm_handle *h, int32_t tx, int32_t ty, int32_t tz);
+int mpm_get_tile(mpm_handle *h, int32_t *tx, int32_t *ty, int32_t *tz);
 int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, double *Ti_out,
                  int32_t *sort_every_out, int32_t *tiled_out, double *trial_ms, int32_t trial_cap);
 

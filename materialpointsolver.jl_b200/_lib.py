@@ -41,7 +41,7 @@ EXPORTS = [
     "mpm_download", "mpm_compute_p2c", "mpm_download_order", "mpm_sort", "mpm_run_stages",
     "mpm_download_grid", "mpm_get_stats", "mpm_last_error", "mpm_peak_bandwidth",
     "mpm_set_profiling", "mpm_get_kernel_times", "mpm_abi_sizes", "mpm_cell_order_noalloc",
-    "mpm_grf_eval", "mpm_set_tuning", "mpm_get_tuning", "mpm_autotune",
+    "mpm_grf_eval", "mpm_set_tuning", "mpm_get_tuning", "mpm_set_tile", "mpm_get_tile", "mpm_autotune",
     "mpm_mlp_nparams", "mpm_mlp_forward", "mpm_mlp_grad", "mpm_mlp_adam", "mpm_set_surrogate", "mpm_log_samples",
     "mpm_h5_create", "mpm_h5_write", "mpm_h5_close", "mpm_snapshot", "mpm_snapshot_wait",
 ]
@@ -153,6 +153,8 @@ def lib():
     L.mpm_cell_order_noalloc.argtypes = [C.POINTER(Desc)] + [C.c_void_p] * 6
     L.mpm_set_tuning.argtypes = [vp, C.c_int32, C.c_int32]
     L.mpm_get_tuning.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.mpm_set_tile.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
+    L.mpm_get_tile.argtypes = [vp] + [C.POINTER(C.c_int32)] * 3
     L.mpm_autotune.argtypes = [vp, C.c_double, C.c_double, C.c_int64, C.POINTER(C.c_double),
                                C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32]
     L.mpm_set_surrogate.argtypes = [vp, vp, vp, C.c_int32, C.c_float, C.c_float, C.c_int32]

@@ -55,6 +55,16 @@ struct KTimer {
     int64_t n = 0;
 };
 
+// The tile shapes the autotuner tries (32 cells, one warp lane per cell; the
+// box passes are compiled for these), default first.
+struct TileShape {
+    int tx, ty, tz;
+};
+inline std::vector<TileShape> tile_shapes(int dim) {
+    if (dim == 3) return {{2, 8, 2}, {4, 8, 1}, {4, 4, 2}};
+    return {{4, 8, 1}, {2, 16, 1}};
+}
+
 }  // namespace
 
 namespace mpm_detail {
@@ -70,6 +80,7 @@ struct GraphCache {
     int sort_every = 0;
     bool tiled = false;
     int surr_mode = 0;
+    int tile = 0;   // tx | ty << 8 | tz << 16
     int64_t launches = 0, steps = 0, sorts = 0;
 };
 
@@ -158,7 +169,7 @@ struct mpm_handle {
     // sort
     uint32_t *keys = nullptr, *cnt = nullptr, *off = nullptr, *bsum = nullptr, *big = nullptr, *nbig = nullptr;
     uint2 *pairs = nullptr, *pairs2 = nullptr;
-    uint32_t nk = 0, big_cap = 0;
+    uint32_t nk = 0, big_cap = 0, nk_cap = 0;
     uint32_t *tiles = nullptr, *ntiles = nullptr;
     uint32_t ntile_total = 0;
     int nsm = 148;
@@ -657,6 +668,8 @@ template <int D, int TX, int TY, int TZ> struct BoxPass {
     }
 };
 
+int tile_code(const SortGeom &sg) { return sg.tx | sg.ty << 8 | sg.tz << 16; }
+
 // Shared-memory limits of the box passes (outside any stream capture).
 void box_prepare(mpm_handle *h) {
 #define MPM_BOX_PREP(D, A, B, C) \
@@ -844,7 +857,7 @@ template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double T
     GraphCache &gc = h->graph;
     const int S = h->sort_every;
     const bool match = gc.exec && gc.dt == dt && gc.pbuf0 == h->pbuf[0] && gc.sort_every == S &&
-                       gc.tiled == h->tiled && gc.surr_mode == h->surr_mode;
+                       gc.tiled == h->tiled && gc.surr_mode == h->surr_mode && gc.tile == tile_code(h->sg);
     if (!match) {
         if (gc.exec) { cudaGraphExecDestroy(gc.exec); gc.exec = nullptr; }
         if (h->tiled) {   // kernel attributes are set outside the capture
@@ -871,6 +884,7 @@ template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double T
         gc.sort_every = S;
         gc.tiled = h->tiled;
         gc.surr_mode = h->surr_mode;
+        gc.tile = tile_code(h->sg);
         gc.launches = h->launches - l0;
         gc.steps = h->steps_done - s0;
         gc.sorts = h->sorts_done - q0;
@@ -1571,21 +1585,28 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         if (tsh[0] < 1 || tsh[1] < 1 || tsh[2] < 1 || (cpt != 32 && cpt != 64 && cpt != 128))
             throw Err{MPM_E_ARG, "tile shape must hold 32, 64 or 128 cells"};
         const int64_t nk = sort_geom(sg, d->dim, d->nnx, d->nny, nnz, tsh[0], tsh[1], tsh[2]);
-        if (nk >= (int64_t)LOW29 || d->np >= (int64_t)LOW29)
+        // the sort buffers hold the keys of any tile shape mpm_set_tile may pick
+        int64_t nk_max = nk;
+        for (const TileShape &ts : tile_shapes(d->dim)) {
+            SortGeom t{};
+            nk_max = std::max(nk_max, sort_geom(t, d->dim, d->nnx, d->nny, nnz, ts.tx, ts.ty, ts.tz));
+        }
+        if (nk_max >= (int64_t)LOW29 || d->np >= (int64_t)LOW29)
             throw Err{MPM_E_ARG, "grid or particle count beyond the sort's 2^29 limit"};
         h->nk = (uint32_t)nk;
+        h->nk_cap = (uint32_t)nk_max;
         int64_t npa = std::max<int64_t>(d->np, 1);
         h->keys = (uint32_t *)dalloc(h, npa * 4);
-        h->cnt = (uint32_t *)dalloc(h, (size_t)h->nk * 4);
-        h->off = (uint32_t *)dalloc(h, ((size_t)h->nk + 1) * 4);
-        h->bsum = (uint32_t *)dalloc(h, (cdiv(h->nk, SCAN_CHUNK) + 1) * 4);
+        h->cnt = (uint32_t *)dalloc(h, (size_t)h->nk_cap * 4);
+        h->off = (uint32_t *)dalloc(h, ((size_t)h->nk_cap + 1) * 4);
+        h->bsum = (uint32_t *)dalloc(h, (cdiv(h->nk_cap, SCAN_CHUNK) + 1) * 4);
         h->big_cap = 65536;
         h->big = (uint32_t *)dalloc(h, h->big_cap * 4);
         h->nbig = (uint32_t *)dalloc(h, 4);
         h->pairs = (uint2 *)dalloc(h, npa * 8);
         h->pairs2 = (uint2 *)dalloc(h, npa * 8);
         h->ntile_total = h->nk / (uint32_t)sg.cpt;
-        h->tiles = (uint32_t *)dalloc(h, (size_t)h->ntile_total * 4);
+        h->tiles = (uint32_t *)dalloc(h, (size_t)(h->nk_cap / 32 + 1) * 4);
         h->ntiles = (uint32_t *)dalloc(h, 4);
         CK(cudaMemset(h->ntiles, 0, 4));
         CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, d->device));
@@ -1747,12 +1768,43 @@ int mpm_get_tuning(mpm_handle *h, int32_t *sort_every, int32_t *tiled) {
     return MPM_OK;
 }
 
-// Times every candidate (sort period x particle-pass variant) on steps_per_trial
-// real steps of the simulation, each trial starting with a fresh sort, and
-// keeps the fastest.  The trial steps advance the model like mpm_step does.
+int mpm_set_tile(mpm_handle *h, int32_t tx, int32_t ty, int32_t tz) {
+    if (!h) return MPM_E_ARG;
+    try {
+        const int D = h->d.dim;
+        if (D == 2) tz = 1;
+        bool known = false;
+        for (const TileShape &t : tile_shapes(D)) known = known || (t.tx == tx && t.ty == ty && t.tz == tz);
+        if (!known) throw Err{MPM_E_ARG, "tile shape not among the compiled ones (3D: 2x8x2, 4x8x1, 4x4x2; 2D: 4x8, 2x16)"};
+        SortGeom sg{};
+        const int64_t nk = sort_geom(sg, D, h->d.nnx, h->d.nny, D == 3 ? h->d.nnz : 1, tx, ty, tz);
+        if (nk > (int64_t)h->nk_cap) throw Err{MPM_E_STATE, "tile shape needs more sort keys than allocated"};
+        h->sg = sg;
+        h->nk = (uint32_t)nk;
+        h->ntile_total = h->nk / (uint32_t)sg.cpt;
+        h->since_sort = 1 << 30;   // the next step re-sorts with the new tiles
+        return MPM_OK;
+    } catch (const Err &e) { return fail(h, e); }
+}
+
+int mpm_get_tile(mpm_handle *h, int32_t *tx, int32_t *ty, int32_t *tz) {
+    if (!h) return MPM_E_ARG;
+    if (tx) *tx = h->sg.tx;
+    if (ty) *ty = h->sg.ty;
+    if (tz) *tz = h->sg.tz;
+    return MPM_OK;
+}
+
+// Times every candidate on real steps of the simulation and keeps the fastest.
+// Candidates, in the order of trial_ms: for each compiled tile shape (the
+// default first) the re-sort periods 8, 16, 32, 64 with the default particle
+// passes, then the shared-memory tiled passes (default shape) at periods 16
+// and 32.  A trial runs max(steps_per_trial, period) steps starting with a
+// sort, so the sort is charged once per period.  The trial steps advance the
+// model like mpm_step does.  The chosen shape is reported by mpm_get_tile.
 int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, double *Ti_out,
                  int32_t *sort_every_out, int32_t *tiled_out, double *trial_ms, int32_t trial_cap) {
-    static const int32_t periods[] = {4, 8, 16, 32};
+    static const int32_t periods[] = {8, 16, 32, 64};
     if (!h) return MPM_E_ARG;
     if (steps_per_trial < 1) {
         h->last_error = "steps_per_trial must be >= 1";
@@ -1761,20 +1813,29 @@ int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, 
     double Ti = Ti0;
     double best = 1e300;
     int32_t best_s = h->sort_every, best_t = h->tiled ? 1 : 0;
+    TileShape best_shape{h->sg.tx, h->sg.ty, h->sg.tz};
     int k = 0;
-    for (int32_t t = 0; t < 2; ++t) {
-        for (int32_t S : periods) {
-            int rc = mpm_set_tuning(h, S, t);
-            if (rc) return rc;
-            h->since_sort = 1 << 30;   // every trial starts with a sort
-            rc = mpm_step(h, dt, Ti, steps_per_trial, &Ti);
-            if (rc) return rc;
-            const double ms = h->last_step_ms / (double)steps_per_trial;
-            if (trial_ms && k < trial_cap) trial_ms[k] = ms;
-            ++k;
-            if (ms < best) { best = ms; best_s = S; best_t = t; }
-        }
-    }
+    auto trial = [&](const TileShape &ts, int32_t S, int32_t t) -> int {
+        int rc = mpm_set_tile(h, ts.tx, ts.ty, ts.tz);
+        if (!rc) rc = mpm_set_tuning(h, S, t);
+        if (rc) return rc;
+        h->since_sort = 1 << 30;   // every trial starts with a sort
+        const int64_t n = std::max<int64_t>(steps_per_trial, S);
+        rc = mpm_step(h, dt, Ti, n, &Ti);
+        if (rc) return rc;
+        const double ms = h->last_step_ms / (double)n;
+        if (trial_ms && k < trial_cap) trial_ms[k] = ms;
+        ++k;
+        if (ms < best) { best = ms; best_s = S; best_t = t; best_shape = ts; }
+        return MPM_OK;
+    };
+    const std::vector<TileShape> shapes = tile_shapes(h->d.dim);
+    for (const TileShape &ts : shapes)
+        for (int32_t S : periods)
+            if (int rc = trial(ts, S, 0)) return rc;
+    for (int32_t S : {16, 32})
+        if (int rc = trial(shapes[0], S, 1)) return rc;
+    mpm_set_tile(h, best_shape.tx, best_shape.ty, best_shape.tz);
     mpm_set_tuning(h, best_s, best_t);
     if (Ti_out) *Ti_out = Ti;
     if (sort_every_out) *sort_every_out = best_s;

@@ -174,15 +174,27 @@ class DeviceModel:
         _lib.check(_lib.lib().mpm_get_tuning(self.h, C.byref(s), C.byref(t)), self.h)
         return s.value, bool(t.value)
 
+    def set_tile(self, tx, ty, tz=1):
+        """Sort tile shape in cells (one of the compiled shapes); the next step re-sorts."""
+        _lib.check(_lib.lib().mpm_set_tile(self.h, int(tx), int(ty), int(tz)), self.h)
+
+    def tile(self):
+        t = [C.c_int32() for _ in range(3)]
+        _lib.check(_lib.lib().mpm_get_tile(self.h, *[C.byref(x) for x in t]), self.h)
+        return tuple(x.value for x in t)
+
     def autotune(self, dt, Ti, steps_per_trial=32):
-        """Time every (sort period, particle-pass variant) candidate on real
-        steps of this model and keep the fastest.  Returns (Ti after the trial
-        steps, sort_every, tiled, per-trial ms per step)."""
+        """Time every (tile shape, sort period, particle-pass variant)
+        candidate on real steps of this model and keep the fastest.  Returns
+        (Ti after the trial steps, sort_every, tiled, per-trial ms per step in
+        the library's candidate order); self.tile() gives the chosen shape."""
         Tout, s, t = C.c_double(), C.c_int32(), C.c_int32()
-        ms = (C.c_double * 8)()
+        cap = 32
+        ms = (C.c_double * cap)()
         _lib.check(_lib.lib().mpm_autotune(self.h, dt, Ti, steps_per_trial, C.byref(Tout), C.byref(s),
-                                           C.byref(t), ms, 8), self.h)
-        return Tout.value, s.value, bool(t.value), list(ms)
+                                           C.byref(t), ms, cap), self.h)
+        ntrial = 4 * (3 if self.grid.dim == 3 else 2) + 2
+        return Tout.value, s.value, bool(t.value), list(ms)[:ntrial]
 
     # stress-return surrogate (no counterpart in the reference)
     def set_surrogate(self, sur, tol=1e-3, sref=1e3):

@@ -109,21 +109,26 @@ def test_batch_matches_oracle(pkg, orc, gpu_lib):
 
 
 @pytest.mark.gpu
-def test_autotune_steps_are_model_steps(pkg, orc, gpu_lib):
-    """The autotuner's 8 trials of 12 steps are 96 ordinary steps: the state
-    equals the oracle's after 96 steps, and the chosen tuning is one of the
-    candidates and stays set."""
-    case = small_batch(pkg, 3, gpu_precision="fp64")
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_autotune_steps_are_model_steps(pkg, orc, gpu_lib, prec, tol):
+    """The autotuner's trials (2 tile shapes x re-sort periods 8, 16, 32, 64 at
+    max(12, period) steps each, then the tiled passes at periods 16 and 32)
+    are 296 ordinary steps: the state equals the oracle's after 296 steps (in
+    the mixed mode through the box passes of every tile shape), and the chosen
+    tuning is one of the candidates and stays set."""
+    case = small_batch(pkg, 3, gpu_precision=prec)
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
     Ti, S, tiled, ms = dev.autotune(case.dt, 0.0, 12)
-    assert S in (4, 8, 16, 32) and all(m > 0 for m in ms)
+    nsteps = 2 * (12 + 16 + 32 + 64) + 16 + 32
+    assert S in (8, 16, 32, 64) and len(ms) == 10 and all(m > 0 for m in ms)
     assert dev.tuning() == (S, tiled)
-    assert Ti == pytest.approx(96 * case.dt, rel=1e-12)
-    assert dev.stats().steps_done == 96
+    assert dev.tile() in ((4, 8, 1), (2, 16, 1))
+    assert Ti == pytest.approx(nsteps * case.dt, rel=1e-12)
+    assert dev.stats().steps_done == nsteps
     out = fresh_particles(pkg, case.mp)
     dev.download(pkg._lib.F_REFERENCE, out)
     dev.close()
     o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc)
-    o.run(case.dt, 0.0, 96)
-    assert rel(out.xi - case.mp.xi, o.xi - case.mp.xi) < 1e-9
-    assert rel(out.sig, o.sig) < 1e-9
+    o.run(case.dt, 0.0, nsteps)
+    assert rel(out.xi - case.mp.xi, o.xi - case.mp.xi) < tol
+    assert rel(out.sig, o.sig) < (tol if prec == "fp64" else 1e-3)
