@@ -214,6 +214,9 @@ EXAMPLES = {"example3d": ("collapse_3d_example", EXAMPLE3D_PUBLISHED,
                           "examples/2d_collapse.ipynb:385: 2.11e3 it/s x 20 000 particles, FP64, unstated NVIDIA GPU")}
 
 
+PASS_VARIANTS = {0: "lane-merged per-particle", 1: "tiled", 2: "box"}
+
+
 def make_case(mc3d, workload="column3d", surrogate=False):
     import __graft_entry__ as g
     pkg = g.load_package()
@@ -358,8 +361,9 @@ def run_b200(args):
     if args.workload == "batch2d":
         # untimed: the autotuner's trials are real steps of the model
         Ti, S, tiled, trial_ms = dev.autotune(dt, Ti, 16)
-        tuning = {"sort_every": S, "tiled": tiled, "tile": dev.tile(), "trial_ms_per_step": trial_ms,
-                  "candidates": "tile shapes x sort periods 8/16/32/64 (box passes), tiled passes at 16/32; max(16, period) steps each"}
+        tuning = {"sort_every": S, "variant": PASS_VARIANTS[tiled], "tile": dev.tile(), "trial_ms_per_step": trial_ms,
+                  "candidates": "tile shapes x sort periods 8/16/32/64 (lane-merged passes), then tiled and box "
+                                "passes at 16/32; max(16, period) steps each"}
     surr_info = None
     if args.surrogate:
         if args.workload != "slope3d":
@@ -392,6 +396,7 @@ def run_b200(args):
     na = st.active_nodes
     Ti = advance_time(Ti, dt, K, dev.desc.time_f32)
     sort_used, tiled_used = dev.tuning()
+    tile_used = dev.tile()
     if surr_info is not None:
         st_s = dev.stats()
         surr_info["rows"] = int(st_s.surr_rows)
@@ -452,7 +457,7 @@ def run_b200(args):
                        particles=npart, nodes=case.grid.ni, active_nodes=na, h=case.meta["h"],
                        mc3d=args.mc3d, precision=("all FP64" if args.workload == "column2d"
                                                    else "FP32 bulk, FP64 positions and det(F)"), sort_every=sort_used,
-                       particle_passes="tiled" if tiled_used else "per-particle",
+                       particle_passes=PASS_VARIANTS[tiled_used], tile=tile_used,
                        l2=(f"particle state {npart * bp_step / 1e9:.2f} GB > 126 MB L2 (no flush needed)"
                            if npart * bp_step > 126e6 else
                            f"particle state {npart * bp_step / 1e6:.1f} MB < 126 MB L2: L2-resident, not "
@@ -543,7 +548,8 @@ def extra_forms(pkg, local, K, W):
     out["batch2d"] = {"workload": "256 independent 2D slopes in one grid (Drucker-Prager, FP32)",
                       "particles": int(case.mp.np), "ms_per_step": ms / K,
                       "particle_updates_per_s": case.mp.np * K / (ms * 1e-3),
-                      "tuning": {"sort_every": S, "tiled": tiled, "tile": tile, "trial_ms_per_step": trial_ms},
+                      "tuning": {"sort_every": S, "variant": PASS_VARIANTS[tiled], "tile": tile,
+                                 "trial_ms_per_step": trial_ms},
                       "runout_err_vs_alone": {"slopes": 2, "steps": n_total, "max": max(errs)}}
     del case
     # ---- slope3d, plain and surrogate from the same state ----

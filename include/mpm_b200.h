@@ -211,15 +211,16 @@ int mpm_sync(mpm_handle *h);
 
 /* ---- tuning (no counterpart in the reference) ----
  * Run-time choices of the step: the cell re-sort period (steps), the
- * particle-pass variant (0 = the default passes: in FP32 with va = :a and no
- * PIC/MVL/USL/two-phase the shared-memory box passes, one warp per tile of 32
- * cells, else per-particle kernels with vector reductions into L2; 1 =
- * shared-memory tiled kernels) and the sort's tile shape (cells; 3D 2x8x2
+ * particle-pass variant (0 = per-particle kernels whose scatters merge the
+ * windows of neighbouring lanes and reduce into L2, the default; 1 =
+ * shared-memory tiled kernels; 2 = box passes: one warp per tile of 32 cells
+ * with the tile's node data in shared memory, in FP32 with va = :a and no
+ * PIC/MVL/USL/two-phase, else variant 0) and the sort's tile shape (cells; 3D 2x8x2
  * (default), 4x8x1, 4x4x2; 2D 4x8 (default), 2x16; mpm_set_tile re-sorts at
  * the next step).  mpm_autotune times, on REAL steps of the model (they advance
  * the simulation exactly like mpm_step, from Ti0, and *Ti_out receives the end
  * time), every tile shape with the re-sort periods 8, 16, 32, 64 (default
- * passes), then the tiled passes at periods 16 and 32; each trial runs
+ * passes), then the tiled and the box passes at periods 16 and 32; each trial runs
  * max(steps_per_trial, period) steps starting with a sort.  It keeps the
  * fastest (mpm_get_tile reports its shape) and writes each trial's ms per step
  * to trial_ms (optional, trial_cap entries) in that order. */

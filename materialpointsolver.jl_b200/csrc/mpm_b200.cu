@@ -78,7 +78,7 @@ struct GraphCache {
     double dt = 0;
     void *pbuf0 = nullptr;
     int sort_every = 0;
-    bool tiled = false;
+    bool tiled = false, box = false;
     int surr_mode = 0;
     int tile = 0;   // tx | ty << 8 | tz << 16
     int64_t launches = 0, steps = 0, sorts = 0;
@@ -127,7 +127,7 @@ struct mpm_handle {
     bool prefetch = true;    // FP32 particle pass stages fields by cp.async (MPM_B200_PREFETCH=0 turns it off)
     bool cell_major = false; // order inside a tile: rank-major (default) or cell-major (MPM_B200_ORDER=cell)
     bool chain = true;       // FP32 scatters merge chained warp lanes (MPM_B200_CHAIN=0 turns it off)
-    bool box = true;         // FP32 MUSL passes with the tile's nodes in shared memory (MPM_B200_BOX=0: off)
+    bool box = false;        // FP32 MUSL passes with the tile's nodes in shared memory (variant 2; MPM_B200_BOX=1)
     uint32_t *work = nullptr;   // tile counters of the box passes
     GraphCache graph;
     int64_t graph_launches = 0;
@@ -857,7 +857,8 @@ template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double T
     GraphCache &gc = h->graph;
     const int S = h->sort_every;
     const bool match = gc.exec && gc.dt == dt && gc.pbuf0 == h->pbuf[0] && gc.sort_every == S &&
-                       gc.tiled == h->tiled && gc.surr_mode == h->surr_mode && gc.tile == tile_code(h->sg);
+                       gc.tiled == h->tiled && gc.box == h->box && gc.surr_mode == h->surr_mode &&
+                       gc.tile == tile_code(h->sg);
     if (!match) {
         if (gc.exec) { cudaGraphExecDestroy(gc.exec); gc.exec = nullptr; }
         if (h->tiled) {   // kernel attributes are set outside the capture
@@ -883,6 +884,7 @@ template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double T
         gc.pbuf0 = h->pbuf[0];
         gc.sort_every = S;
         gc.tiled = h->tiled;
+        gc.box = h->box;
         gc.surr_mode = h->surr_mode;
         gc.tile = tile_code(h->sg);
         gc.launches = h->launches - l0;
@@ -1752,19 +1754,20 @@ int mpm_log_samples(mpm_handle *h, float *feat, float *target, uint32_t *count, 
 
 int mpm_set_tuning(mpm_handle *h, int32_t sort_every, int32_t tiled) {
     if (!h) return MPM_E_ARG;
-    if (sort_every < 1 || sort_every > 1024 || (tiled != 0 && tiled != 1)) {
-        h->last_error = "sort_every must be 1..1024 and tiled 0 or 1";
+    if (sort_every < 1 || sort_every > 1024 || tiled < 0 || tiled > 2) {
+        h->last_error = "sort_every must be 1..1024 and the particle-pass variant 0, 1 or 2";
         return MPM_E_ARG;
     }
     h->sort_every = sort_every;
-    h->tiled = tiled != 0;
+    h->tiled = tiled == 1;
+    h->box = tiled == 2;
     return MPM_OK;
 }
 
 int mpm_get_tuning(mpm_handle *h, int32_t *sort_every, int32_t *tiled) {
     if (!h) return MPM_E_ARG;
     if (sort_every) *sort_every = h->sort_every;
-    if (tiled) *tiled = h->tiled ? 1 : 0;
+    if (tiled) *tiled = h->tiled ? 1 : (h->box ? 2 : 0);
     return MPM_OK;
 }
 
@@ -1798,8 +1801,8 @@ int mpm_get_tile(mpm_handle *h, int32_t *tx, int32_t *ty, int32_t *tz) {
 // Times every candidate on real steps of the simulation and keeps the fastest.
 // Candidates, in the order of trial_ms: for each compiled tile shape (the
 // default first) the re-sort periods 8, 16, 32, 64 with the default particle
-// passes, then the shared-memory tiled passes (default shape) at periods 16
-// and 32.  A trial runs max(steps_per_trial, period) steps starting with a
+// passes, then the shared-memory tiled passes and the box passes (default
+// shape) at periods 16 and 32 each.  A trial runs max(steps_per_trial, period) steps starting with a
 // sort, so the sort is charged once per period.  The trial steps advance the
 // model like mpm_step does.  The chosen shape is reported by mpm_get_tile.
 int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, double *Ti_out,
@@ -1812,7 +1815,7 @@ int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, 
     }
     double Ti = Ti0;
     double best = 1e300;
-    int32_t best_s = h->sort_every, best_t = h->tiled ? 1 : 0;
+    int32_t best_s = h->sort_every, best_t = h->tiled ? 1 : (h->box ? 2 : 0);
     TileShape best_shape{h->sg.tx, h->sg.ty, h->sg.tz};
     int k = 0;
     auto trial = [&](const TileShape &ts, int32_t S, int32_t t) -> int {
@@ -1833,8 +1836,9 @@ int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, 
     for (const TileShape &ts : shapes)
         for (int32_t S : periods)
             if (int rc = trial(ts, S, 0)) return rc;
-    for (int32_t S : {16, 32})
-        if (int rc = trial(shapes[0], S, 1)) return rc;
+    for (int32_t v : {1, 2})
+        for (int32_t S : {16, 32})
+            if (int rc = trial(shapes[0], S, v)) return rc;
     mpm_set_tile(h, best_shape.tx, best_shape.ty, best_shape.tz);
     mpm_set_tuning(h, best_s, best_t);
     if (Ti_out) *Ti_out = Ti;

@@ -166,13 +166,14 @@ class DeviceModel:
         return {names[i].decode(): (ms[i], nl[i]) for i in range(min(cnt.value, cap))}
 
     # run-time tuning of the step (no counterpart in the reference)
-    def set_tuning(self, sort_every, tiled=False):
-        _lib.check(_lib.lib().mpm_set_tuning(self.h, int(sort_every), int(bool(tiled))), self.h)
+    def set_tuning(self, sort_every, tiled=0):
+        """Re-sort period and particle-pass variant (0 lane-merged, 1 tiled, 2 box)."""
+        _lib.check(_lib.lib().mpm_set_tuning(self.h, int(sort_every), int(tiled)), self.h)
 
     def tuning(self):
         s, t = C.c_int32(), C.c_int32()
         _lib.check(_lib.lib().mpm_get_tuning(self.h, C.byref(s), C.byref(t)), self.h)
-        return s.value, bool(t.value)
+        return s.value, t.value
 
     def set_tile(self, tx, ty, tz=1):
         """Sort tile shape in cells (one of the compiled shapes); the next step re-sorts."""
@@ -186,15 +187,15 @@ class DeviceModel:
     def autotune(self, dt, Ti, steps_per_trial=32):
         """Time every (tile shape, sort period, particle-pass variant)
         candidate on real steps of this model and keep the fastest.  Returns
-        (Ti after the trial steps, sort_every, tiled, per-trial ms per step in
+        (Ti after the trial steps, sort_every, variant, per-trial ms per step in
         the library's candidate order); self.tile() gives the chosen shape."""
         Tout, s, t = C.c_double(), C.c_int32(), C.c_int32()
         cap = 32
         ms = (C.c_double * cap)()
         _lib.check(_lib.lib().mpm_autotune(self.h, dt, Ti, steps_per_trial, C.byref(Tout), C.byref(s),
                                            C.byref(t), ms, cap), self.h)
-        ntrial = 4 * (3 if self.grid.dim == 3 else 2) + 2
-        return Tout.value, s.value, bool(t.value), list(ms)[:ntrial]
+        ntrial = 4 * (3 if self.grid.dim == 3 else 2) + 4
+        return Tout.value, s.value, t.value, list(ms)[:ntrial]
 
     # stress-return surrogate (no counterpart in the reference)
     def set_surrogate(self, sur, tol=1e-3, sref=1e3):
