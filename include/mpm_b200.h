@@ -315,16 +315,23 @@ int mpm_mlp_grad(const float *params, const float *norm, const float *feat, cons
 int mpm_mlp_adam(float *params, float *grad, float *m, float *v, float lr, float b1, float b2, float eps,
                  int64_t step, void *stream);
 
-/* The surrogate inside the step (3D Drucker-Prager): with on = 1 every
+/* The surrogate inside the step (3D Drucker-Prager, or the restated 3D
+ * Mohr-Coulomb return of desc.mc3d = MPM_MC3D_RESTATED): with on = 1 every
  * yielding particle's return is deferred, the MLP (params / norm: HOST arrays
  * as above, copied) predicts it, and the prediction is kept when its yield
- * residual |f| / max(kphi, |qphi sigma_m|, sref) is at most tol, else the plain
- * return (dpP!) is used; plastic strains follow the plain return's closed-form
- * multiplier.  Counts in mpm_stats.surr_rows / surr_fallbacks.  on = 0
- * restores the plain return. */
+ * residual is at most tol -- Drucker-Prager: |f| / max(kphi, |qphi sigma_m|,
+ * sref); Mohr-Coulomb: the yield function of the trial's mode at the
+ * prediction, and neither yield function above it, relative to max(c,
+ * |sigma_m| tan(phi), sref) -- else the plain return (dpP! / the restated
+ * Mohr-Coulomb predictor-corrector) is used.  Drucker-Prager plastic strains
+ * follow the plain return's closed-form multiplier; an accepted Mohr-Coulomb
+ * row adds the plastic shear strain of its stress correction to epsq.
+ * Counts in mpm_stats.surr_rows / surr_fallbacks.  on = 0 restores the plain
+ * return. */
 int mpm_set_surrogate(mpm_handle *h, const float *params, const float *norm, int32_t flags, float tol, float sref,
                       int32_t on);
-/* Training samples from plain steps: one yielding particle in `every` (hashed
+/* Training samples from plain steps (3D Drucker-Prager or restated
+ * Mohr-Coulomb): one yielding particle in `every` (hashed
  * by index and step) writes its 16 features (trial stress 6, strain increment
  * 6, plastic strain, cohesion, friction, 0) to feat and the plain return's
  * stress to target (DEVICE arrays of cap rows); *count (device) counts rows

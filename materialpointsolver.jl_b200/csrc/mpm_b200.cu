@@ -136,6 +136,7 @@ struct mpm_handle {
     mpm::SurrCtx surr{};
     float *surr_params = nullptr, *surr_norm = nullptr, *surr_out = nullptr, *surr_feat = nullptr;
     uint32_t *surr_cnt = nullptr, *surr_list = nullptr;
+    float *surr_s0 = nullptr;   // deferred Mohr-Coulomb rows: rotated pre-increment stress (np x 6)
     unsigned long long *surr_stats = nullptr;   // rows deferred, fallbacks
     int *surr_err = nullptr;
     float surr_tol = 1e-3f, surr_sref = 1e3f;
@@ -583,7 +584,10 @@ template <int D, typename R> StepParams make_params(mpm_handle *h, double dt, do
     // is the reference's float type (the user's ϵ), whatever the device stores
     sp.meps = h->d.time_f32 ? 1.1920928955078125e-07 : 2.220446049250313e-16;
     sp.surr = h->surr;
-    sp.surr.mode = (D == 3 && h->d.constitutive == MPM_DRUCKERPRAGER && !h->ts) ? h->surr_mode : 0;
+    sp.surr.mode = (D == 3 && !h->ts && (h->d.constitutive == MPM_DRUCKERPRAGER ||
+                                          (h->d.constitutive == MPM_MOHRCOULOMB && h->d.mc3d == MPM_MC3D_RESTATED)))
+                       ? h->surr_mode
+                       : 0;
     sp.surr.salt = (uint32_t)(h->steps_done * 0x9E3779B9ull);
     return sp;
 }
@@ -802,22 +806,29 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
     } else if (sp.surr.mode == 2 && sp.plastic && np) {
         // surrogate: G2P + update with the yielding particles' returns deferred,
         // the MLP over the deferred rows, accept-or-fallback, then the scatter
-        L.run("dmap", [&] { k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("dmap", [&] { k_dmap_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         CK(cudaMemsetAsync(h->surr_cnt, 0, 4, h->stream));
-        L.run("g2p", [&] { k_g2p<D, R, false><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp); });
+        L.run("g2p", [&] {
+            if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+            else k_g2p<D, R, false><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+        });
         L.run("mlp", [&] {
             CK(mpm_detail::mlp_forward_dev(h->surr_params, h->surr_norm, h->surr_feat, h->surr_out, np, h->surr_cnt,
                                            h->surr_residual, h->surr_err, h->stream, h->nsm));
         });
         if constexpr (D == 3) {
             L.run("surr_fix", [&] {
-                k_surr_fix<R><<<h->nsm * 8, 256, 0, h->stream>>>(P, g, sp.surr, h->surr_out, h->surr_tol, h->surr_sref,
-                                                              h->surr_stats);
+                if (mc3)
+                    k_surr_fix_mc<R><<<h->nsm * 8, 256, 0, h->stream>>>(P, g, sp.surr, h->surr_out, h->surr_tol,
+                                                                     h->surr_sref, h->surr_stats);
+                else
+                    k_surr_fix<R><<<h->nsm * 8, 256, 0, h->stream>>>(P, g, sp.surr, h->surr_out, h->surr_tol,
+                                                                  h->surr_sref, h->surr_stats);
             });
         }
-        L.run("p2g", [&] { k_p2g<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("p2g", [&] { k_p2g_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
     } else if (std::is_same<R, float>::value && h->box && sp.va == MPM_VA_A && !sp.need_vs && box_shape_ok(h)) {
         // FP32 MUSL :a: the box passes (node data of a tile in shared memory)
         if constexpr (std::is_same<R, float>::value) {
@@ -1693,8 +1704,10 @@ int mpm_set_surrogate(mpm_handle *h, const float *params, const float *norm, int
             return MPM_OK;
         }
         if (!params || !norm || !(tol > 0) || !(sref > 0)) throw Err{MPM_E_ARG, "surrogate: params, norm, tol > 0, sref > 0"};
-        if (h->d.dim != 3 || h->d.constitutive != MPM_DRUCKERPRAGER)
-            throw Err{MPM_E_UNSUPPORTED, "the surrogate replaces the 3D Drucker-Prager return"};
+        const bool mc = h->d.constitutive == MPM_MOHRCOULOMB && h->d.mc3d == MPM_MC3D_RESTATED;
+        if (h->d.dim != 3 || (h->d.constitutive != MPM_DRUCKERPRAGER && !mc))
+            throw Err{MPM_E_UNSUPPORTED,
+                      "the surrogate replaces the 3D Drucker-Prager or the restated 3D Mohr-Coulomb return"};
         if (h->d.mvl || h->d.scheme != MPM_SCHEME_MUSL)
             throw Err{MPM_E_UNSUPPORTED, "the surrogate runs with the MUSL scheme and without MVL"};
         const int64_t np = h->d.np;
@@ -1705,6 +1718,7 @@ int mpm_set_surrogate(mpm_handle *h, const float *params, const float *norm, int
             h->surr_feat = (float *)dalloc(h, (size_t)std::max<int64_t>(np, 1) * 16 * 4);
             h->surr_out = (float *)dalloc(h, (size_t)std::max<int64_t>(np, 1) * 6 * 4);
             h->surr_list = (uint32_t *)dalloc(h, (size_t)std::max<int64_t>(np, 1) * 4);
+            h->surr_s0 = (float *)dalloc(h, (size_t)std::max<int64_t>(np, 1) * 6 * 4);
             h->surr_cnt = (uint32_t *)dalloc(h, 4);
             h->surr_stats = (unsigned long long *)dalloc(h, 16);
             h->surr_err = (int *)dalloc(h, 4);
@@ -1723,6 +1737,7 @@ int mpm_set_surrogate(mpm_handle *h, const float *params, const float *norm, int
         h->surr.feat = h->surr_feat;
         h->surr.cnt = h->surr_cnt;
         h->surr.list = h->surr_list;
+        h->surr.tgt = mc ? h->surr_s0 : nullptr;   // Mohr-Coulomb: the deferred rows' pre-increment stress
         h->surr_mode = 2;
         return MPM_OK;
     } catch (const Err &e) { return fail(h, e); }
@@ -1738,8 +1753,9 @@ int mpm_log_samples(mpm_handle *h, float *feat, float *target, uint32_t *count, 
         h->last_error = "mpm_log_samples: feat, target, count and cap > 0 are required";
         return MPM_E_ARG;
     }
-    if (h->d.dim != 3 || h->d.constitutive != MPM_DRUCKERPRAGER) {
-        h->last_error = "sample logging covers the 3D Drucker-Prager return";
+    if (h->d.dim != 3 || !(h->d.constitutive == MPM_DRUCKERPRAGER ||
+                           (h->d.constitutive == MPM_MOHRCOULOMB && h->d.mc3d == MPM_MC3D_RESTATED))) {
+        h->last_error = "sample logging covers the 3D Drucker-Prager and the restated 3D Mohr-Coulomb return";
         return MPM_E_UNSUPPORTED;
     }
     h->surr = mpm::SurrCtx{};

@@ -1015,10 +1015,18 @@ __device__ __forceinline__ bool hash_keep(int64_t i, uint32_t salt, uint32_t eve
     return every <= 1 || x % every == 0;
 }
 
-// one row of surrogate features (and, when `out` is given, its target)
+// restated 3D Mohr-Coulomb parameters of a material
+template <typename R> __device__ __forceinline__ mc3d::Par mc3d_par(const Mat<R> &M) {
+    return mc3d::Par{(double)M.K, (double)M.G, (double)M.c, (double)M.phi, (double)M.psi,
+                     (double)M.sigt, (double)M.sphi, (double)M.cphi, (double)M.tphi, (double)M.tpsi};
+}
+
+// one row of surrogate features (and, when `out` is given, its target; when
+// `s0` is given -- a deferred Mohr-Coulomb return -- the rotated pre-increment
+// stress, in the target row, which deferral leaves unused)
 template <typename R>
 __device__ __forceinline__ void surr_features(const SurrCtx &c, int64_t i, const R *trial, const R *de, R eq,
-                                              const Mat<R> &M, const R *out) {
+                                              const Mat<R> &M, const R *out, const R *s0 = nullptr) {
     const uint32_t r = atomicAdd(c.cnt, 1u);
     if (r >= c.cap) return;
     float4 *f = reinterpret_cast<float4 *>(c.feat + (size_t)r * 16);
@@ -1029,6 +1037,10 @@ __device__ __forceinline__ void surr_features(const SurrCtx &c, int64_t i, const
     if (out) {
 #pragma unroll
         for (int k = 0; k < 6; ++k) c.tgt[(size_t)r * 6 + k] = (float)out[k];
+    }
+    if (s0 && c.tgt) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) c.tgt[(size_t)r * 6 + k] = (float)s0[k];
     }
     if (c.list) c.list[r] = (uint32_t)i;
 }
@@ -1136,13 +1148,28 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
         double sd[6], s0d[6], ded[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) { sd[k] = s[k]; s0d[k] = srot[k]; ded[k] = de[k]; }
-        const mc3d::Par mp = {(double)M.K, (double)M.G, (double)M.c, (double)M.phi, (double)M.psi,
-                              (double)M.sigt, (double)M.sphi, (double)M.cphi, (double)M.tphi, (double)M.tpsi};
-        const mc3d::Ret r = mc3d::mohr_coulomb_3d(sd, s0d, ded, mp);
-        if (r.yielded) {
+        const mc3d::Par mp = mc3d_par<R>(M);
+        if (sp.surr.mode == 2) {
+            // surrogate: a yielding trial keeps its trial stress and is queued
+            // (features, and the rotated pre-increment stress the fallback needs)
+            mc3d::Inv v;
+            double ft, fs;
+            mc3d::invariants(sd, v);
+            if (mc3d::yield(v, mp, ft, fs) != mc3d::ELASTIC) {
+                const R eq = pf(pre, PF_EPSQ, P.epsq + i);
+                surr_features<R>(sp.surr, i, s, de, eq, M, nullptr, srot);
+            }
+        } else {
+            const mc3d::Ret r = mc3d::mohr_coulomb_3d(sd, s0d, ded, mp);
+            if (r.yielded) {
+                R trial[6];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) s[k] = (R)sd[k];
-            stcs(P.epsq + i, (R)((double)pf(pre, PF_EPSQ, P.epsq + i) + r.dq));
+                for (int k = 0; k < 6; ++k) { trial[k] = s[k]; s[k] = (R)sd[k]; }
+                const R eq0 = pf(pre, PF_EPSQ, P.epsq + i);
+                stcs(P.epsq + i, (R)((double)eq0 + r.dq));
+                if (sp.surr.mode == 1 && hash_keep(i, sp.surr.salt, sp.surr.every))
+                    surr_features<R>(sp.surr, i, trial, de, eq0, M, s);
+            }
         }
     }
 #pragma unroll
@@ -1469,6 +1496,120 @@ __global__ void __launch_bounds__(256) k_surr_fix(PDev<3, R> P, GDev<R> g, SurrC
         atomicAdd(&stats[0], (unsigned long long)nrows);
         atomicAdd(&stats[1], (unsigned long long)nfall);
     }
+}
+
+// The deferred restated 3D Mohr-Coulomb returns (mohr_coulomb_3d): keep the
+// network's stress σ̂ when it lies on the yield surface the trial crossed --
+// |f_mode(σ̂)| <= tol·scale and neither yield function above tol·scale, with
+// scale = max(c, |σ̂m|·tanφ, sref) -- else run the plain return from the
+// trial stress (stored as the particle's stress), the rotated pre-increment
+// stress (kept in the row's target slot) and the strain increment (features
+// 6..11).  An accepted row's ϵq grows by √(2/3)·|e|, e = dev(σtrial - σ̂)/(2G),
+// the plastic shear strain of the correction (ϵq does not enter the restated
+// return: it has no softening).
+template <typename R>
+__global__ void __launch_bounds__(256) k_surr_fix_mc(PDev<3, R> P, GDev<R> g, SurrCtx c, const float *out, float tol,
+                                                     float sref, unsigned long long *stats) {
+    const uint32_t n = min(*c.cnt, c.cap);
+    uint32_t nfall = 0, nrows = 0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int64_t i = c.list[k];
+        Mat<R> M = g.mat[P.mat[i]];
+        if (P.coh) M.c = P.coh[i];
+        const mc3d::Par mp = mc3d_par<R>(M);
+        double tr[6], s0[6], de[6], sh[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            tr[q] = (double)P.sig[q][i];
+            s0[q] = (double)c.tgt[(size_t)k * 6 + q];
+            de[q] = (double)c.feat[(size_t)k * 16 + 6 + q];
+            sh[q] = (double)out[(size_t)k * 6 + q];
+        }
+        mc3d::Inv vt, vh;
+        double ftt, fst, fth, fsh;
+        mc3d::invariants(tr, vt);
+        const int type = mc3d::yield(vt, mp, ftt, fst);
+        mc3d::invariants(sh, vh);
+        mc3d::yield(vh, mp, fth, fsh);
+        const double scale = fmax(fmax(mp.c, fabs(vh.sm) * mp.tphi), (double)sref);
+        const double fact = type == mc3d::TENSILE ? fth : fsh;
+        const bool ok = isfinite(fact) && isfinite(fsh) && isfinite(fth) && fabs(fact) <= tol * scale &&
+                        fmax(fth, fsh) <= tol * scale;
+        double dq;
+        if (ok) {
+            const double ds = ((tr[0] - sh[0]) + (tr[1] - sh[1]) + (tr[2] - sh[2])) / 3.0;
+            double ee = 0.0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const double e = ((tr[q] - sh[q]) - ds) / (2.0 * mp.G);
+                ee += e * e;
+            }
+#pragma unroll
+            for (int q = 3; q < 6; ++q) {
+                const double e = (tr[q] - sh[q]) / (2.0 * mp.G);
+                ee += 2.0 * e * e;
+            }
+            dq = sqrt(2.0 / 3.0 * ee);
+        } else {
+            const mc3d::Ret r = mc3d::mohr_coulomb_3d(tr, s0, de, mp);
+            dq = r.dq;
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) P.sig[q][i] = (R)(ok ? sh[q] : tr[q]);
+        P.epsq[i] = (R)((double)P.epsq[i] + dq);
+        nfall += ok ? 0u : 1u;
+        nrows += 1u;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nfall += __shfl_xor_sync(0xffffffffu, nfall, o);
+        nrows += __shfl_xor_sync(0xffffffffu, nrows, o);
+    }
+    if ((threadIdx.x & 31) == 0 && nrows) {
+        atomicAdd(&stats[0], (unsigned long long)nrows);
+        atomicAdd(&stats[1], (unsigned long long)nfall);
+    }
+}
+
+// P2G_OS! alone (the scatter after the surrogate's accept-or-fallback pass),
+// with the scatters of chained lanes merged.
+template <int D, typename R = float>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM_P_MINB)
+    k_p2g_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool live = i < sp.np;
+    AxisW<R> w[3];
+    R s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, v[3] = {0, 0, 0}, m = 0;
+    if (live) {
+        double x[3];
+        load_x<D, R>(P, i, x);
+        if (!particle_weights<D, R>(x, g, w)) {
+            atomicOr(g.err, ERR_OOG);
+            live = false;
+        } else {
+#pragma unroll
+            for (int d = 0; d < D; ++d) v[d] = ldcs(P.v[d] + i);
+#pragma unroll
+            for (int k = 0; k < PDev<D, R>::NV; ++k) s[k] = ldcs(P.sig[k] + i);
+            m = ldcs(P.m + i);
+            vol = ldcs(P.vol + i);
+        }
+    }
+    int n0 = 0, key = dead_key();
+    if (live) {
+        n0 = key = window_n0<D, R>(g, w);
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            w[a].base = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { w[a].N[k] = R(0.0); w[a].dN[k] = R(0.0); }
+        }
+    }
+    MarkState mk;
+    if (live) mk = mark_begin<D, R>(g, w);
+    p2g_scatter_chain<D, R>(g, w, n0, key, m, vol, v, s, (R)sp.G);
+    if (live) mark_end<R>(g, mk);
 }
 
 // p2c of the current positions, 1-based, in the original particle order.
