@@ -290,7 +290,8 @@ int mpm_grf_eval(int32_t device, const double *x, const double *y, const double 
                  const double *harm, int64_t nh, double scale, double *out);
 
 /* ---- stress-return surrogate (no counterpart in the reference) ----
- * A 15 -> 64 -> 64 -> 64 -> 6 GELU MLP standing in for the Drucker-Prager /
+ * A 15 -> 64 -> 64 -> 64 -> 6 MLP (GELU in the tanh form of Hendrycks & Gimpel
+ * 2016, hardware tanh) standing in for the Drucker-Prager /
  * Mohr-Coulomb return (druckerprager.jl:89-155), BF16 weights and FP32
  * accumulation on the tensor cores (tcgen05).  params: mpm_mlp_nparams() FP32
  * master values, per layer W[k][n] then b[n] with the input padded to 16 and

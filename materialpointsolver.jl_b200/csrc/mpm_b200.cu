@@ -810,9 +810,10 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         CK(cudaMemsetAsync(h->surr_cnt, 0, 4, h->stream));
-        L.run("g2p", [&] {
-            if (mc3) k_g2p<D, R, false, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
-            else k_g2p<D, R, false><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+        // the fused pass: particles whose return is deferred skip its scatter
+        L.run("g2p_p2g", [&] {
+            if (mc3) k_g2p_chain<D, D == 3, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            else k_g2p_chain<D, false, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
         });
         L.run("mlp", [&] {
             CK(mpm_detail::mlp_forward_dev(h->surr_params, h->surr_norm, h->surr_feat, h->surr_out, np, h->surr_cnt,
@@ -828,7 +829,9 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
                                                                   h->surr_sref, h->surr_stats);
             });
         }
-        L.run("p2g", [&] { k_p2g_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("p2g", [&] {
+            k_p2g_list<D, R><<<h->nsm * 8, 256, 0, h->stream>>>(P, g, sp, h->surr_list, h->surr_cnt, (uint32_t)np);
+        });
     } else if (std::is_same<R, float>::value && h->box && sp.va == MPM_VA_A && !sp.need_vs && box_shape_ok(h)) {
         // FP32 MUSL :a: the box passes (node data of a tile in shared memory)
         if constexpr (std::is_same<R, float>::value) {

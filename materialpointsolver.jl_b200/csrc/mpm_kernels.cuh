@@ -1026,14 +1026,15 @@ template <typename R> __device__ __forceinline__ mc3d::Par mc3d_par(const Mat<R>
 // stress, in the target row, which deferral leaves unused)
 template <typename R>
 __device__ __forceinline__ void surr_features(const SurrCtx &c, int64_t i, const R *trial, const R *de, R eq,
-                                              const Mat<R> &M, const R *out, const R *s0 = nullptr) {
+                                              const Mat<R> &M, const R *out, const R *s0 = nullptr,
+                                              float tag = 0.0f) {
     const uint32_t r = atomicAdd(c.cnt, 1u);
     if (r >= c.cap) return;
     float4 *f = reinterpret_cast<float4 *>(c.feat + (size_t)r * 16);
     f[0] = make_float4((float)trial[0], (float)trial[1], (float)trial[2], (float)trial[3]);
     f[1] = make_float4((float)trial[4], (float)trial[5], (float)de[0], (float)de[1]);
     f[2] = make_float4((float)de[2], (float)de[3], (float)de[4], (float)de[5]);
-    f[3] = make_float4((float)eq, (float)M.c, (float)M.phi, 0.0f);
+    f[3] = make_float4((float)eq, (float)M.c, (float)M.phi, tag);   // tag: the network ignores column 15
     if (out) {
 #pragma unroll
         for (int k = 0; k < 6; ++k) c.tgt[(size_t)r * 6 + k] = (float)out[k];
@@ -1051,7 +1052,8 @@ __device__ __forceinline__ void surr_features(const SurrCtx &c, int64_t i, const
 template <int D, typename R, bool MC3 = false>
 __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp,
                                                 int64_t i, double *x, const R *tT, const R *dF, R *s, R &vol,
-                                                const float *pre = nullptr, double *Jout = nullptr) {
+                                                const float *pre = nullptr, double *Jout = nullptr,
+                                                bool *deferred = nullptr) {
     constexpr int NV = PDev<D, R>::NV, NF = PDev<D, R>::NF;
     // position: ξ += ΔT·ΣN·vsT, accumulated in FP64
 #pragma unroll
@@ -1128,7 +1130,10 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
     if (sp.plastic && (sp.constitutive == 1 || (sp.constitutive == 2 && D == 2))) {
         R eq = pf(pre, PF_EPSQ, P.epsq + i), ek = pf(pre, PF_EPSK, P.epsk + i);
         if (D == 3 && sp.constitutive == 1 && sp.surr.mode == 2) {
-            if (dp_yielding<R>(s, M)) surr_features<R>(sp.surr, i, s, de, eq, M, nullptr);
+            if (dp_yielding<R>(s, M)) {
+                surr_features<R>(sp.surr, i, s, de, eq, M, nullptr);
+                if (deferred) *deferred = true;
+            }
         } else if (D == 3 && sp.constitutive == 1 && sp.surr.mode == 1) {
             R trial[6];
 #pragma unroll
@@ -1155,9 +1160,11 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
             mc3d::Inv v;
             double ft, fs;
             mc3d::invariants(sd, v);
-            if (mc3d::yield(v, mp, ft, fs) != mc3d::ELASTIC) {
+            const int mode = mc3d::yield(v, mp, ft, fs);
+            if (mode != mc3d::ELASTIC) {
                 const R eq = pf(pre, PF_EPSQ, P.epsq + i);
-                surr_features<R>(sp.surr, i, s, de, eq, M, nullptr, srot);
+                surr_features<R>(sp.surr, i, s, de, eq, M, nullptr, srot, (float)mode);
+                if (deferred) *deferred = true;
             }
         } else {
             const mc3d::Ret r = mc3d::mohr_coulomb_3d(sd, s0d, ded, mp);
@@ -1187,7 +1194,8 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
 // updated position x, stress s and volume vol for the next scatter.
 template <int D, typename R, bool FUSE, bool MC3, bool USL>
 __device__ __forceinline__ void g2p_core(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp, int64_t i,
-                                         float *pre, double *x, AxisW<R> *w, R *s, R &vol) {
+                                         float *pre, double *x, AxisW<R> *w, R *s, R &vol,
+                                         bool *deferred = nullptr) {
     load_x<D, R>(P, i, x);
     particle_weights<D, R>(x, g, w);
     const int n0 = window_n0<D, R>(g, w);
@@ -1296,7 +1304,7 @@ __device__ __forceinline__ void g2p_core(const PDev<D, R> &P, const GDev<R> &g, 
         cell = (cz * g.ax[0].nc + cx) * g.ax[1].nc + cy;
     }
     if (pre) prefetch_wait();
-    update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol, pre);
+    update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol, pre, nullptr, deferred);
     if (!FUSE && sp.mvl) {
         const R sm = (s[0] + s[1] + s[2]) * R(0.333333);
         atomicAdd(&g.csigm[cell], vol * sm);
@@ -1343,8 +1351,11 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM
     AxisW<R> w[3];
     R s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, v[3] = {0, 0, 0}, m = 0;
     if (live) {
-        g2p_core<D, R, true, MC3, USL>(P, g, sp, i, nullptr, x, w, s, vol);
-        if (!particle_weights<D, R>(x, g, w)) {
+        bool deferred = false;   // (surrogate) return queued: scattered after the accept-or-fallback pass
+        g2p_core<D, R, true, MC3, USL>(P, g, sp, i, nullptr, x, w, s, vol, &deferred);
+        if (deferred) {
+            live = false;
+        } else if (!particle_weights<D, R>(x, g, w)) {
             atomicOr(g.err, ERR_OOG);
             live = false;
         } else {
@@ -1499,7 +1510,8 @@ __global__ void __launch_bounds__(256) k_surr_fix(PDev<3, R> P, GDev<R> g, SurrC
 }
 
 // The deferred restated 3D Mohr-Coulomb returns (mohr_coulomb_3d): keep the
-// network's stress σ̂ when it lies on the yield surface the trial crossed --
+// network's stress σ̂ when it lies on the yield surface the trial crossed (its
+// mode, tensile or shear, is tagged in feature column 15 at deferral) --
 // |f_mode(σ̂)| <= tol·scale and neither yield function above tol·scale, with
 // scale = max(c, |σ̂m|·tanφ, sref) -- else run the plain return from the
 // trial stress (stored as the particle's stress), the rotated pre-increment
@@ -1525,10 +1537,9 @@ __global__ void __launch_bounds__(256) k_surr_fix_mc(PDev<3, R> P, GDev<R> g, Su
             de[q] = (double)c.feat[(size_t)k * 16 + 6 + q];
             sh[q] = (double)out[(size_t)k * 6 + q];
         }
-        mc3d::Inv vt, vh;
-        double ftt, fst, fth, fsh;
-        mc3d::invariants(tr, vt);
-        const int type = mc3d::yield(vt, mp, ftt, fst);
+        mc3d::Inv vh;
+        double fth, fsh;
+        const int type = (int)c.feat[(size_t)k * 16 + 15];   // the trial's mode, tagged at deferral
         mc3d::invariants(sh, vh);
         mc3d::yield(vh, mp, fth, fsh);
         const double scale = fmax(fmax(mp.c, fabs(vh.sm) * mp.tphi), (double)sref);
@@ -1568,6 +1579,26 @@ __global__ void __launch_bounds__(256) k_surr_fix_mc(PDev<3, R> P, GDev<R> g, Su
     if ((threadIdx.x & 31) == 0 && nrows) {
         atomicAdd(&stats[0], (unsigned long long)nrows);
         atomicAdd(&stats[1], (unsigned long long)nfall);
+    }
+}
+
+// P2G_OS! of the particles whose returns the surrogate pass finished (the rows
+// of the deferred list); the fused pass scattered all the others.
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_p2g_list(PDev<D, R> P, GDev<R> g, StepParams sp, const uint32_t *list,
+                                                  const uint32_t *cnt, uint32_t cap) {
+    const uint32_t n = min(*cnt, cap);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int64_t i = list[k];
+        double x[3];
+        load_x<D, R>(P, i, x);
+        AxisW<R> w[3];
+        if (!particle_weights<D, R>(x, g, w)) { atomicOr(g.err, ERR_OOG); continue; }
+        R v[3] = {P.v[0][i], P.v[1][i], D == 3 ? P.v[2][i] : R(0)};
+        R s[6];
+#pragma unroll
+        for (int q = 0; q < PDev<D, R>::NV; ++q) s[q] = P.sig[q][i];
+        p2g_scatter<D, R>(g, w, P.m[i], P.vol[i], v, s, (R)sp.G);
     }
 }
 

@@ -45,9 +45,23 @@ static_assert(ob(3) + 16 == NPAR, "parameter layout");
 // norm: in_mean[16], in_std[16], out_mean[16], out_std[16]
 constexpr int NORM = 64;
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in the tanh form of Hendrycks & Gimpel (2016), "Gaussian Error Linear
+// Units": 0.5 z (1 + tanh(k (z + a z^3))), k = sqrt(2/pi), a = 0.044715, with
+// the hardware tanh (tanh.approx.f32).  Its derivative follows from the same
+// form: 0.5 (1 + t) + 0.5 z (1 - t^2) k (1 + 3 a z^2), t = tanh(k (z + a z^3)).
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float GELU_K = 0.7978845608028654f, GELU_A = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+    const float t = tanh_hw(GELU_K * z * fmaf(GELU_A * z, z, 1.0f));
+    return 0.5f * z * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.3989422804014327f * __expf(-0.5f * z * z);
+    const float t = tanh_hw(GELU_K * z * fmaf(GELU_A * z, z, 1.0f));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * GELU_K * fmaf(3.0f * GELU_A * z, z, 1.0f);
 }
 
 __device__ __forceinline__ void st_bf16(uint8_t *base, uint32_t off, float v) {

@@ -1186,6 +1186,14 @@ inline double dot6(const double *a, const double *b) {
 
 }  // namespace
 
+// the restated 3D Mohr-Coulomb yield functions (tension ft, shear fs) of a stress;
+// returns the state (0 elastic, 1 tensile, 2 shear)
+extern "C" int orc_mc3d_yield(const double *sig, double c, double phi, double st, double *ft, double *fs) {
+    MCInv v;
+    mc_invariants(sig, &v);
+    return mc_yield(v, phi, c, st, ft, fs);
+}
+
 extern "C" void orc_mc3d_point(double *sig, const double *sig0, const double *de, double *epsq,
                                double K, double G, double c, double phi, double psi, double st) {
     const double tol = 1e-1;

@@ -109,6 +109,8 @@ void orc_dp_point(int dim, double *sig, double *epsq, double *epsk,
                   double K, double G, double c, double phi, double psi, double sigt);
 /* Restated 3D Mohr-Coulomb: sig = elastic trial (in/out), sig0 = rotated
  * pre-increment stress, de = strain increment (engineering shear). */
+/* Restated 3D Mohr-Coulomb yield functions of a stress (Voigt); returns 0 elastic, 1 tensile, 2 shear. */
+int orc_mc3d_yield(const double *sig, double c, double phi, double st, double *ft, double *fs);
 void orc_mc3d_point(double *sig, const double *sig0, const double *de, double *epsq,
                     double K, double G, double c, double phi, double psi, double sigt);
 

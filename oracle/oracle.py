@@ -100,6 +100,8 @@ def lib():
         L.orc_ugimp.argtypes = [C.c_double, C.c_double, C.c_double, _dp, _dp]
         L.orc_dp_point.argtypes = [C.c_int, _dp, _dp, _dp] + [C.c_double] * 6
         L.orc_mc3d_point.argtypes = [_dp, _dp, _dp, _dp] + [C.c_double] * 6
+        L.orc_mc3d_yield.argtypes = [_dp, C.c_double, C.c_double, C.c_double, _dp, _dp]
+        L.orc_mc3d_yield.restype = C.c_int
         for name in ("orc_resetgrid", "orc_resetmp"):
             getattr(L, name).argtypes = [C.POINTER(OrcModel)]
         L.orc_p2g.argtypes = [C.POINTER(OrcModel), C.c_double]
@@ -276,3 +278,12 @@ def mc3d_point(sig, sig0, de, epsq, K, G, c, phi, psi, sigt):
     q = C.c_double(epsq)
     lib().orc_mc3d_point(_ptr(s), _ptr(s0), _ptr(d), C.byref(q), K, G, c, phi, psi, sigt)
     return s, q.value
+
+
+def mc3d_yield(sig, c, phi, psi, sigt):
+    """Restated 3D Mohr-Coulomb yield functions (ft, fs) of a Voigt stress."""
+    s = np.array(sig, np.float64)
+    ft, fs = C.c_double(), C.c_double()
+    lib().orc_mc3d_yield(_ptr(s), c, phi, sigt, C.byref(ft), C.byref(fs))
+    return ft.value, fs.value
+

@@ -5,7 +5,6 @@ activations, back-propagated pre-activation gradients)."""
 import math
 
 import numpy as np
-from scipy.special import erf
 
 
 def bf16(x):
@@ -15,12 +14,17 @@ def bf16(x):
     return r.astype(np.float64)
 
 
+GELU_K, GELU_A = math.sqrt(2.0 / math.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / math.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks & Gimpel 2016), as the device kernels use."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_K * (z + GELU_A * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(GELU_K * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_K * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def forward(layers, norm, feat16, emulate_bf16=False):

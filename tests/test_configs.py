@@ -1,0 +1,78 @@
+"""The benchmark configurations against the FP64 oracle on the GPU.
+
+Config 1 (the 2D granular column, 3 200 particles, FP64, 1 s = 20 657 steps)
+runs in full: the all-FP64 device step against the oracle (both OpenMP-
+threaded, so both sum their nodal contributions in varying order; the
+oracle's own sequential run differs from its threaded one by 1.7e-12 in
+displacement), and the mixed mode, whose displacement error the flow itself
+bounds: a perturbation of 1e-9 cell of the initial positions moves the FP64
+oracle's final displacement field by 2.3e-3, so FP32 rounding anywhere in the
+state gives ~2e-3 while the run-out stays within ~1e-5.  Config 2 (the 3D
+column, 2 560 000 particles) runs a 20-step prefix against the oracle in both
+modes.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import fresh_particles, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def runout(x0, x):
+    return float(x[:, 0].max() - x0[:, 0].max())
+
+
+def device_run(pkg, case, nsteps):
+    dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
+    dev.step(case.dt, 0.0, nsteps)
+    out = fresh_particles(pkg, case.mp)
+    dev.download(pkg._lib.F_REFERENCE, out)
+    dev.close()
+    return out
+
+
+def oracle_run(orc, case, nsteps):
+    o = orc.Oracle(case.args, case.grid, case.mp, case.attr, case.bc, nthreads=len(os.sched_getaffinity(0)))
+    o.run(case.dt, 0.0, nsteps)
+    return o
+
+
+@pytest.fixture(scope="module")
+def config1(pkg, orc, gpu_lib):
+    case = pkg.workloads.column_collapse_2d()
+    assert case.mp.np == 3200 and case.nsteps_full == 20657
+    return case, oracle_run(orc, case, case.nsteps_full)
+
+
+def test_config1_full_run_fp64(pkg, config1):
+    case, o = config1
+    out = device_run(pkg, pkg.workloads.column_collapse_2d(gpu_precision="fp64"), case.nsteps_full)
+    x0 = case.mp.xi
+    assert rel(out.xi - x0, o.xi - x0) < 1e-9
+    assert rel(out.sig, o.sig) < 1e-7
+    assert abs(runout(x0, out.xi) - runout(x0, o.xi)) < 1e-9
+
+
+def test_config1_full_run_mixed(pkg, config1):
+    case, o = config1
+    out = device_run(pkg, pkg.workloads.column_collapse_2d(gpu_precision="mixed"), case.nsteps_full)
+    x0, h = case.mp.xi, case.meta["h"]
+    ro = runout(x0, o.xi)
+    assert abs(runout(x0, out.xi) - ro) <= 1e-4 * max(abs(ro), h)
+    assert rel(out.xi - x0, o.xi - x0) < 1e-2
+
+
+@pytest.mark.parametrize("prec,tol,tol_s", [("fp64", 1e-9, 1e-9), ("mixed", 1e-5, 1e-4)])
+def test_config2_prefix(pkg, orc, gpu_lib, prec, tol, tol_s):
+    case = pkg.workloads.column_collapse_3d(gpu_precision=prec)
+    assert case.mp.np == 2_560_000
+    nsteps = 20
+    out = device_run(pkg, case, nsteps)
+    o = oracle_run(orc, pkg.workloads.column_collapse_3d(), nsteps)
+    x0 = case.mp.xi
+    assert rel(out.xi - x0, o.xi - x0) < tol
+    assert rel(out.vs, o.vs) < tol
+    assert rel(out.sig, o.sig) < tol_s

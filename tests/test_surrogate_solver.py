@@ -84,3 +84,90 @@ def test_trained_surrogate_gains(pkg, samples):
     assert rel(os_.xi - cs.mp.xi, op.xi - cp.mp.xi) < 1e-2
     h = c.meta["h"]
     assert abs(runout(cs, os_) - runout(cp, op)) <= 1e-3 * max(abs(runout(cp, op)), h)
+
+
+# ---- the restated 3D Mohr-Coulomb return (desc.mc3d = restated) ----------------
+
+def mc_column(pkg):
+    """A cohesive Mohr-Coulomb column (c = 1 kPa, σt = 300 Pa: away from the
+    restated return's apex singularity of c = σt = 0), most of it yielding."""
+    return pkg.workloads.column_collapse_3d(h=0.02, column=(0.2, 0.1, 0.16), domain=(0.4, 0.16, 0.24), seed=41,
+                                            mc3d="restated", c=1000.0, sigt=300.0, gpu_precision="mixed")
+
+
+def run_mc(pkg, sur=None, tol=1e-3, nsteps=120):
+    c = mc_column(pkg)
+    d = pkg.DeviceModel(c.args, c.grid, c.mp, c.attr, c.bc)
+    Ti = d.step(c.dt, 0.0, 60)
+    if sur is not None:
+        d.set_surrogate(sur, tol=tol, sref=1e3)
+    d.step(c.dt, Ti, nsteps)
+    out = fresh_particles(pkg, c.mp)
+    d.download(pkg._lib.F_REFERENCE, out)
+    st = d.stats()
+    d.close()
+    return c, out, st
+
+
+@pytest.fixture(scope="module")
+def mc_samples(pkg, gpu_lib):
+    c = mc_column(pkg)
+    d = pkg.DeviceModel(c.args, c.grid, c.mp, c.attr, c.bc)
+    Ti = d.step(c.dt, 0.0, 60)
+    feat, tgt, _ = pkg.surrogate.collect_samples(d, c.dt, Ti, 120, 2_000_000, every=1)
+    d.close()
+    return c, feat, tgt
+
+
+def test_mc_samples_lie_on_the_surface(pkg, orc, mc_samples):
+    """Logged Mohr-Coulomb samples: trial stresses outside the yield surface,
+    returned stresses inside it within the return's tolerance (0.1 Pa)."""
+    c, feat, tgt = mc_samples
+    assert feat.shape[0] > 10_000
+    f, y = feat.cpu().numpy().astype(np.float64), tgt.cpu().numpy().astype(np.float64)
+    K, G = c.meta["K"], c.meta["G"]
+    rng = np.random.default_rng(1)
+    for i in rng.choice(len(f), 100, replace=False):
+        ft, fs = orc.mc3d_yield(f[i, :6], f[i, 13], f[i, 14], 0.0, 300.0)
+        assert max(ft, fs) > 0.0
+        ft, fs = orc.mc3d_yield(y[i], f[i, 13], f[i, 14], 0.0, 300.0)
+        assert max(ft, fs) < 0.1 + 1e-4 * np.abs(y[i]).max()
+
+
+def test_mc_zero_tolerance_is_the_plain_step(pkg, mc_samples):
+    """With an acceptance tolerance of zero every deferred Mohr-Coulomb return
+    falls back to the plain return, from the same trial stress, pre-increment
+    stress and strain increment: the run equals the plain one up to the
+    summation order of the nodal sums (the deferred particles scatter in a
+    pass of their own), which the restated return's discontinuity at the
+    yield surface (its first corrector switches on |f| < 0.1 Pa of the
+    pre-increment stress) carries into the displacements at the level of two
+    plain runs' own difference."""
+    c, feat, tgt = mc_samples
+    sur = pkg.surrogate.Surrogate(seed=2)
+    sur.set_norm(feat, tgt)
+    cp, op, _ = run_mc(pkg)
+    cq, oq, _ = run_mc(pkg)
+    cs, os_, st = run_mc(pkg, sur, tol=1e-30)
+    assert st.surr_rows > 0 and st.surr_fallbacks >= st.surr_rows - 3
+    spread = rel(oq.xi - cq.mp.xi, op.xi - cp.mp.xi)
+    err = rel(os_.xi - cs.mp.xi, op.xi - cp.mp.xi)
+    assert err < max(20.0 * spread, 1e-5) and err < 1e-3, (err, spread)
+
+
+def test_mc_trained_surrogate(pkg, mc_samples):
+    """A network trained on the logged Mohr-Coulomb returns takes a share of
+    them and keeps the run-out within 1e-3 (of a cell) of the plain step; the
+    accepted fraction is reported."""
+    c, feat, tgt = mc_samples
+    sur = pkg.surrogate.Surrogate(seed=1)
+    sur.set_norm(feat, tgt)
+    losses = sur.train(feat, tgt, epochs=60, batch=4096, lr=3e-3, lr_end=5e-5)
+    assert losses[-1] < 0.3 * losses[0]
+    cp, op, _ = run_mc(pkg)
+    cs, os_, st = run_mc(pkg, sur)
+    acc = 1.0 - st.surr_fallbacks / st.surr_rows
+    print(f"Mohr-Coulomb surrogate: {st.surr_rows} rows, accepted {acc:.3f}")
+    assert acc > 0.1
+    h = c.meta["h"]
+    assert abs(runout(cs, os_) - runout(cp, op)) <= 1e-3 * max(abs(runout(cp, op)), h)
