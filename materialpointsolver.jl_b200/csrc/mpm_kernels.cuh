@@ -1082,27 +1082,32 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
         for (int k = 0; k < 6; ++k) stcs(P.eps[k] + i, pf(pre, PF_EPS + k, P.eps[k] + i) + de[k]);
     }
     stcs(P.epsv + i, ev);
-    // F <- (I + ΔF) F; J = det F in FP64; Ω = J Ω0
+    // F <- (I + ΔF) F, formed as F + ΔF·F; J = det F in FP64; Ω = J Ω0.
+    // In FP32, (1 + ΔF_ii) would keep ΔF_ii (≈1e-5 per step) only to the
+    // absolute 6e-8 of 1's half-ulp -- a relative error up to ~1e-2 that repeats
+    // with the same sign while a column settles under gravity and biases J,
+    // hence the volumes and the nodal forces.  F + ΔF·F rounds once, at F's
+    // own half-ulp, where the rounding changes sign from step to step.
     R f[9], fn[9];
 #pragma unroll
     for (int k = 0; k < NF; ++k) f[k] = pf(pre, PF_F + k, P.F[k] + i);
     double J;
     if (D == 2) {
-        fn[0] = (dF[0] + R(1)) * f[0] + dF[1] * f[2];
-        fn[1] = (dF[0] + R(1)) * f[1] + dF[1] * f[3];
-        fn[2] = (dF[3] + R(1)) * f[2] + dF[2] * f[0];
-        fn[3] = (dF[3] + R(1)) * f[3] + dF[2] * f[1];
+        fn[0] = f[0] + (dF[0] * f[0] + dF[1] * f[2]);
+        fn[1] = f[1] + (dF[0] * f[1] + dF[1] * f[3]);
+        fn[2] = f[2] + (dF[3] * f[2] + dF[2] * f[0]);
+        fn[3] = f[3] + (dF[3] * f[3] + dF[2] * f[1]);
         J = (double)fn[0] * (double)fn[3] - (double)fn[1] * (double)fn[2];
     } else {
-        fn[0] = (dF[0] + R(1)) * f[0] + dF[1] * f[3] + dF[2] * f[6];
-        fn[1] = (dF[0] + R(1)) * f[1] + dF[1] * f[4] + dF[2] * f[7];
-        fn[2] = (dF[0] + R(1)) * f[2] + dF[1] * f[5] + dF[2] * f[8];
-        fn[3] = (dF[4] + R(1)) * f[3] + dF[3] * f[0] + dF[5] * f[6];
-        fn[4] = (dF[4] + R(1)) * f[4] + dF[3] * f[1] + dF[5] * f[7];
-        fn[5] = (dF[4] + R(1)) * f[5] + dF[3] * f[2] + dF[5] * f[8];
-        fn[6] = (dF[8] + R(1)) * f[6] + dF[7] * f[3] + dF[6] * f[0];
-        fn[7] = (dF[8] + R(1)) * f[7] + dF[7] * f[4] + dF[6] * f[1];
-        fn[8] = (dF[8] + R(1)) * f[8] + dF[7] * f[5] + dF[6] * f[2];
+        fn[0] = f[0] + (dF[0] * f[0] + dF[1] * f[3] + dF[2] * f[6]);
+        fn[1] = f[1] + (dF[0] * f[1] + dF[1] * f[4] + dF[2] * f[7]);
+        fn[2] = f[2] + (dF[0] * f[2] + dF[1] * f[5] + dF[2] * f[8]);
+        fn[3] = f[3] + (dF[4] * f[3] + dF[3] * f[0] + dF[5] * f[6]);
+        fn[4] = f[4] + (dF[4] * f[4] + dF[3] * f[1] + dF[5] * f[7]);
+        fn[5] = f[5] + (dF[4] * f[5] + dF[3] * f[2] + dF[5] * f[8]);
+        fn[6] = f[6] + (dF[8] * f[6] + dF[7] * f[3] + dF[6] * f[0]);
+        fn[7] = f[7] + (dF[8] * f[7] + dF[7] * f[4] + dF[6] * f[1]);
+        fn[8] = f[8] + (dF[8] * f[8] + dF[7] * f[5] + dF[6] * f[2]);
         double g0 = fn[0], g1 = fn[1], g2 = fn[2], g3 = fn[3], g4 = fn[4], g5 = fn[5], g6 = fn[6],
                g7 = fn[7], g8 = fn[8];
         J = g0 * g4 * g8 + g1 * g5 * g6 + g2 * g3 * g7 - g6 * g4 * g2 - g7 * g5 * g0 - g8 * g3 * g1;
@@ -1516,7 +1521,8 @@ __global__ void __launch_bounds__(256) k_surr_fix(PDev<3, R> P, GDev<R> g, SurrC
 // scale = max(c, |σ̂m|·tanφ, sref) -- else run the plain return from the
 // trial stress (stored as the particle's stress), the rotated pre-increment
 // stress (kept in the row's target slot) and the strain increment (features
-// 6..11).  An accepted row's ϵq grows by √(2/3)·|e|, e = dev(σtrial - σ̂)/(2G),
+// 6..11); the acceptance test evaluates the yield functions in FP32.  An
+// accepted row's ϵq grows by √(2/3)·|e|, e = dev(σtrial - σ̂)/(2G),
 // the plastic shear strain of the correction (ϵq does not enter the restated
 // return: it has no softening).
 template <typename R>
@@ -1529,23 +1535,22 @@ __global__ void __launch_bounds__(256) k_surr_fix_mc(PDev<3, R> P, GDev<R> g, Su
         Mat<R> M = g.mat[P.mat[i]];
         if (P.coh) M.c = P.coh[i];
         const mc3d::Par mp = mc3d_par<R>(M);
-        double tr[6], s0[6], de[6], sh[6];
+        double tr[6], sh[6];
+        float shf[6];
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
             tr[q] = (double)P.sig[q][i];
-            s0[q] = (double)c.tgt[(size_t)k * 6 + q];
-            de[q] = (double)c.feat[(size_t)k * 16 + 6 + q];
-            sh[q] = (double)out[(size_t)k * 6 + q];
+            shf[q] = out[(size_t)k * 6 + q];
+            sh[q] = (double)shf[q];
         }
-        mc3d::Inv vh;
-        double fth, fsh;
+        // the acceptance test in FP32 (the plain return stays FP64)
+        float fth, fsh, smh;
+        mc3d::yield_f32(shf, mp, fth, fsh, smh);
         const int type = (int)c.feat[(size_t)k * 16 + 15];   // the trial's mode, tagged at deferral
-        mc3d::invariants(sh, vh);
-        mc3d::yield(vh, mp, fth, fsh);
-        const double scale = fmax(fmax(mp.c, fabs(vh.sm) * mp.tphi), (double)sref);
-        const double fact = type == mc3d::TENSILE ? fth : fsh;
-        const bool ok = isfinite(fact) && isfinite(fsh) && isfinite(fth) && fabs(fact) <= tol * scale &&
-                        fmax(fth, fsh) <= tol * scale;
+        const float scale = fmaxf(fmaxf((float)mp.c, fabsf(smh) * (float)mp.tphi), sref);
+        const float fact = type == mc3d::TENSILE ? fth : fsh;
+        const bool ok = isfinite(fact) && isfinite(fsh) && isfinite(fth) && fabsf(fact) <= tol * scale &&
+                        fmaxf(fth, fsh) <= tol * scale;
         double dq;
         if (ok) {
             const double ds = ((tr[0] - sh[0]) + (tr[1] - sh[1]) + (tr[2] - sh[2])) / 3.0;
@@ -1562,6 +1567,12 @@ __global__ void __launch_bounds__(256) k_surr_fix_mc(PDev<3, R> P, GDev<R> g, Su
             }
             dq = sqrt(2.0 / 3.0 * ee);
         } else {
+            double s0[6], de[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                s0[q] = (double)c.tgt[(size_t)k * 6 + q];
+                de[q] = (double)c.feat[(size_t)k * 16 + 6 + q];
+            }
             const mc3d::Ret r = mc3d::mohr_coulomb_3d(tr, s0, de, mp);
             dq = r.dq;
         }

@@ -75,6 +75,27 @@ __host__ __device__ __forceinline__ int yield(const Inv &v, const Par &p, double
     return ELASTIC;
 }
 
+// The two yield functions in FP32, for cheap acceptance tests of a stress
+// that should lie on the surface (the surrogate's predictions): the same
+// invariants and functions as invariants() and yield() above.
+__device__ __forceinline__ void yield_f32(const float *s, const Par &p, float &ft, float &fs, float &sm_out) {
+    const float sm = (s[0] + s[1] + s[2]) * (1.0f / 3.0f);
+    const float d0 = s[0] - sm, d1 = s[1] - sm, d2 = s[2] - sm;
+    const float j2 = (d0 * d0 + d1 * d1 + d2 * d2) * 0.5f + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
+    const float j3 = d0 * d1 * d2 + 2.0f * s[3] * s[4] * s[5] - d0 * s[4] * s[4] - d1 * s[5] * s[5] -
+                     d2 * s[3] * s[3];
+    float lode = j2 > 1e-30f ? 2.598076211f * (j3 / (j2 * sqrtf(j2))) : 0.0f;
+    lode = fminf(1.0f, fmaxf(-1.0f, lode));
+    const float theta = acosf(lode) * (1.0f / 3.0f);
+    const float rho = sqrtf(2.0f * j2), eps = 1.732050808f * sm;
+    const float cphi = (float)p.cphi, tphi = (float)p.tphi;
+    ft = 0.8164965809f * cosf(theta) * rho + eps * 0.5773502692f - (float)p.st;
+    fs = 1.224744871f * rho *
+             (sinf(theta + 1.047197551f) / (1.732050808f * cphi) + cosf(theta + 1.047197551f) * tphi * (1.0f / 3.0f)) +
+         eps * 0.5773502692f * tphi - (float)p.c;
+    sm_out = sm;
+}
+
 // df/dsigma, dg/dsigma (Voigt, engineering shear) and dg/dq for the given mode.
 __host__ __device__ __forceinline__ void gradients(int type, const Inv &v, const Par &p, double *df, double *dg,
                                           double &dg_dq) {

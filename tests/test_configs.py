@@ -9,7 +9,12 @@ bounds: a perturbation of 1e-9 cell of the initial positions moves the FP64
 oracle's final displacement field by 2.3e-3, so FP32 rounding anywhere in the
 state gives ~2e-3 while the run-out stays within ~1e-5.  Config 2 (the 3D
 column, 2 560 000 particles) runs a 20-step prefix against the oracle in both
-modes.
+modes; its flow is well conditioned, and over the whole second the mixed mode
+stays within ~1e-6 of the all-FP64 device mode (checked here on the same
+column at h = 0.02 m and on a 2D elastic column): the deformation gradient is
+advanced as F + ΔF·F, since FP32's (1 + ΔF)·F drops the low bits of the
+per-step increment with the same sign every step and biased the displacement
+by ~1e-3.
 """
 import os
 
@@ -65,7 +70,7 @@ def test_config1_full_run_mixed(pkg, config1):
     assert rel(out.xi - x0, o.xi - x0) < 1e-2
 
 
-@pytest.mark.parametrize("prec,tol,tol_s", [("fp64", 1e-9, 1e-9), ("mixed", 1e-5, 1e-4)])
+@pytest.mark.parametrize("prec,tol,tol_s", [("fp64", 1e-9, 1e-9), ("mixed", 1e-5, 1e-5)])
 def test_config2_prefix(pkg, orc, gpu_lib, prec, tol, tol_s):
     case = pkg.workloads.column_collapse_3d(gpu_precision=prec)
     assert case.mp.np == 2_560_000
@@ -76,3 +81,21 @@ def test_config2_prefix(pkg, orc, gpu_lib, prec, tol, tol_s):
     assert rel(out.xi - x0, o.xi - x0) < tol
     assert rel(out.vs, o.vs) < tol
     assert rel(out.sig, o.sig) < tol_s
+
+
+@pytest.mark.parametrize("name", ["column3d_h0.02", "column2d_elastic"])
+def test_mixed_tracks_fp64_over_the_full_second(pkg, gpu_lib, name):
+    def make(prec):
+        if name == "column2d_elastic":
+            return pkg.workloads.column_collapse_2d(h=0.005, width=0.5, height=0.4, domain=(1.2, 0.6),
+                                                    constitutive="linearelastic", E=1e6, nu=0.3, rho=2650.0,
+                                                    seed=7, gpu_precision=prec)
+        return pkg.workloads.column_collapse_3d(h=0.02, gpu_precision=prec)
+    c64 = make("fp64")
+    n = c64.nsteps_full
+    x0 = c64.mp.xi.copy()
+    ref = device_run(pkg, c64, n)
+    mix = device_run(pkg, make("mixed"), n)
+    # measured 2.8e-6 (3D) and 3.8e-6 (2D); (1 + ΔF)·F in FP32 gave 5.8e-4 and 1.1e-3
+    assert rel(mix.xi - x0, ref.xi - x0) < 2e-5
+    assert abs(runout(x0, mix.xi) - runout(x0, ref.xi)) <= 1e-5 * max(abs(runout(x0, ref.xi)), c64.meta["h"])
