@@ -75,8 +75,11 @@ template <typename R> struct AxisC {
 };
 
 // 1-D uGIMP weight and derivative.  FP64 mode evaluates the CPU (division)
-// form of uGIMPbasis; FP32 mode the reciprocal form of uGIMPbasisx/y/z, with
-// |Δ|/h also taken as |Δ|·(1/h).
+// form of uGIMPbasis piece by piece; FP32 mode the same function (the
+// reciprocal form of uGIMPbasisx/y/z, |Δ|/h taken as |Δ|·(1/h)) written
+// without branches, so the lanes of a warp whose particles fall in different
+// pieces do not diverge (9 evaluations per window, two windows per particle in
+// the fused pass).
 template <typename R> __device__ __forceinline__ void ugimp1(R d, const AxisC<R> &c, R &N, R &dN) {
     R a = fabs(d);
     N = R(0); dN = R(0);
@@ -94,17 +97,14 @@ template <typename R> __device__ __forceinline__ void ugimp1(R d, const AxisC<R>
             dN = -sgn(d) * (t / (h * lp));
         }
     } else {
-        if (a < c.half_lp) {
-            N = R(1) - ((R(4) * d * d + c.lp * c.lp) * c.inv4hl);
-            dN = -R(8) * d * c.inv4hl;
-        } else if (a < c.h_m_hl) {
-            N = R(1) - a * c.invh;
-            dN = sgn(d) * -c.invh;
-        } else if (a < c.h_p_hl) {
-            R t = c.h_p_hl - a;
-            N = t * t * R(0.5) * c.invhl;
-            dN = -sgn(d) * t * c.invhl;
-        }
+        // branch-free: the hat 1 - a/h with its kinks at 0 and at h smoothed over
+        // the particle length lp (the three pieces of uGIMPbasisx/y/z in one
+        // expression: -u0²/(h·lp) for a < lp/2, +u1²/(2h·lp) for a > h - lp/2)
+        const R u0 = fmax(c.half_lp - a, R(0)), u1 = fmax(a - c.h_m_hl, R(0));
+        const R in = a < c.h_p_hl ? R(1) : R(0);
+        N = in * (R(1) - a * c.invh - u0 * u0 * c.invhl + R(0.5) * u1 * u1 * c.invhl);
+        const R da = -c.invh + (R(2) * u0 + u1) * c.invhl;   // dN/d|Δ|
+        dN = in * (d < R(0) ? -da : da);
     }
 }
 

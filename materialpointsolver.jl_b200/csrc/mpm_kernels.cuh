@@ -273,8 +273,41 @@ __device__ __forceinline__ void particle_cell(const double *xp, const GDev<R> &g
 
 // Weights of the 3^D window of a particle.  Returns false if the particle is
 // out of the grid (its contributions are then dropped and the flag raised).
+//
+// FP32 mode takes a short cut for windows inside the grid: the window corner
+// is node ci - 1 below the cell centre and ci above it (axis_weights), i.e.
+// node floor(t - 1/2) with t = (ξ - x1)/h, whichever of Julia's fld / cld the
+// cell index uses (they differ only at t integral, where both give that node);
+// the distances to the three nodes are then s - k·h with s = ξ - x_corner.  At
+// t - 1/2 integral (a particle exactly at a cell centre) the two candidate
+// windows differ only by a node of weight 0.  Windows that touch the grid's
+// last node layer, and non-finite positions, take the general path below.
 template <int D, typename R>
 __device__ __forceinline__ bool particle_weights(const double *xp, const GDev<R> &g, AxisW<R> *w) {
+    if constexpr (sizeof(R) == 4) {
+        bool inner = true;
+        double sd[3];
+        int bs[3];
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            const double t = (xp[a] - g.ax[a].x1) * g.ax[a].inv_h - 0.5;
+            const double f = floor(t);
+            inner = inner && f >= 0.0 && f + 2.0 < (double)g.ax[a].nn;   // false for NaN
+            bs[a] = inner ? (int)f : 0;
+            sd[a] = xp[a] - (g.ax[a].x1 + (double)bs[a] * g.ax[a].h);
+        }
+        if (inner) {
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                const float sf = (float)sd[a];
+                w[a].base = bs[a];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) ugimp1<R>(sf - (float)k * g.ax[a].hr, g.ax[a], w[a].N[k], w[a].dN[k]);
+            }
+            if (D == 2) w[2].base = 0;
+            return true;
+        }
+    }
     int ci[3];
     particle_cell<D, R>(xp, g, ci);
     bool bad = false;
@@ -1159,7 +1192,10 @@ __device__ __forceinline__ void update_particle(const PDev<D, R> &P, const GDev<
 #pragma unroll
         for (int k = 0; k < 6; ++k) { sd[k] = s[k]; s0d[k] = srot[k]; ded[k] = de[k]; }
         const mc3d::Par mp = mc3d_par<R>(M);
-        if (sp.surr.mode == 2) {
+        if (mc3d::surely_elastic(sd, mp)) {
+            // elastic by a margin above the FP32 screen's error: the FP64
+            // classification would say ELASTIC, the stress stays the trial one
+        } else if (sp.surr.mode == 2) {
             // surrogate: a yielding trial keeps its trial stress and is queued
             // (features, and the rotated pre-increment stress the fallback needs)
             mc3d::Inv v;

@@ -96,6 +96,25 @@ __device__ __forceinline__ void yield_f32(const float *s, const Par &p, float &f
     sm_out = sm;
 }
 
+// FP32 screen of the classification, for skipping the FP64 invariants of
+// clearly elastic stresses: true only when both yield functions, evaluated in
+// FP32, lie below -0.02·(Σ|σ| + c + |σt|).  The FP32 evaluation errs by well
+// under that: the invariants to a few ulp of the stress scale, and θ =
+// acos(lode)/3 enters only through cos θ, sin(θ + π/3) and cos(θ + π/3), which
+// are Hölder-1/2 in lode at lode = -1, so a lode error δ (≲ 1e-6·Σ|σ|/ρ) moves
+// the ρ terms by ≲ ρ·sqrt(δ) ≤ 1.1e-3·Σ|σ|, times at most ~2.5 for the friction
+// factors.  A screened stress is therefore ELASTIC in FP64 as well.  NaN or
+// overflow fails the screen (the comparisons are false).
+__device__ __forceinline__ bool surely_elastic(const double *s, const Par &p) {
+    float sf[6], sa = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { sf[k] = (float)s[k]; sa += fabsf(sf[k]); }
+    float ft, fs, sm;
+    yield_f32(sf, p, ft, fs, sm);
+    const float m = -0.02f * (sa + (float)p.c + fabsf((float)p.st));
+    return ft < m && fs < m;
+}
+
 // df/dsigma, dg/dsigma (Voigt, engineering shear) and dg/dq for the given mode.
 __host__ __device__ __forceinline__ void gradients(int type, const Inv &v, const Par &p, double *df, double *dg,
                                           double &dg_dq) {
