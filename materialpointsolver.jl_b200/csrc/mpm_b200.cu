@@ -716,6 +716,15 @@ template <int D> void box_launch(mpm_handle *h, int which, const PDev<D, float> 
 }
 
 // The launches of one step (solve, double mapping, DM3, fused G2P + next P2G).
+// the lane-merged double mapping, specialised for va = :a without the separate
+// grid velocity (its gathers then read one half-record per node, no switches)
+template <int D, typename R>
+void launch_dmap_chain(mpm_handle *h, const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp) {
+    const int64_t np = sp.np;
+    if (sp.va == MPM_VA_A && !sp.need_vs) k_dmap_chain<D, R, false><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+    else k_dmap_chain<D, R, true><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+}
+
 template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double dt, double Ti, double Tn) {
     const int64_t np = h->d.np;
     const int nblk = h->nbx * h->nby * h->nbz;
@@ -788,7 +797,7 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         // (the scatters of chained lanes merged, as in the default passes)
         const bool chain = h->chain;
         L.run("dmap", [&] {
-            if (chain) k_dmap_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (chain) launch_dmap_chain<D, R>(h, P, g, sp);
             else k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
         });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
@@ -806,7 +815,7 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
     } else if (sp.surr.mode == 2 && sp.plastic && np) {
         // surrogate: G2P + update with the yielding particles' returns deferred,
         // the MLP over the deferred rows, accept-or-fallback, then the scatter
-        L.run("dmap", [&] { k_dmap_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp); });
+        L.run("dmap", [&] { launch_dmap_chain<D, R>(h, P, g, sp); });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         CK(cudaMemsetAsync(h->surr_cnt, 0, 4, h->stream));
@@ -843,7 +852,7 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
     } else {
         const bool chain = h->chain;
         if (np) L.run("dmap", [&] {
-            if (chain) k_dmap_chain<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (chain) launch_dmap_chain<D, R>(h, P, g, sp);
             else k_dmap<D, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
         });
         L.run("dm3", [&] { k_dm3<D, R><<<ngrid, Blk<D>::NT, 0, h->stream>>>(g, sp); });

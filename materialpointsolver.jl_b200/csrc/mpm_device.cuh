@@ -31,9 +31,21 @@ __device__ __forceinline__ void red_add4(float4 *a, float x, float y, float z, f
     asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};"
                  :: "l"(a), "f"(x), "f"(y), "f"(z), "f"(w) : "memory");
 }
+// The same reduction issued under a predicate instead of a branch: lanes whose
+// contribution is zero (or that do not own the node) skip it without a
+// divergent branch and its reconvergence point.  The address must be formed
+// (it is not dereferenced when p is false).
+__device__ __forceinline__ void red_add4_if(bool p, float4 *a, float x, float y, float z, float w) {
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %5, 0;\n\t"
+                 "@q red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n\t}"
+                 :: "l"(a), "f"(x), "f"(y), "f"(z), "f"(w), "r"((unsigned)p) : "memory");
+}
 __device__ __forceinline__ void red_add4(dvec4 *a, double x, double y, double z, double w) {
     atomicAdd(&a->x, x); atomicAdd(&a->y, y); atomicAdd(&a->z, z);
     if (w != 0.0) atomicAdd(&a->w, w);
+}
+__device__ __forceinline__ void red_add4_if(bool p, dvec4 *a, double x, double y, double z, double w) {
+    if (p) red_add4(a, x, y, z, w);
 }
 
 // ---------------------------------------------------------------------------

@@ -602,20 +602,18 @@ __device__ __forceinline__ void dm2_scatter_chain(const GDev<R> &g, const AxisW<
             const R a1 = ch.c1 ? u1 : R(0.0), a2 = ch.c2 ? u2 : R(0.0), b2 = ch.c1 ? v2 : R(0.0);
 #pragma unroll
             for (int k = 0; k < 3; ++k) r0[a][k] = N0 * p[k] + a1 * p1[k] + a2 * p2[k];
-            if (ch.end) {
-                Node8<R> *col = g.acc + (n0 + a * g.nny + c * plane);
-                if (N1 + b2 != R(0.0))
-                    red_add4(&col[1].a, R(0.0), N1 * p[0] + b2 * p1[0], N1 * p[1] + b2 * p1[1], N1 * p[2] + b2 * p1[2]);
-                if (N2 != R(0.0)) red_add4(&col[2].a, R(0.0), N2 * p[0], N2 * p[1], N2 * p[2]);
-            }
+            // rows 1 and 2 by the chain's last lane (predicated, not branched)
+            Node8<R> *col = g.acc + (n0 + a * g.nny + c * plane);
+            red_add4_if(ch.end && N1 + b2 != R(0.0), &col[1].a, R(0.0), N1 * p[0] + b2 * p1[0],
+                        N1 * p[1] + b2 * p1[1], N1 * p[2] + b2 * p1[2]);
+            red_add4_if(ch.end && N2 != R(0.0), &col[2].a, R(0.0), N2 * p[0], N2 * p[1], N2 * p[2]);
         }
         bool emit[3];
         xmerge_row0<R, 3>(ch, r0, emit);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            if (!emit[a] || (r0[a][0] == R(0.0) && r0[a][1] == R(0.0) && r0[a][2] == R(0.0))) continue;
-            red_add4(&g.acc[n0 + a * g.nny + c * plane].a, R(0.0), r0[a][0], r0[a][1], r0[a][2]);
-        }
+        for (int a = 0; a < 3; ++a)
+            red_add4_if(emit[a] && (r0[a][0] != R(0.0) || r0[a][1] != R(0.0) || r0[a][2] != R(0.0)),
+                        &g.acc[n0 + a * g.nny + c * plane].a, R(0.0), r0[a][0], r0[a][1], r0[a][2]);
     }
 }
 
@@ -822,7 +820,9 @@ __device__ __forceinline__ void p2g_scatter_chain(const GDev<R> &g, const AxisW<
 // ---------------------------------------------------------------------------
 // doublemapping1 of one particle: gathers, new velocity (stored), momentum p
 // for the re-scatter; w receives the particle's window.
-template <int D, typename R>
+// GEN = false: the va = :a scheme without the separate grid velocity (the
+// common case), with the two run-time gather switches folded away.
+template <int D, typename R, bool GEN = true>
 __device__ __forceinline__ void dmap_core(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp, int64_t i,
                                           AxisW<R> *w, R *p) {
     using T4 = typename Vec<R>::T4;
@@ -837,7 +837,7 @@ __device__ __forceinline__ void dmap_core(const PDev<D, R> &P, const GDev<R> &g,
     const int plane = g.nnx * g.nny;
     R tT[3] = {0, 0, 0}, ta[3] = {0, 0, 0}, tv[3] = {0, 0, 0};
     constexpr int NC = D == 3 ? 3 : 1;
-    const bool va_v = sp.va != 0, need_vs = sp.need_vs != 0;
+    const bool va_v = GEN && sp.va != 0, need_vs = GEN && sp.need_vs != 0;
     // ΣN·q = Σ_(x,z) Nx·Nz·(Σ_y Ny·q): inner sums along the contiguous y run
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
@@ -921,7 +921,7 @@ __global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<
 }
 
 // The same pass with the re-scatter of chained lanes merged (FP32 and FP64).
-template <int D, typename R = float>
+template <int D, typename R = float, bool GEN = true>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM_DMAP_CHAIN_MINB) k_dmap_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < sp.np;
@@ -929,7 +929,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM
     R p[3] = {0, 0, 0};
     int n0 = 0, key = dead_key();
     if (live) {
-        dmap_core<D, R>(P, g, sp, i, w, p);
+        dmap_core<D, R, GEN>(P, g, sp, i, w, p);
         n0 = key = window_n0<D, R>(g, w);
     } else {
 #pragma unroll
