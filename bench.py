@@ -475,7 +475,7 @@ def run_b200(args):
                      "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
                      "step_achieved": step_achieved, "step_frac": step_achieved / peak},
         "e2e": {"value": npart * K / e2e_t, "unit": "particle-updates/s",
-                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K, "steps": K,
                 "what": "DeviceModel upload from pinned host arrays + K steps + device2host! field set"},
         "clocks": clk.summary(),
     }

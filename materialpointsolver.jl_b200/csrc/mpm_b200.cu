@@ -784,8 +784,8 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         } else {
             L.run("g2p_p2g", [&] {
                 if (h->chain) {
-                    if (mc3) k_g2p_chain<D, D == 3, true, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                    else k_g2p_chain<D, false, true, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                    if (mc3) k_g2p_chain<D, D == 3, true, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+                    else k_g2p_chain<D, false, true, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
                     return;
                 }
                 if (mc3) k_g2p<D, R, true, D == 3, true><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
@@ -821,8 +821,8 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         CK(cudaMemsetAsync(h->surr_cnt, 0, 4, h->stream));
         // the fused pass: particles whose return is deferred skip its scatter
         L.run("g2p_p2g", [&] {
-            if (mc3) k_g2p_chain<D, D == 3, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-            else k_g2p_chain<D, false, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+            if (mc3) k_g2p_chain<D, D == 3, false, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+            else k_g2p_chain<D, false, false, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
         });
         L.run("mlp", [&] {
             CK(mpm_detail::mlp_forward_dev(h->surr_params, h->surr_norm, h->surr_feat, h->surr_out, np, h->surr_cnt,
@@ -859,8 +859,8 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         if (np) L.run("g2p_p2g", [&] {
             if (chain) {
-                if (mc3) k_g2p_chain<D, D == 3, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                else k_g2p_chain<D, false, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                if (mc3) k_g2p_chain<D, D == 3, false, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+                else k_g2p_chain<D, false, false, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
                 return;
             }
             if (mc3) k_g2p<D, R, true, D == 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);

@@ -1391,9 +1391,17 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM
     double x[3];
     AxisW<R> w[3];
     R s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, v[3] = {0, 0, 0}, m = 0;
+    // FP32: the particle's fields are requested (cp.async into shared memory)
+    // before the gathers, so their DRAM latency overlaps the node reads
+    extern __shared__ float g2p_pre[];   // PF_N slots x 256 threads when sp.prefetch
+    float *pre = nullptr;
+    if (sizeof(R) == 4 && sp.prefetch && live) {
+        pre = g2p_pre + threadIdx.x;
+        prefetch_particle<D, R>(pre, P, i);
+    }
     if (live) {
         bool deferred = false;   // (surrogate) return queued: scattered after the accept-or-fallback pass
-        g2p_core<D, R, true, MC3, USL>(P, g, sp, i, nullptr, x, w, s, vol, &deferred);
+        g2p_core<D, R, true, MC3, USL>(P, g, sp, i, pre, x, w, s, vol, &deferred);
         if (deferred) {
             live = false;
         } else if (!particle_weights<D, R>(x, g, w)) {
@@ -1401,8 +1409,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM
             live = false;
         } else {
 #pragma unroll
-            for (int d = 0; d < D; ++d) v[d] = P.v[d][i];
-            m = P.m[i];
+            for (int d = 0; d < D; ++d) v[d] = pf(pre, PF_V + d, P.v[d] + i);
+            m = pf(pre, PF_M, P.m + i);
         }
     }
     int n0 = 0, key = dead_key();

@@ -501,10 +501,12 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ 
                     my_loss += 0.5f * d * d * inv_btot;
                     d *= inv_btot;
                 }
-                st_bf16(T.dz, kmajor_offset(t, o, 16), d);
                 st_bf16(T.dzT, kmajor_offset(o, t, TILE), d);
                 z[o] = d;
             }
+            // the row-major copy as two 16-byte stores (a thread owns its row)
+            st_bf16x8(T.dz, kmajor_offset(t, 0, 16), z);
+            st_bf16x8(T.dz, kmajor_offset(t, 8, 16), z + 8);
             rows_sum16(z, T.dbias + 192);
         }
         // ---- backward through layers 3, 2, 1 (dW_l and dY_{l-1}), then dW_0
@@ -532,10 +534,11 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float *__restrict__ 
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
                     const float d = valid ? dy[i] * gelu_grad(z[i] + S.bias[64 * lp + c + i]) : 0.0f;
-                    st_bf16(T.dz, kmajor_offset(t, c + i, 64), d);
                     st_bf16(T.dzT, kmajor_offset(c + i, t, TILE), d);
                     dy[i] = d;
                 }
+                st_bf16x8(T.dz, kmajor_offset(t, c, 64), dy);
+                st_bf16x8(T.dz, kmajor_offset(t, c + 8, 64), dy + 8);
                 rows_sum16(dy, T.dbias + 64 * lp + c);
             }
         }
