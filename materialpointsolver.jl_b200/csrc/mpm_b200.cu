@@ -745,8 +745,8 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         CK(cudaMemsetAsync(h->bcount, 0, 4, h->stream));
         if (np) L.run("g2p_p2g", [&] {
             if (h->chain) {
-                if (mc3) k_g2p_ts_chain<D, D == 3, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
-                else k_g2p_ts_chain<D, false, R><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);
+                if (mc3) k_g2p_ts_chain<D, D == 3, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+                else k_g2p_ts_chain<D, false, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
                 return;
             }
             if (mc3) k_g2p_ts<D, R, true, D == 3><<<cdiv(np, 256), 256, 0, h->stream>>>(P, g, sp);

@@ -390,7 +390,8 @@ __global__ void __launch_bounds__(128) k_dm3_ts(GDev<R> g, StepParams sp) {
 // position x, stress s, volume vol, porosity nn and pore pressure sw_out.
 template <int D, typename R, bool MC3>
 __device__ __forceinline__ void g2p_ts_core(const PDev<D, R> &P, const GDev<R> &g, const StepParams &sp, int64_t i,
-                                            double *x, AxisW<R> *w, R *s, R &vol, R &nn, R &sw_out, R &kperm) {
+                                            double *x, AxisW<R> *w, R *s, R &vol, R &nn, R &sw_out, R &kperm,
+                                            float *pre = nullptr) {
     load_x<D, R>(P, i, x);
     particle_weights<D, R>(x, g, w);
     const int n0 = window_n0<D, R>(g, w);
@@ -433,7 +434,8 @@ __device__ __forceinline__ void g2p_ts_core(const PDev<D, R> &P, const GDev<R> &
     }
     const R vol_old = P.vol[i];
     double J = 1.0;
-    update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol, nullptr, &J);
+    if (pre) prefetch_wait();
+    update_particle<D, R, MC3>(P, g, sp, i, x, tT, dF, s, vol, pre, &J);
     // water part of G2P_TS!
     const Mat<R> &M = g.mat[P.mat[i]];
     kperm = M.kperm;
@@ -569,8 +571,15 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_TS_P_MINB_F64 : MPM_
     AxisW<R> w[3];
     R s[6] = {0, 0, 0, 0, 0, 0}, vol = 0, nn = 0, sw = 0, kperm = 0;
     R vs[3] = {0, 0, 0}, vw[3] = {0, 0, 0}, ms = 0, mw = 0;
+    // FP32: the one-phase fields requested by cp.async before the gathers
+    extern __shared__ float g2p_pre[];   // PF_N slots x 256 threads when sp.prefetch
+    float *pre = nullptr;
+    if (sizeof(R) == 4 && sp.prefetch && live) {
+        pre = g2p_pre + threadIdx.x;
+        prefetch_particle<D, R>(pre, P, i);
+    }
     if (live) {
-        g2p_ts_core<D, R, MC3>(P, g, sp, i, x, w, s, vol, nn, sw, kperm);
+        g2p_ts_core<D, R, MC3>(P, g, sp, i, x, w, s, vol, nn, sw, kperm, pre);
         if (!particle_weights<D, R>(x, g, w)) {
             atomicOr(g.err, ERR_OOG);
             live = false;
