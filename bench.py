@@ -47,7 +47,7 @@ def parse():
                     choices=["column3d", "slope3d", "batch2d", "column2d", "saturated3d", "example3d", "example2d"],
                     help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
                          "3D slope with a lognormal cohesion field; batch2d: 256 independent 2D slopes "
-                         "(15.5 M particles) advanced together, autotuned during warm-up; column2d: the 3 200-"
+                         "(15.5 M particles) advanced together (both autotuned during warm-up); column2d: the 3 200-"
                          "particle 2D column in FP64 (launch-bound; CUDA graph replay); saturated3d: the 2.56 M-particle column "
                          "as a two-phase (solid + water) saturated soil, coupling TS; example3d: the reference's "
                          "own 3D example (512 000 particles, MVL on), against its published 66.3 it/s; example2d: its "
@@ -214,7 +214,8 @@ EXAMPLES = {"example3d": ("collapse_3d_example", EXAMPLE3D_PUBLISHED,
                           "examples/2d_collapse.ipynb:385: 2.11e3 it/s x 20 000 particles, FP64, unstated NVIDIA GPU")}
 
 
-PASS_VARIANTS = {0: "lane-merged per-particle", 1: "tiled", 2: "box"}
+PASS_VARIANTS = {0: "lane-merged per-particle", 1: "tiled", 2: "box",
+                 3: "lane-merged per-particle, fused pass at 3 CTAs/SM"}
 
 
 def make_case(mc3d, workload="column3d", surrogate=False):
@@ -358,12 +359,13 @@ def run_b200(args):
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
     tuning = None
     Ti = 0.0
-    if args.workload == "batch2d":
+    if args.workload in ("batch2d", "slope3d"):
         # untimed: the autotuner's trials are real steps of the model
         Ti, S, tiled, trial_ms = dev.autotune(dt, Ti, 16)
         tuning = {"sort_every": S, "variant": PASS_VARIANTS[tiled], "tile": dev.tile(), "trial_ms_per_step": trial_ms,
-                  "candidates": "tile shapes x sort periods 8/16/32/64 (lane-merged passes), then tiled and box "
-                                "passes at 16/32; max(16, period) steps each"}
+                  "candidates": "tile shapes x sort periods 8/16/32/64 (lane-merged passes), then the fused "
+                                "pass at 3 CTAs/SM at 32/64, then tiled and box passes at 16/32; "
+                                "max(16, period) steps each"}
     surr_info = None
     if args.surrogate:
         if args.workload != "slope3d":
@@ -463,7 +465,8 @@ def run_b200(args):
                            f"particle state {npart * bp_step / 1e6:.1f} MB < 126 MB L2: L2-resident, not "
                            "flushed (a model of this size runs from L2; launch-bound)"),
                        parallelism=f"replicas x{world}",
-                       **({"slopes": len(case.meta["slopes"]), "tuning": tuning} if tuning else {}),
+                       **({"tuning": tuning} if tuning else {}),
+                       **({"slopes": len(case.meta["slopes"])} if "slopes" in case.meta else {}),
                        **({"surrogate": surr_info} if surr_info else {})),
         "gpu_launches": launches,
         "timed_window": {"ms_per_step": ms_window / K, "sorts": sorts_window, "sort_ms": sort_ms,

@@ -215,12 +215,16 @@ int mpm_sync(mpm_handle *h);
  * windows of neighbouring lanes and reduce into L2, the default; 1 =
  * shared-memory tiled kernels; 2 = box passes: one warp per tile of 32 cells
  * with the tile's node data in shared memory, in FP32 with va = :a and no
- * PIC/MVL/USL/two-phase, else variant 0) and the sort's tile shape (cells; 3D 2x8x2
+ * PIC/MVL/USL/two-phase, else variant 0; 3 = variant 0 with the fused pass
+ * compiled for 3 instead of 4 resident CTAs per SM, i.e. 85 instead of 64
+ * registers, for the FP32 one-phase MUSL step without the restated 3D
+ * Mohr-Coulomb, else variant 0) and the sort's tile shape (cells; 3D 2x8x2
  * (default), 4x8x1, 4x4x2; 2D 4x8 (default), 2x16; mpm_set_tile re-sorts at
  * the next step).  mpm_autotune times, on REAL steps of the model (they advance
  * the simulation exactly like mpm_step, from Ti0, and *Ti_out receives the end
  * time), every tile shape with the re-sort periods 8, 16, 32, 64 (default
- * passes), then the tiled and the box passes at periods 16 and 32; each trial runs
+ * passes), then variant 3 at the best shape so far with periods 32 and 64,
+ * then the tiled and the box passes at periods 16 and 32; each trial runs
  * max(steps_per_trial, period) steps starting with a sort.  It keeps the
  * fastest (mpm_get_tile reports its shape) and writes each trial's ms per step
  * to trial_ms (optional, trial_cap entries) in that order. */

@@ -78,7 +78,7 @@ struct GraphCache {
     double dt = 0;
     void *pbuf0 = nullptr;
     int sort_every = 0;
-    bool tiled = false, box = false;
+    bool tiled = false, box = false, wide = false;
     int surr_mode = 0;
     int tile = 0;   // tx | ty << 8 | tz << 16
     int64_t launches = 0, steps = 0, sorts = 0;
@@ -128,6 +128,7 @@ struct mpm_handle {
     bool cell_major = false; // order inside a tile: rank-major (default) or cell-major (MPM_B200_ORDER=cell)
     bool chain = true;       // FP32 scatters merge chained warp lanes (MPM_B200_CHAIN=0 turns it off)
     bool box = false;        // FP32 MUSL passes with the tile's nodes in shared memory (variant 2; MPM_B200_BOX=1)
+    bool wide = false;       // variant 3: the lane-merged fused pass at 3 resident CTAs per SM (85 registers)
     uint32_t *work = nullptr;   // tile counters of the box passes
     GraphCache graph;
     int64_t graph_launches = 0;
@@ -860,6 +861,7 @@ template <int D, typename R> void issue_step(mpm_handle *h, Launcher &L, double 
         if (np) L.run("g2p_p2g", [&] {
             if (chain) {
                 if (mc3) k_g2p_chain<D, D == 3, false, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
+                else if (h->wide) k_g2p_chain<D, false, false, R, 3><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
                 else k_g2p_chain<D, false, false, R><<<cdiv(np, 256), 256, g2p_smem(sp), h->stream>>>(P, g, sp);
                 return;
             }
@@ -880,7 +882,7 @@ template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double T
     GraphCache &gc = h->graph;
     const int S = h->sort_every;
     const bool match = gc.exec && gc.dt == dt && gc.pbuf0 == h->pbuf[0] && gc.sort_every == S &&
-                       gc.tiled == h->tiled && gc.box == h->box && gc.surr_mode == h->surr_mode &&
+                       gc.tiled == h->tiled && gc.box == h->box && gc.wide == h->wide && gc.surr_mode == h->surr_mode &&
                        gc.tile == tile_code(h->sg);
     if (!match) {
         if (gc.exec) { cudaGraphExecDestroy(gc.exec); gc.exec = nullptr; }
@@ -908,6 +910,7 @@ template <int D, typename R> bool graph_block(mpm_handle *h, double dt, double T
         gc.sort_every = S;
         gc.tiled = h->tiled;
         gc.box = h->box;
+        gc.wide = h->wide;
         gc.surr_mode = h->surr_mode;
         gc.tile = tile_code(h->sg);
         gc.launches = h->launches - l0;
@@ -1782,20 +1785,21 @@ int mpm_log_samples(mpm_handle *h, float *feat, float *target, uint32_t *count, 
 
 int mpm_set_tuning(mpm_handle *h, int32_t sort_every, int32_t tiled) {
     if (!h) return MPM_E_ARG;
-    if (sort_every < 1 || sort_every > 1024 || tiled < 0 || tiled > 2) {
-        h->last_error = "sort_every must be 1..1024 and the particle-pass variant 0, 1 or 2";
+    if (sort_every < 1 || sort_every > 1024 || tiled < 0 || tiled > 3) {
+        h->last_error = "sort_every must be 1..1024 and the particle-pass variant 0, 1, 2 or 3";
         return MPM_E_ARG;
     }
     h->sort_every = sort_every;
     h->tiled = tiled == 1;
     h->box = tiled == 2;
+    h->wide = tiled == 3;
     return MPM_OK;
 }
 
 int mpm_get_tuning(mpm_handle *h, int32_t *sort_every, int32_t *tiled) {
     if (!h) return MPM_E_ARG;
     if (sort_every) *sort_every = h->sort_every;
-    if (tiled) *tiled = h->tiled ? 1 : (h->box ? 2 : 0);
+    if (tiled) *tiled = h->tiled ? 1 : (h->box ? 2 : (h->wide ? 3 : 0));
     return MPM_OK;
 }
 
@@ -1843,7 +1847,7 @@ int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, 
     }
     double Ti = Ti0;
     double best = 1e300;
-    int32_t best_s = h->sort_every, best_t = h->tiled ? 1 : (h->box ? 2 : 0);
+    int32_t best_s = h->sort_every, best_t = h->tiled ? 1 : (h->box ? 2 : (h->wide ? 3 : 0));
     TileShape best_shape{h->sg.tx, h->sg.ty, h->sg.tz};
     int k = 0;
     auto trial = [&](const TileShape &ts, int32_t S, int32_t t) -> int {
@@ -1864,6 +1868,10 @@ int mpm_autotune(mpm_handle *h, double dt, double Ti0, int64_t steps_per_trial, 
     for (const TileShape &ts : shapes)
         for (int32_t S : periods)
             if (int rc = trial(ts, S, 0)) return rc;
+    // the fused pass with the other register cap, at the best shape so far
+    const TileShape shape0 = best_shape;
+    for (int32_t S : {32, 64})
+        if (int rc = trial(shape0, S, 3)) return rc;
     for (int32_t v : {1, 2})
         for (int32_t S : {16, 32})
             if (int rc = trial(shapes[0], S, v)) return rc;

@@ -1384,8 +1384,11 @@ __global__ void __launch_bounds__(256, MPM_P_MINB) k_g2p(PDev<D, R> P, GDev<R> g
 }
 
 // The same pass (FUSE) with the scatter of chained lanes merged (FP32 and FP64).
-template <int D, bool MC3 = false, bool USL = false, typename R = float>
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM_P_MINB) k_g2p_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
+// MINB: resident CTAs per SM in FP32 (the register cap); 4 by default, 3 for
+// particle-pass variant 3 (models whose fused pass runs faster with 85
+// registers and fewer warps, e.g. the random-field slope).
+template <int D, bool MC3 = false, bool USL = false, typename R = float, int MINB = MPM_P_MINB>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MINB) k_g2p_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool live = i < sp.np;
     double x[3];

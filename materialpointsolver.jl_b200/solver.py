@@ -167,7 +167,8 @@ class DeviceModel:
 
     # run-time tuning of the step (no counterpart in the reference)
     def set_tuning(self, sort_every, tiled=0):
-        """Re-sort period and particle-pass variant (0 lane-merged, 1 tiled, 2 box)."""
+        """Re-sort period and particle-pass variant (0 lane-merged, 1 tiled, 2 box,
+        3 lane-merged with the fused pass at 3 resident CTAs per SM)."""
         _lib.check(_lib.lib().mpm_set_tuning(self.h, int(sort_every), int(tiled)), self.h)
 
     def tuning(self):
@@ -194,7 +195,7 @@ class DeviceModel:
         ms = (C.c_double * cap)()
         _lib.check(_lib.lib().mpm_autotune(self.h, dt, Ti, steps_per_trial, C.byref(Tout), C.byref(s),
                                            C.byref(t), ms, cap), self.h)
-        ntrial = 4 * (3 if self.grid.dim == 3 else 2) + 4
+        ntrial = 4 * (3 if self.grid.dim == 3 else 2) + 2 + 4
         return Tout.value, s.value, t.value, list(ms)[:ntrial]
 
     # stress-return surrogate (no counterpart in the reference)

@@ -24,7 +24,7 @@ def tol_stress(tol):
     return TOL32_STRESS if tol == TOL32 else tol
 
 
-def run_both(pkg, orc, case, nsteps, tiled=False, box=True):
+def run_both(pkg, orc, case, nsteps, tiled=False, box=True, variant=None):
     import os
     lib = pkg._lib
     env = {"MPM_B200_TILED": "1" if tiled else "0", "MPM_B200_BOX": "1" if box else "0"}
@@ -38,6 +38,8 @@ def run_both(pkg, orc, case, nsteps, tiled=False, box=True):
                 del os.environ[k]
             else:
                 os.environ[k] = v
+    if variant is not None:
+        dev.set_tuning(dev.tuning()[0], variant)
     dev.step(case.dt, 0.0, nsteps)
     out = fresh_particles(pkg, case.mp)
     dev.download(lib.F_REFERENCE | lib.F_F, out)
@@ -168,16 +170,16 @@ def test_tiled_path(pkg, orc, gpu_lib, dim, prec, tol):
     check_fields(out, o, case.mp, tol, tol_stress(tol))
 
 
-@pytest.mark.parametrize("box", [False, True])
+@pytest.mark.parametrize("variant", [0, 2, 3])
 @pytest.mark.parametrize("dim", [2, 3])
 @pytest.mark.parametrize("model", ["linearelastic", "druckerprager"])
-def test_box_and_chain_passes(pkg, orc, gpu_lib, dim, model, box):
-    """The mixed-mode step through the shared-memory box passes (one warp per
-    tile) and through the per-particle lane-merged passes, each against the
-    oracle."""
+def test_box_and_chain_passes(pkg, orc, gpu_lib, dim, model, variant):
+    """The mixed-mode step through the per-particle lane-merged passes (variant
+    0; 3: the fused pass compiled for 3 resident CTAs per SM) and through the
+    shared-memory box passes (2: one warp per tile), each against the oracle."""
     mk = small2d if dim == 2 else small3d
     case = mk(pkg, constitutive=model, gpu_precision="mixed", sort_every=8)
-    out, o = run_both(pkg, orc, case, 24, box=box)
+    out, o = run_both(pkg, orc, case, 24, box=variant == 2, variant=variant)
     check_fields(out, o, case.mp, TOL32, TOL32_STRESS)
 
 
