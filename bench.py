@@ -47,7 +47,7 @@ def parse():
                     choices=["column3d", "slope3d", "batch2d", "column2d", "saturated3d", "example3d", "example2d"],
                     help="column3d: the 2.56 M-particle 3D column (the headline); slope3d: the 8.0 M-particle "
                          "3D slope with a lognormal cohesion field; batch2d: 256 independent 2D slopes "
-                         "(15.5 M particles) advanced together (both autotuned during warm-up); column2d: the 3 200-"
+                         "(15.5 M particles) advanced together, autotuned during warm-up; column2d: the 3 200-"
                          "particle 2D column in FP64 (launch-bound; CUDA graph replay); saturated3d: the 2.56 M-particle column "
                          "as a two-phase (solid + water) saturated soil, coupling TS; example3d: the reference's "
                          "own 3D example (512 000 particles, MVL on), against its published 66.3 it/s; example2d: its "
@@ -359,13 +359,14 @@ def run_b200(args):
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc, device=local)
     tuning = None
     Ti = 0.0
-    if args.workload in ("batch2d", "slope3d"):
+    if args.workload == "batch2d":
         # untimed: the autotuner's trials are real steps of the model
         Ti, S, tiled, trial_ms = dev.autotune(dt, Ti, 16)
         tuning = {"sort_every": S, "variant": PASS_VARIANTS[tiled], "tile": dev.tile(), "trial_ms_per_step": trial_ms,
                   "candidates": "tile shapes x sort periods 8/16/32/64 (lane-merged passes), then the fused "
-                                "pass at 3 CTAs/SM at 32/64, then tiled and box passes at 16/32; "
-                                "max(16, period) steps each"}
+                                "pass at 3 CTAs/SM at 32/64, then tiled and box passes at 16/32 "
+                                "(max(16, period) steps each), then the best variant-0 and the best "
+                                "other candidate again back to back (64 steps each)"}
     surr_info = None
     if args.surrogate:
         if args.workload != "slope3d":
@@ -517,7 +518,7 @@ def extra_forms(pkg, local, K, W):
     its slopes against the same slopes stepped alone; slope3d -- the 8.0 M-
     particle 3D slope (lognormal cohesion field, Drucker-Prager) stepped
     plainly and with the trained stress-return surrogate from the same state
-    (samples logged from 60 plain steps, 6 epochs of training on the device),
+    (samples logged from 60 plain steps, 20 epochs of training on the device),
     with the surrogate's accepted fraction and its run-out / displacement
     error against the plain step after the same K steps."""
     out = {}
@@ -568,9 +569,9 @@ def extra_forms(pkg, local, K, W):
                 feat, tgt, Ti = S_.collect_samples(dev, case.dt, 0.0, 60, 6_000_000, every=8, device=local)
                 sur = S_.Surrogate(seed=1, device=local)
                 sur.set_norm(feat, tgt)
-                losses = sur.train(feat, tgt, epochs=6, batch=16384, lr=3e-3, lr_end=1e-4)
+                losses = sur.train(feat, tgt, epochs=20, batch=16384, lr=3e-3, lr_end=1e-4)
                 dev.set_surrogate(sur, tol=1e-3, sref=1e3)
-                info = {"train_samples": int(feat.shape[0]), "epochs": 6,
+                info = {"train_samples": int(feat.shape[0]), "epochs": 20,
                         "loss_first_last": [losses[0], losses[-1]], "setup_s": time.perf_counter() - t0}
                 del feat, tgt
             else:

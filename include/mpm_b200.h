@@ -225,9 +225,13 @@ int mpm_sync(mpm_handle *h);
  * time), every tile shape with the re-sort periods 8, 16, 32, 64 (default
  * passes), then variant 3 at the best shape so far with periods 32 and 64,
  * then the tiled and the box passes at periods 16 and 32; each trial runs
- * max(steps_per_trial, period) steps starting with a sort.  It keeps the
- * fastest (mpm_get_tile reports its shape) and writes each trial's ms per step
- * to trial_ms (optional, trial_cap entries) in that order. */
+ * max(steps_per_trial, period) steps starting with a sort.  Since the trials
+ * advance the model (and a growing flow makes later trials slower), the
+ * fastest variant-0 candidate and the fastest other candidate are then timed
+ * again back to back, 64 steps each, and the faster of the two is kept
+ * (mpm_get_tile reports its shape).  Each timed run's ms per step goes to
+ * trial_ms (optional, trial_cap entries) in that order, the two final runs
+ * last. */
 int mpm_set_tuning(mpm_handle *h, int32_t sort_every, int32_t tiled);
 int mpm_get_tuning(mpm_handle *h, int32_t *sort_every, int32_t *tiled);
 int mpm_set_tile(mpm_handle *h, int32_t tx, int32_t ty, int32_t tz);

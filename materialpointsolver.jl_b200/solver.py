@@ -187,7 +187,8 @@ class DeviceModel:
 
     def autotune(self, dt, Ti, steps_per_trial=32):
         """Time every (tile shape, sort period, particle-pass variant)
-        candidate on real steps of this model and keep the fastest.  Returns
+        candidate on real steps of this model, time the two finalists again
+        back to back and keep the faster.  Returns
         (Ti after the trial steps, sort_every, variant, per-trial ms per step in
         the library's candidate order); self.tile() gives the chosen shape."""
         Tout, s, t = C.c_double(), C.c_int32(), C.c_int32()
@@ -195,7 +196,7 @@ class DeviceModel:
         ms = (C.c_double * cap)()
         _lib.check(_lib.lib().mpm_autotune(self.h, dt, Ti, steps_per_trial, C.byref(Tout), C.byref(s),
                                            C.byref(t), ms, cap), self.h)
-        ntrial = 4 * (3 if self.grid.dim == 3 else 2) + 2 + 4
+        ntrial = 4 * (3 if self.grid.dim == 3 else 2) + 2 + 4 + 2
         return Tout.value, s.value, t.value, list(ms)[:ntrial]
 
     # stress-return surrogate (no counterpart in the reference)

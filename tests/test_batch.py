@@ -113,16 +113,17 @@ def test_batch_matches_oracle(pkg, orc, gpu_lib):
 def test_autotune_steps_are_model_steps(pkg, orc, gpu_lib, prec, tol):
     """The autotuner's trials (2 tile shapes x re-sort periods 8, 16, 32, 64 at
     max(12, period) steps each, then the fused pass at 3 CTAs per SM at periods
-    32 and 64, then the tiled and the box passes at periods 16 and 32) are 440
-    ordinary steps: the state equals the oracle's after 440 steps (in the mixed
-    mode through every variant and tile shape), and the chosen tuning is one of
-    the candidates and stays set."""
+    32 and 64, then the tiled and the box passes at periods 16 and 32, then the
+    two finalists again, 64 steps each) are 568 ordinary steps: the state
+    equals the oracle's after 568 steps (in the mixed mode through every
+    variant and tile shape), and the chosen tuning is one of the candidates and
+    stays set."""
     case = small_batch(pkg, 3, gpu_precision=prec)
     dev = pkg.DeviceModel(case.args, case.grid, case.mp, case.attr, case.bc)
     Ti, S, tiled, ms = dev.autotune(case.dt, 0.0, 12)
-    nsteps = 2 * (12 + 16 + 32 + 64) + (32 + 64) + 2 * (16 + 32)
-    assert nsteps == 440
-    assert S in (8, 16, 32, 64) and tiled in (0, 1, 2, 3) and len(ms) == 14 and all(m > 0 for m in ms)
+    nsteps = 2 * (12 + 16 + 32 + 64) + (32 + 64) + 2 * (16 + 32) + 2 * 64
+    assert nsteps == 568
+    assert S in (8, 16, 32, 64) and tiled in (0, 1, 2, 3) and len(ms) == 16 and all(m > 0 for m in ms)
     assert dev.tuning() == (S, tiled)
     assert dev.tile() in ((4, 8, 1), (2, 16, 1))
     assert Ti == pytest.approx(nsteps * case.dt, rel=1e-12)
