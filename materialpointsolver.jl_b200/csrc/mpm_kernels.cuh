@@ -1268,9 +1268,15 @@ __device__ __forceinline__ void g2p_core(const PDev<D, R> &P, const GDev<R> &g, 
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 const R wy = w[1].N[b], gy = w[1].dN[b];
-                if (wy == R(0)) continue;
-                const Node8<R> q = g.gat[col + b];
-                const auto du = USL ? q.a : q.b;
+                // a node of zero weight (it then has zero dN too) is not read,
+                // and its sums are formed with Δu = Δu_c and q = 0, i.e. add
+                // nothing: the load is skipped by a predicate, the sums run
+                // unconditionally (no divergent branch in the inner loop)
+                Node8<R> q;
+                q.a = mk4<R>(0, 0, 0, 0);
+                q.b = q.a;
+                if (wy != R(0)) q = g.gat[col + b];
+                const auto du = USL ? q.a : (wy != R(0) ? q.b : duc);
                 if constexpr (std::is_same<R, float>::value) {
                     // x and y components as packed FP32 pairs
                     const float2 w2 = make_float2(wy, wy), g2 = make_float2(gy, gy);
