@@ -10,7 +10,7 @@ oracle's final displacement field by 2.3e-3, so FP32 rounding anywhere in the
 state gives ~2e-3 while the run-out stays within ~1e-5.  Config 2 (the 3D
 column, 2 560 000 particles) runs a 20-step prefix against the oracle in both
 modes; its flow is well conditioned, and over the whole second the mixed mode
-stays within ~1e-6 of the all-FP64 device mode (checked here on the same
+stays within a few 1e-6 of the all-FP64 device mode (checked here on the same
 column at h = 0.02 m and on a 2D elastic column): the deformation gradient is
 advanced as F + ΔF·F, since FP32's (1 + ΔF)·F drops the low bits of the
 per-step increment with the same sign every step and biased the displacement
