@@ -268,7 +268,6 @@ template <typename R> GDev<R> gdev_from(mpm_handle *h) {
         c.half_lp = (R)(0.5 * lp[a]);
         c.h_m_hl = (R)(hh[a] - 0.5 * lp[a]);
         c.h_p_hl = (R)(hh[a] + 0.5 * lp[a]);
-        c.inv4hl = (R)(1.0 / (4.0 * hh[a] * lp[a]));
         c.invhl = (R)(1.0 / (hh[a] * lp[a]));
         c.invh = (R)(1.0 / hh[a]);
         c.nn = (int)nn[a];

@@ -82,7 +82,7 @@ template <typename R> struct AxisC {
     double inv_h;       // 1/h (FP64) for the fast cell index
     double supp;        // h + lp/2: candidate test |Δ| < supp (utils_OS.jl:220-221)
     R hr, lp, half_lp, h_m_hl, h_p_hl;   // h, lp, lp/2, h - lp/2, h + lp/2
-    R inv4hl, invhl, invh;               // 1/(4 h lp), 1/(h lp), 1/h
+    R invhl, invh;                       // 1/(h lp), 1/h
     int nn, nc;         // nodes / cells on this axis
 };
 
