@@ -923,7 +923,11 @@ __global__ void __launch_bounds__(256, MPM_DMAP_MINB) k_dmap(PDev<D, R> P, GDev<
 // The same pass with the re-scatter of chained lanes merged (FP32 and FP64).
 template <int D, typename R = float, bool GEN = true>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM_DMAP_CHAIN_MINB) k_dmap_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // the particles in reverse block order: the pass before this one (the
+    // fused pass) ends on the last particles and the one after it starts on
+    // the first, so each pass starts on the data the previous one touched last
+    // (still in L2; the column's double mapping touches ~130 MB, about L2's size)
+    const int64_t i = (int64_t)(gridDim.x - 1 - blockIdx.x) * blockDim.x + threadIdx.x;
     const bool live = i < sp.np;
     AxisW<R> w[3];
     R p[3] = {0, 0, 0};
