@@ -116,10 +116,12 @@ template <typename R> struct GDev {
 template <typename T> __device__ __forceinline__ T ldcs(const T *p) { return __ldcs(p); }
 template <typename T> __device__ __forceinline__ void stcs(T *p, T v) { __stcs(p, v); }
 
-// Node blocks: 4 (x) x 8 (y) x 4 (z) nodes in 3D, 16 (x) x 8 (y) in 2D; one
-// 128-thread CTA per block in the node passes, y fastest.
+// Node blocks: 4 (x) x 8 (y) x 4 (z) nodes in 3D, 8 (x) x 8 (y) in 2D; one
+// CTA per block in the node passes (128 / 64 threads), y fastest.  The 2D
+// blocks are the smaller because thin 2D bodies (slopes) leave more of a
+// larger block's nodes massless; halving the 3D blocks measured slower.
 template <int D> struct Blk {
-    static constexpr int BX = D == 3 ? 4 : 16, BY = 8, BZ = D == 3 ? 4 : 1;
+    static constexpr int BX = D == 3 ? 4 : 8, BY = 8, BZ = D == 3 ? 4 : 1;
     static constexpr int NT = BX * BY * BZ;
 };
 
