@@ -280,7 +280,9 @@ __global__ void __launch_bounds__(256) k_dmap_ts(PDev<D, R> P, GDev<R> g, StepPa
 // dm2_scatter_chain).
 template <int D, typename R = float>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? MPM_CHAIN_MINB_F64 : MPM_TS_DMAP_CHAIN_MINB) k_dmap_ts_chain(PDev<D, R> P, GDev<R> g, StepParams sp) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // reverse block order, as k_dmap_chain: each pass starts on the particles
+    // the previous pass touched last
+    const int64_t i = (int64_t)(gridDim.x - 1 - blockIdx.x) * blockDim.x + threadIdx.x;
     const bool live = i < sp.np;
     AxisW<R> w[3];
     R ps[3] = {0, 0, 0}, pw[3] = {0, 0, 0};
