@@ -218,7 +218,8 @@ int mpm_sync(mpm_handle *h);
  * PIC/MVL/USL/two-phase, else variant 0; 3 = variant 0 with the fused pass
  * compiled for 3 instead of 4 resident CTAs per SM, i.e. 85 instead of 64
  * registers, for the FP32 one-phase MUSL step without the restated 3D
- * Mohr-Coulomb, else variant 0) and the sort's tile shape (cells; 3D 2x8x2
+ * Mohr-Coulomb, else variant 0; variant 3 is the default of 3D models, variant
+ * 0 of 2D ones) and the sort's tile shape (cells; 3D 2x8x2
  * (default), 4x8x1, 4x4x2; 2D 4x8 (default), 2x16; mpm_set_tile re-sorts at
  * the next step).  mpm_autotune times, on REAL steps of the model (they advance
  * the simulation exactly like mpm_step, from Ti0, and *Ti_out receives the end

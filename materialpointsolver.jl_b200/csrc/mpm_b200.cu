@@ -128,7 +128,7 @@ struct mpm_handle {
     bool cell_major = false; // order inside a tile: rank-major (default) or cell-major (MPM_B200_ORDER=cell)
     bool chain = true;       // FP32 scatters merge chained warp lanes (MPM_B200_CHAIN=0 turns it off)
     bool box = false;        // FP32 MUSL passes with the tile's nodes in shared memory (variant 2; MPM_B200_BOX=1)
-    bool wide = false;       // variant 3: the lane-merged fused pass at 3 resident CTAs per SM (85 registers)
+    bool wide = false;       // variant 3: the lane-merged fused pass at 3 resident CTAs per SM (85 registers; the 3D default)
     uint32_t *work = nullptr;   // tile counters of the box passes
     GraphCache graph;
     int64_t graph_launches = 0;
@@ -1649,6 +1649,10 @@ int mpm_create(const mpm_desc *d, mpm_handle **out) {
         if (const char *e = getenv("MPM_B200_ORDER")) h->cell_major = (std::string(e) == "cell");
         if (const char *e = getenv("MPM_B200_CHAIN")) h->chain = std::atoi(e) != 0;
         if (const char *e = getenv("MPM_B200_BOX")) h->box = std::atoi(e) != 0;
+        // 3D models start with the fused pass at 3 resident CTAs per SM
+        // (variant 3): measured faster on the 3D column and slope (0.414 ->
+        // 0.400 ms, 1.267 -> 1.243 ms), slower on the 2D slope batch
+        h->wide = h->d.dim == 3 && !h->box;
         h->work = (uint32_t *)dalloc(h, 16);
         if (!h->fp64) box_prepare(h);
         *out = h;
