@@ -262,7 +262,7 @@ def pin_particles(mp):
         setattr(mp, name, b)
 
 
-G2P_TRAFFIC_PER_PARTICLE = 254.2   # B, dram__bytes_read.sum + dram__bytes_write.sum / np
+G2P_TRAFFIC_PER_PARTICLE = 250.9   # B, dram__bytes_read.sum + dram__bytes_write.sum / np
 
 # algorithmic bytes per particle / per active node
 BP_STEP_3D = 212       # particle state read + written once per step
